@@ -1,0 +1,188 @@
+/*
+ * libvox: B200-native piecewise-constant JVIE-II frequency solve.
+ *
+ * C-ABI boundary for VoxPhoton's hot path.  Each entry point replaces one
+ * MATLAB call of the reference (paths relative to the reference project):
+ *
+ *   vox_op_create        the device upload done once per operator in
+ *                        piecewise_constant/src_vie/src_solver/JVIE_Solver_const.m:277-284
+ *                        (fN, Mr, Mc sent to the GPU), with the operator itself
+ *                        from getOPERATORS_SAM.m:83-91 (fN) or its Toeplitz form
+ *   vox_mv_AN            mv_AN_const(JIn0,fN,Mr,Mc,Gram,transp_flag,idx,GPU_flag)
+ *                        piecewise_constant/src_vie/src_mvp/mv_AN_const.m:1
+ *   vox_mv_L             mv_L_const(JIn0,fN,r,Gram,idx,GPU_flag)
+ *                        piecewise_constant/src_vie/src_mvp/mv_L_const.m:1
+ *   vox_precond_create_level1 + vox_precond_apply
+ *                        level_1_parallel_func_N.m:1 + Bragg_MOR_script.m:61-72 (build)
+ *                        and chan_mvp_idx(inv_blocks,JIn,L,M,N,idx)
+ *                        piecewise_constant/src_preconditioning/chan_mvp_idx.m:2 (apply)
+ *   vox_precond_create_blocks
+ *                        chan_mvp_idx with caller-supplied inverse blocks
+ *   vox_pgmres           [x,flag,relres,iter,resvec] = pgmres(A,b,restart,tol,maxit,L1,[],R1)
+ *                        piecewise_constant/src_numeric/src_iterative/pgmres.m:70
+ *   vox_solve_refined    complex64 GMRES inside an FP64 iterative-refinement loop
+ *                        (no reference counterpart; meets pgmres.m:175's relres test)
+ *   vox_jvie_rhs         Vrhs of JVIE_Solver_const.m:151-157 with the JVIE-II scaling :243-251
+ *   vox_assemble_toeplitz  assembly_nop_const.m:1-174 (far/medium/near cubature,
+ *                        singular self/edge/vertex terms, face projection) on the host
+ *
+ * Conventions: complex arrays are split real/imaginary double arrays as in
+ * MATLAB's classic mxArray (mxGetPr/mxGetPi); grids are column-major (x
+ * fastest); index vectors are 1-based doubles as MATLAB passes them.  The
+ * caller owns all host buffers; the library owns device state behind opaque
+ * handles.  A handle is used by one host thread at a time.  Every call returns
+ * a vox_status; vox_last_error() gives the text of the last failure on the
+ * calling thread.
+ */
+#ifndef VOX_H_
+#define VOX_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VOX_ABI_VERSION 1
+
+typedef enum {
+  VOX_OK = 0,
+  VOX_ERR_BAD_ARG = 1,
+  VOX_ERR_OOM = 2,
+  VOX_ERR_NOT_CONVERGED = 3,
+  VOX_ERR_TIMEOUT = 4,
+  VOX_ERR_CUDA = 5,
+  VOX_ERR_UNSUPPORTED = 6
+} vox_status;
+#define VOX_CUDA_ERROR VOX_ERR_CUDA
+
+typedef enum { VOX_C128 = 0, VOX_C64 = 1 } vox_prec;
+typedef enum { VOX_NOTRANSP = 0, VOX_TRANSP = 1 } vox_transp;
+typedef enum { VOX_PREC_NONE = 0, VOX_PREC_LEFT = 1, VOX_PREC_RIGHT = 2 } vox_side;
+
+typedef struct vox_op_s* vox_op_t;
+typedef struct vox_precond_s* vox_precond_t;
+
+typedef struct {
+  int L, M, N;               /* domain grid */
+  /* Either the FFT-circulant fN (LfN x MfN x NfN x 6, column-major, the
+   * array mv_AN_const receives) ... */
+  int LfN, MfN, NfN;
+  const double* fN_re;
+  const double* fN_im;
+  /* ... or the Toeplitz tensor G_mn (L x M x N x 6, assembly_nop_const's
+   * output).  Exactly one of fN_re / G_re must be non-NULL. */
+  const double* G_re;
+  const double* G_im;
+  const double* Mr_re;       /* L x M x N; NULL => Mr == 1 (JVIE-II) */
+  const double* Mr_im;       /* may be NULL (real Mr) */
+  const double* Mc_re;       /* L x M x N */
+  const double* Mc_im;       /* may be NULL (real Mc) */
+  double gram;               /* voxel volume dx^3 */
+  const double* idx;         /* n_idx 1-based positions in the 3*L*M*N grid */
+  long long n_idx;
+  int precisions;            /* bit 0: complex128, bit 1: complex64 (0 => both) */
+  int device;                /* CUDA device ordinal */
+} vox_op_desc;
+
+typedef struct {
+  int flag;                  /* 0 converged (relres <= tol), 1 not converged */
+  double relres;             /* ||b - A x|| / ||b|| in FP64 (pgmres.m:175) */
+  int iter_inner;            /* iterations of the last restart cycle (iter(1)) */
+  int iter_outer;            /* restart cycles (iter(2)) */
+  int total_iters;           /* Arnoldi steps over all cycles (and refinements) */
+  int refinements;           /* FP64 refinement steps (vox_solve_refined) */
+  double* resvec;            /* optional caller buffer for the preconditioned */
+  long long resvec_cap;      /*   relative residual history (pgmres's resvec) */
+  long long n_resvec;        /* entries written */
+  double seconds;            /* wall time of the call */
+} vox_gmres_info;
+
+const char* vox_last_error(void);
+int vox_abi_version(void);
+
+vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out);
+void vox_op_destroy(vox_op_t op);
+/* Sizes chosen for the device matvec: padded grid and vector length. */
+vox_status vox_op_info(vox_op_t op, int* Px, int* Py, int* Pz, long long* n);
+/* Run this operator's work on the caller's cudaStream_t (NULL restores the
+ * operator's own stream).  No reference counterpart (MATLAB has no streams). */
+vox_status vox_op_set_stream(vox_op_t op, void* stream);
+/* Kernels launched so far by the solver entry points on this operator. */
+vox_status vox_op_stats(vox_op_t op, long long* launches);
+/* Device time (ms, CUDA events on the operator's stream, mean of reps) of each
+ * kernel of one GMRES iteration: [0..2] matvec x-forward / plane / x-inverse,
+ * [3..5] preconditioner x-forward / per-mode solve / x-inverse (0 if pc is
+ * NULL), [6..9] Gram-Schmidt dots / update+dots / update+norm / scale at a
+ * basis of kgs+1 vectors.  ms_out holds 10 doubles. */
+vox_status vox_profile_stages(vox_op_t op, vox_precond_t pc, vox_prec prec, int restart, int kgs,
+                              int reps, double* ms_out);
+
+/* JOut = A JIn (transp == VOX_NOTRANSP) or A' JIn, on the support idx.
+ * Host buffers of length n_idx (split complex). */
+vox_status vox_mv_AN(vox_op_t op, int transp, vox_prec prec, const double* in_re,
+                     const double* in_im, double* out_re, double* out_im);
+/* JOut = (N - Gram) JIn on the support (mv_L_const). */
+vox_status vox_mv_L(vox_op_t op, vox_prec prec, const double* in_re, const double* in_im,
+                    double* out_re, double* out_im);
+/* Device variant: interleaved complex (double2 for C128, float2 for C64)
+ * device pointers of length n; stream is a cudaStream_t (NULL = the op's). */
+vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* in, void* out,
+                            void* stream);
+
+/* Level-1 circulant preconditioner (T. Chan circulant along x, per-mode dense
+ * blocks inv(Gram*I - diag(face3)*circ_i)); face3 = (m-1)/m with m the x-mean of
+ * Mr (length 3*M*N, real).  G_re/G_im: the L x M x N x 6 Toeplitz tensor. */
+vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const double* G_im,
+                                     const double* face3, vox_precond_t* out);
+/* Preconditioner from caller-supplied inverse blocks: L blocks of (3MN)^2,
+ * each column-major, concatenated (chan_mvp_idx's inv_blocks). */
+vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const double* blk_im,
+                                     vox_precond_t* out);
+void vox_precond_destroy(vox_precond_t p);
+/* mvp = chan_mvp_idx(inv_blocks, JIn, L, M, N, idx), host buffers of length n_idx. */
+vox_status vox_precond_apply(vox_precond_t p, vox_prec prec, const double* in_re,
+                             const double* in_im, double* out_re, double* out_im);
+
+/* pgmres(A, b, restart, tol, maxit, L1) / (..., [], [], R1): one precision end to end. */
+vox_status vox_pgmres(vox_op_t op, vox_precond_t pc, int side, vox_prec prec, const double* b_re,
+                      const double* b_im, int restart, double tol, int maxit, double* x_re,
+                      double* x_im, vox_gmres_info* info);
+
+/* complex64 GMRES (matvec, preconditioner, Krylov basis in FP32; inner
+ * products, norms and Givens in FP64) inside FP64 iterative refinement:
+ * repeat { r = b - A x (FP64); d = GMRES_c64(A, r/|r|, inner_tol); x += |r| d }
+ * until ||b - A x|| / ||b|| <= tol.  inner_tol <= 0 picks 1e-3. */
+vox_status vox_solve_refined(vox_op_t op, vox_precond_t pc, int side, const double* b_re,
+                             const double* b_im, double tol, int restart, int maxit_inner,
+                             double inner_tol, int max_refine, double* x_re, double* x_im,
+                             vox_gmres_info* info);
+
+/* Device-resident variants (interleaved double2 device vectors of length n). */
+vox_status vox_pgmres_device(vox_op_t op, vox_precond_t pc, int side, vox_prec prec,
+                             const void* b, int restart, double tol, int maxit, void* x,
+                             vox_gmres_info* info);
+vox_status vox_solve_refined_device(vox_op_t op, vox_precond_t pc, int side, const void* b,
+                                    double tol, int restart, int maxit_inner, double inner_tol,
+                                    int max_refine, void* x, vox_gmres_info* info);
+
+/* Vrhs = Gram * (j omega eo Mc_raw) .* Einc(idx) ./ Mr(idx)  (JVIE-II), with
+ * Mc_raw = e_r - 1, Mr = e_r; e_r and Einc column-major (L x M x N, x3 for Einc). */
+vox_status vox_jvie_rhs(int L, int M, int N, const double* er_re, const double* er_im,
+                        const double* Einc_re, const double* Einc_im, double gram, double freq,
+                        const double* idx, long long n_idx, double* out_re, double* out_im);
+
+/* Host assembly of the Toeplitz tensor G_mn (L x M x N x 6, column-major),
+ * assembly_nop_const(r, ko, dx, 'DEMCEM').  nthreads <= 0 uses all cores. */
+vox_status vox_assemble_toeplitz(int L, int M, int N, double ko, double dx, int nthreads,
+                                 double* G_re, double* G_im);
+/* The five singular face-pair integrals (self, edge coplanar/orthogonal,
+ * vertex coplanar/orthogonal) of exp(-j ko R)/R over dx-squares: out[10] as
+ * re/im pairs in the order ST, EAc, EAo, VAc, VAo. */
+vox_status vox_singular_integrals(double ko, double dx, int order, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VOX_H_ */

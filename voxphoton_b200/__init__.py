@@ -1,0 +1,13 @@
+"""voxphoton_b200: B200-native piecewise-constant JVIE-II frequency solve.
+
+Hot path (hand-written sm_100a CUDA in libvox.so, C-ABI in include/vox.h):
+FFT-circulant matvec, level-1 circulant preconditioner and device GMRES with
+an FP32 + FP64-refinement solver.  See voxphoton_b200.vie for the
+MATLAB-facing calls (mv_AN_const, chan_mvp_idx, pgmres).
+"""
+from .vie import (Operator, Preconditioner, assemble_toeplitz, chan_mvp_idx, face3_from_Mr,
+                  jvie_rhs, mv_AN_const, mv_L_const, pgmres, singular_integrals, solve_refined)
+
+__all__ = ["Operator", "Preconditioner", "assemble_toeplitz", "chan_mvp_idx", "face3_from_Mr",
+           "jvie_rhs", "mv_AN_const", "mv_L_const", "pgmres", "singular_integrals",
+           "solve_refined"]

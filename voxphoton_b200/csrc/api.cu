@@ -1,0 +1,699 @@
+// libvox C-ABI: operator handles, matvec entry points, device GMRES driver and
+// the FP32 + FP64-refinement solver.  One translation unit holds all device
+// code so constant tables and templates are instantiated once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <type_traits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vox.h"
+#include "krylov.cuh"
+#include "mvp.cuh"
+#include "precond.cuh"
+
+namespace vox {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+
+// ------------------------------------------------------------ size choice
+// Cost (in complex-add units per point) of one Stockham stage of radix r.
+static double stage_cost(int r) {
+  switch (r) {
+    case 2: return 2.0;
+    case 3: return 2.7;
+    case 4: return 2.5;
+    case 5: return 3.2;
+    case 7: return 4.5;
+    case 8: return 3.0;
+    default: return 1.0 + 0.5 * r;
+  }
+}
+
+static bool smooth7(int n) {
+  for (int p : {2, 3, 5, 7})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+static double fft_cost(int n) {
+  FftPlan p;
+  if (!make_fft_plan(n, &p)) return 1e300;
+  double c = 0;
+  for (int s = 0; s < p.nst; s++) c += stage_cost(p.radix[s]);
+  return c * n;
+}
+
+// Padded length for a Toeplitz axis of length n: the cheapest 7-smooth size
+// in [2n-1, 1.15*(2n-1)+8].
+static int choose_pad(int n) {
+  const int lo = std::max(1, 2 * n - 1);
+  const int hi = (int)(lo * 1.15) + 8;
+  int best = -1;
+  double bc = 1e300;
+  for (int p = lo; p <= hi; p++) {
+    if (!smooth7(p)) continue;
+    const double c = fft_cost(p);
+    if (c < bc) {
+      bc = c;
+      best = p;
+    }
+  }
+  return best;
+}
+
+// Forward twiddle table W_n^m = exp(-2 pi i m / n), m in [0, n).
+static std::vector<double2> twiddles(int n) {
+  std::vector<double2> w(n);
+  for (int m = 0; m < n; m++) {
+    // reduce the angle to the first octant for accuracy
+    const long long num = (long long)m;
+    const double a = 2.0 * M_PI * (double)num / (double)n;
+    w[m] = make_double2(std::cos(a), -std::sin(a));
+  }
+  // exact values at the quarter points
+  for (int m = 0; m < n; m++) {
+    if ((4LL * m) % n == 0) {
+      const int q = (int)((4LL * m) / n);
+      const double c[4] = {1, 0, -1, 0}, s[4] = {0, 1, 0, -1};
+      w[m] = make_double2(c[q], -s[q]);
+    }
+  }
+  return w;
+}
+
+template <typename T>
+static vox_status dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return VOX_OK;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
+              " bytes failed: " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? VOX_ERR_OOM : VOX_ERR_CUDA;
+  }
+  return VOX_OK;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define VOX_TRY(x)                  \
+  do {                              \
+    vox_status s__ = (x);           \
+    if (s__ != VOX_OK) return s__;  \
+  } while (0)
+
+// GMRES workspace for one precision and restart length.
+template <typename R>
+struct GmresWork {
+  int m = 0;
+  Cx<R>* V = nullptr;  // (m+1) x n
+  Cx<R>* w = nullptr;
+  Cx<R>* t = nullptr;  // preconditioner output / right-precond temp
+  Cx<R>* r = nullptr;
+  Cx<R>* x = nullptr;
+  Cx<R>* b = nullptr;
+  GmresDev* st = nullptr;
+  GmresDev* hst = nullptr;  // pinned host mirror for readback
+  std::map<std::pair<void*, int>, cudaGraphExec_t> graphs;  // (precond, side) -> cycle
+  void release() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+    cudaFree(V);
+    cudaFree(w);
+    cudaFree(t);
+    cudaFree(r);
+    cudaFree(x);
+    cudaFree(b);
+    cudaFree(st);
+    if (hst) cudaFreeHost(hst);
+    V = w = t = r = x = b = nullptr;
+    st = nullptr;
+    hst = nullptr;
+  }
+};
+
+}  // namespace vox
+
+using namespace vox;
+
+struct vox_op_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;  // created here; `stream` may be the caller's
+  long long launches = 0;             // kernels launched by solver entry points
+  std::map<cudaGraphExec_t, int> graph_nodes;
+  OpGeom g{};
+  FftPlan px{}, py{}, pz{};
+  int* vmap = nullptr;
+  bool has_d = false, has_f = false;
+  OpBuffers<double> d;
+  OpBuffers<float> f;
+  double gram = 0;
+  // host staging (pinned) and device vectors for host-buffer entry points
+  double2* h_in = nullptr;
+  double2* h_out = nullptr;
+  double2* d_in = nullptr;
+  double2* d_out = nullptr;
+  float2* f_in = nullptr;
+  float2* f_out = nullptr;
+  // refinement workspace (c128 x, r, b) and casts
+  double2* x64 = nullptr;
+  double2* r64 = nullptr;
+  double2* b64 = nullptr;
+  GmresDev* st64 = nullptr;  // scratch for norms in the refinement loop
+  GmresWork<double> wd;
+  GmresWork<float> wf;
+  std::vector<vox_precond_s*> pcs;
+};
+
+namespace vox {
+
+template <typename R> OpBuffers<R>& bufs(vox_op_s* op);
+template <> OpBuffers<double>& bufs<double>(vox_op_s* op) { return op->d; }
+template <> OpBuffers<float>& bufs<float>(vox_op_s* op) { return op->f; }
+template <typename R> GmresWork<R>& work(vox_op_s* op);
+template <> GmresWork<double>& work<double>(vox_op_s* op) { return op->wd; }
+template <> GmresWork<float>& work<float>(vox_op_s* op) { return op->wf; }
+
+static size_t xsmem(const OpGeom& g, size_t csz) { return 2ull * g.ybx * g.sx * csz; }
+static size_t psmem(const OpGeom& g, size_t csz) {
+  const size_t wsize = std::max((size_t)g.rc * g.sy, (size_t)3 * g.kc * g.sz);
+  return ((size_t)3 * g.N * g.sy + 2 * wsize) * csz;
+}
+
+// Launch the three matvec kernels.
+template <typename R>
+static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cudaStream_t st,
+                         const int* skip) {
+  OpBuffers<R>& b = bufs<R>(op);
+  const OpGeom& g = b.geo;
+  const size_t cs = sizeof(Cx<R>);
+  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3);
+  const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
+  k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, b.T1,
+                                            skip);
+  k_plane<R><<<g.Px, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, b.T1, b.fN, b.T2,
+                                               skip);
+  k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, in, b.Mr, b.Mc,
+                                            b.gram, scale, b.out_scale, mode, out, skip);
+  VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
+template <typename R>
+static vox_status set_smem_attrs(const OpGeom& g) {
+  const size_t cs = sizeof(Cx<R>);
+  VOX_CUDA(cudaFuncSetAttribute(k_xfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)xsmem(g, cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_xinv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)xsmem(g, cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_plane<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)psmem(g, cs)));
+  return VOX_OK;
+}
+
+static const size_t kSmemBudget = 110 * 1024;  // two CTAs per SM
+
+// Pick launch shapes for precision of size csz; returns false if a plane
+// cannot be staged in shared memory.
+static bool pick_shapes(OpGeom& g, size_t csz) {
+  g.sx = pad_stride(g.Px);
+  g.sy = pad_stride(g.Py);
+  g.sz = pad_stride(g.Pz);
+  int yb = (int)(kSmemBudget / (2ull * g.sx * csz));
+  if (yb < 1) {
+    if (2ull * g.sx * csz > 220 * 1024) return false;
+    yb = 1;
+  }
+  g.ybx = std::max(1, std::min({yb, 8, g.M}));
+  // kernel 2: try all rows and all ky columns, then shrink the chunks
+  const int rows = 3 * g.N;
+  g.rc = rows;
+  g.kc = g.Py;
+  auto fits = [&](size_t budget) { return psmem(g, csz) <= budget; };
+  while (!fits(kSmemBudget) && (g.kc > 1 || g.rc > 1)) {
+    if ((size_t)3 * g.kc * g.sz >= (size_t)g.rc * g.sy && g.kc > 1)
+      g.kc = (g.kc + 1) / 2;
+    else if (g.rc > 1)
+      g.rc = (g.rc + 1) / 2;
+    else
+      g.kc = (g.kc + 1) / 2;
+  }
+  return fits(220 * 1024);
+}
+
+// In-place batched FFT of a 3-D array along one axis (setup path).
+static vox_status fft_axis_d(double2* data, int d0, int d1, int d2, long long s0, long long s1,
+                             long long s2, long long scomp, int ncomp, int axis, int sign,
+                             cudaStream_t st) {
+  AxisDesc a;
+  a.d[0] = d0;
+  a.d[1] = d1;
+  a.d[2] = d2;
+  a.s[0] = s0;
+  a.s[1] = s1;
+  a.s[2] = s2;
+  a.scomp = scomp;
+  a.axis = axis;
+  int o1 = (axis + 1) % 3, o2 = (axis + 2) % 3;
+  if (a.s[o1] <= a.s[o2]) {
+    a.axA = o1;
+    a.axB = o2;
+  } else {
+    a.axA = o2;
+    a.axB = o1;
+  }
+  const int n = a.d[axis];
+  FftPlan p;
+  if (!make_fft_plan(n, &p)) {
+    set_error("FFT length " + std::to_string(n) + " has a prime factor above 64");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  a.sstride = pad_stride(n);
+  const size_t per = 2ull * a.sstride * sizeof(double2);
+  int lb = (a.s[axis] == 1) ? 1 : (int)std::min<size_t>(8, std::max<size_t>(1, 96 * 1024 / per));
+  lb = std::min(lb, a.d[a.axA]);
+  a.lb = lb;
+  const size_t smem = (size_t)lb * per;
+  if (smem > 220 * 1024) {
+    set_error("FFT length " + std::to_string(n) + " too long for the setup kernel");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  std::vector<double2> tw = twiddles(n);
+  double2* dtw;
+  VOX_TRY(dalloc(&dtw, n));
+  VOX_CUDA(cudaMemcpyAsync(dtw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
+  VOX_CUDA(cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+  const int tilesA = (a.d[a.axA] + lb - 1) / lb;
+  dim3 grid(tilesA * a.d[a.axB], ncomp);
+  k_fft_axis<double><<<grid, 256, smem, st>>>(a, p, dtw, sign, data);
+  VOX_CUDA(cudaGetLastError());
+  VOX_CUDA(cudaStreamSynchronize(st));
+  cudaFree(dtw);
+  return VOX_OK;
+}
+
+template <typename R>
+__global__ void k_to_prec(long long n, const double2* __restrict__ src, double s, Cx<R>* dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = from_d2<Cx<R>>(make_double2(src[i].x * s, src[i].y * s));
+}
+
+static int nblk(long long n, int t = 256) {
+  long long b = (n + t - 1) / t;
+  return (int)std::min<long long>(std::max<long long>(b, 1), 148LL * 16);
+}
+
+template <typename R>
+static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*[comp][P]*/,
+                                   const std::vector<double2>& Mr, bool has_Mr,
+                                   const std::vector<double2>& Mc, double scale) {
+  OpBuffers<R>& b = bufs<R>(op);
+  const OpGeom& g = b.geo;
+  const long long P = (long long)g.Px * g.Py * g.Pz;
+  cudaStream_t st = op->stream;
+  VOX_TRY(dalloc(&b.fN, 6 * P));
+  k_pack_fN<R><<<nblk(6 * P), 256, 0, st>>>(P, fN_packed_src, scale, b.fN);
+  VOX_CUDA(cudaGetLastError());
+  double2* tmp;
+  VOX_TRY(dalloc(&tmp, g.V));
+  if (has_Mr) {
+    VOX_TRY(dalloc(&b.Mr, g.V));
+    VOX_CUDA(cudaMemcpyAsync(tmp, Mr.data(), g.V * sizeof(double2), cudaMemcpyHostToDevice, st));
+    k_to_prec<R><<<nblk(g.V), 256, 0, st>>>(g.V, tmp, 1.0, b.Mr);
+  }
+  VOX_TRY(dalloc(&b.Mc, g.V));
+  VOX_CUDA(cudaMemcpyAsync(tmp, Mc.data(), g.V * sizeof(double2), cudaMemcpyHostToDevice, st));
+  k_to_prec<R><<<nblk(g.V), 256, 0, st>>>(g.V, tmp, 1.0, b.Mc);
+  VOX_CUDA(cudaStreamSynchronize(st));
+  cudaFree(tmp);
+  auto up_tw = [&](int n, Cx<R>** dst) -> vox_status {
+    std::vector<double2> w = twiddles(n);
+    std::vector<Cx<R>> wc(n);
+    for (int i = 0; i < n; i++) wc[i] = from_d2<Cx<R>>(w[i]);
+    VOX_TRY(dalloc(dst, n));
+    VOX_CUDA(cudaMemcpy(*dst, wc.data(), n * sizeof(Cx<R>), cudaMemcpyHostToDevice));
+    return VOX_OK;
+  };
+  VOX_TRY(up_tw(g.Px, &b.twX));
+  VOX_TRY(up_tw(g.Py, &b.twY));
+  VOX_TRY(up_tw(g.Pz, &b.twZ));
+  const long long tsz = (long long)g.Px * 3 * g.N * g.M;
+  VOX_TRY(dalloc(&b.T1, tsz));
+  VOX_TRY(dalloc(&b.T2, tsz));
+  VOX_TRY(set_smem_attrs<R>(b.geo));
+  return VOX_OK;
+}
+
+template <typename R>
+static void free_bufs(OpBuffers<R>& b) {
+  cudaFree(b.fN);
+  cudaFree(b.Mr);
+  cudaFree(b.Mc);
+  cudaFree(b.twX);
+  cudaFree(b.twY);
+  cudaFree(b.twZ);
+  cudaFree(b.T1);
+  cudaFree(b.T2);
+  b = OpBuffers<R>();
+}
+
+static void pc_release(vox_precond_s* p);
+
+static void destroy_op(vox_op_s* op) {
+  if (!op) return;
+  DeviceGuard dg(op->device);
+  cudaDeviceSynchronize();
+  // preconditioners hold the operator's index map: they go with it
+  std::vector<vox_precond_s*> pcs = op->pcs;
+  for (vox_precond_s* p : pcs) pc_release(p);
+  op->pcs.clear();
+  op->wd.release();
+  op->wf.release();
+  free_bufs(op->d);
+  free_bufs(op->f);
+  cudaFree(op->vmap);
+  if (op->h_in) cudaFreeHost(op->h_in);
+  if (op->h_out) cudaFreeHost(op->h_out);
+  cudaFree(op->d_in);
+  cudaFree(op->d_out);
+  cudaFree(op->f_in);
+  cudaFree(op->f_out);
+  cudaFree(op->x64);
+  cudaFree(op->r64);
+  cudaFree(op->b64);
+  cudaFree(op->st64);
+  if (op->own_stream) cudaStreamDestroy(op->own_stream);
+  delete op;
+}
+
+}  // namespace vox
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* vox_last_error(void) { return vox::last_error(); }
+int vox_abi_version(void) { return VOX_ABI_VERSION; }
+
+vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out) {
+  cudaGetLastError();  // drop a stale error left by an unrelated earlier call
+  if (!desc || !out) {
+    set_error("vox_op_create: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  const int L = desc->L, M = desc->M, N = desc->N;
+  if (L < 1 || M < 1 || N < 1) {
+    set_error("vox_op_create: grid dimensions must be positive");
+    return VOX_ERR_BAD_ARG;
+  }
+  if ((desc->fN_re == nullptr) == (desc->G_re == nullptr)) {
+    set_error("vox_op_create: give exactly one of fN_re or G_re");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (!desc->Mc_re || !desc->idx || desc->n_idx < 1) {
+    set_error("vox_op_create: Mc and idx are required");
+    return VOX_ERR_BAD_ARG;
+  }
+  const long long V = (long long)L * M * N;
+  if (3 * V > 2147483647LL) {
+    set_error("vox_op_create: grid too large for 32-bit index maps");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  if (desc->fN_re) {
+    if (desc->LfN < 2 * L - 1 || desc->MfN < 2 * M - 1 || desc->NfN < 2 * N - 1) {
+      set_error("vox_op_create: fN must be at least (2L-1)x(2M-1)x(2N-1)");
+      return VOX_ERR_BAD_ARG;
+    }
+    if (desc->LfN != 2 * L || desc->MfN != 2 * M || desc->NfN != 2 * N) {
+      set_error("vox_op_create: fN must be 2L x 2M x 2N (circulant_nop_const layout)");
+      return VOX_ERR_UNSUPPORTED;
+    }
+  }
+  int precs = desc->precisions ? desc->precisions : 3;
+  std::unique_ptr<vox_op_s, void (*)(vox_op_s*)> op(new vox_op_s(), destroy_op);
+  op->device = desc->device;
+  DeviceGuard dg(op->device);
+  VOX_CUDA(cudaSetDevice(op->device));
+  VOX_CUDA(cudaStreamCreateWithFlags(&op->own_stream, cudaStreamNonBlocking));
+  op->stream = op->own_stream;
+  cudaStream_t st = op->stream;
+  OpGeom& g = op->g;
+  g.L = L;
+  g.M = M;
+  g.N = N;
+  g.V = V;
+  g.n = desc->n_idx;
+  g.Px = choose_pad(L);
+  g.Py = choose_pad(M);
+  g.Pz = choose_pad(N);
+  if (!make_fft_plan(g.Px, &op->px) || !make_fft_plan(g.Py, &op->py) ||
+      !make_fft_plan(g.Pz, &op->pz)) {
+    set_error("vox_op_create: no FFT plan for the padded grid");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  op->gram = desc->gram;
+  // index map
+  {
+    std::vector<int> vmap(3 * V, -1);
+    for (long long i = 0; i < desc->n_idx; i++) {
+      const double di = desc->idx[i];
+      const long long p = (long long)di - 1;
+      if (di != std::floor(di) || p < 0 || p >= 3 * V) {
+        set_error("vox_op_create: idx[" + std::to_string(i) + "] out of range 1..3*L*M*N");
+        return VOX_ERR_BAD_ARG;
+      }
+      if (vmap[p] >= 0) {
+        set_error("vox_op_create: duplicate position in idx");
+        return VOX_ERR_BAD_ARG;
+      }
+      vmap[p] = (int)i;
+    }
+    VOX_TRY(dalloc(&op->vmap, 3 * V));
+    VOX_CUDA(cudaMemcpy(op->vmap, vmap.data(), 3 * V * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  // material arrays
+  std::vector<double2> Mr, Mc(V);
+  const bool has_Mr = desc->Mr_re != nullptr;
+  if (has_Mr) {
+    Mr.resize(V);
+    for (long long i = 0; i < V; i++)
+      Mr[i] = make_double2(desc->Mr_re[i], desc->Mr_im ? desc->Mr_im[i] : 0.0);
+  }
+  for (long long i = 0; i < V; i++)
+    Mc[i] = make_double2(desc->Mc_re[i], desc->Mc_im ? desc->Mc_im[i] : 0.0);
+  // padded circulant [comp][x'][y'][z'] in FP64, transformed
+  const long long P = (long long)g.Px * g.Py * g.Pz;
+  double2* emb;
+  VOX_TRY(dalloc(&emb, 6 * P));
+  std::unique_ptr<double2, decltype(&cudaFree)> emb_guard(emb, cudaFree);
+  if (desc->G_re) {
+    std::vector<double2> G(6 * V);
+    for (long long i = 0; i < 6 * V; i++)
+      G[i] = make_double2(desc->G_re[i], desc->G_im ? desc->G_im[i] : 0.0);
+    double2* dG;
+    VOX_TRY(dalloc(&dG, 6 * V));
+    VOX_CUDA(cudaMemcpy(dG, G.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice));
+    k_embed_from_toeplitz<<<nblk(6 * P), 256, 0, st>>>(g, dG, emb);
+    VOX_CUDA(cudaGetLastError());
+    VOX_CUDA(cudaStreamSynchronize(st));
+    cudaFree(dG);
+  } else {
+    const int L2 = 2 * L, M2 = 2 * M, N2 = 2 * N;
+    const long long Q = (long long)L2 * M2 * N2;
+    std::vector<double2> F(6 * Q);
+    for (long long i = 0; i < 6 * Q; i++)
+      F[i] = make_double2(desc->fN_re[i], desc->fN_im ? desc->fN_im[i] : 0.0);
+    double2* dF;
+    VOX_TRY(dalloc(&dF, 6 * Q));
+    std::unique_ptr<double2, decltype(&cudaFree)> dF_guard(dF, cudaFree);
+    VOX_CUDA(cudaMemcpy(dF, F.data(), 6 * Q * sizeof(double2), cudaMemcpyHostToDevice));
+    // inverse 3-D FFT (unscaled) of each component: x stride 1, y 2L, z 4LM
+    for (int ax = 0; ax < 3; ax++)
+      VOX_TRY(fft_axis_d(dF, L2, M2, N2, 1, L2, (long long)L2 * M2, Q, 6, ax, +1, st));
+    k_to_prec<double><<<nblk(6 * Q), 256, 0, st>>>(6 * Q, dF, 1.0 / (double)Q, dF);
+    k_embed_from_circ<<<nblk(6 * P), 256, 0, st>>>(g, dF, emb);
+    VOX_CUDA(cudaGetLastError());
+    VOX_CUDA(cudaStreamSynchronize(st));
+  }
+  // forward 3-D FFT of the padded circulant: z stride 1, y Pz, x Py*Pz
+  for (int ax = 0; ax < 3; ax++)
+    VOX_TRY(fft_axis_d(emb, g.Px, g.Py, g.Pz, (long long)g.Py * g.Pz, g.Pz, 1, P, 6, ax, -1, st));
+  if (precs & 1) {
+    OpGeom gd = g;
+    if (!pick_shapes(gd, sizeof(double2))) {
+      set_error("vox_op_create: grid planes too large for the complex128 kernels");
+      return VOX_ERR_UNSUPPORTED;
+    }
+    op->d.geo = gd;
+    op->d.gram = desc->gram;
+    op->d.out_scale = 1.0;
+    VOX_TRY(upload_precision<double>(op.get(), emb, Mr, has_Mr, Mc, 1.0));
+    op->has_d = true;
+  }
+  if (precs & 2) {
+    // complex64 copy of A/Gram: fN/Gram, Gram -> 1, output rescaled by Gram
+    OpGeom gf = g;
+    if (!pick_shapes(gf, sizeof(float2))) {
+      set_error("vox_op_create: grid planes too large for the complex64 kernels");
+      return VOX_ERR_UNSUPPORTED;
+    }
+    op->f.geo = gf;
+    op->f.gram = 1.0f;
+    op->f.out_scale = 1.0f;
+    VOX_TRY(upload_precision<float>(op.get(), emb, Mr, has_Mr, Mc, 1.0 / desc->gram));
+    op->has_f = true;
+  }
+  // staging for host-buffer entry points
+  const long long n = g.n;
+  VOX_CUDA(cudaMallocHost((void**)&op->h_in, n * sizeof(double2)));
+  VOX_CUDA(cudaMallocHost((void**)&op->h_out, n * sizeof(double2)));
+  VOX_TRY(dalloc(&op->d_in, n));
+  VOX_TRY(dalloc(&op->d_out, n));
+  VOX_TRY(dalloc(&op->f_in, n));
+  VOX_TRY(dalloc(&op->f_out, n));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  *out = op.release();
+  return VOX_OK;
+}
+
+void vox_op_destroy(vox_op_t op) { destroy_op(op); }
+
+vox_status vox_op_info(vox_op_t op, int* Px, int* Py, int* Pz, long long* n) {
+  if (!op) return VOX_ERR_BAD_ARG;
+  if (Px) *Px = op->g.Px;
+  if (Py) *Py = op->g.Py;
+  if (Pz) *Pz = op->g.Pz;
+  if (n) *n = op->g.n;
+  return VOX_OK;
+}
+
+}  // extern "C"
+
+namespace vox {
+
+template <typename R>
+__global__ void k_from_d2(long long n, const double2* __restrict__ a, Cx<R>* b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = from_d2<Cx<R>>(a[i]);
+}
+template <typename R>
+__global__ void k_to_d2(long long n, const Cx<R>* __restrict__ a, double scale, double2* b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double2 v = to_d2(a[i]);
+    b[i] = make_double2(v.x * scale, v.y * scale);
+  }
+}
+
+static void split_to_d2(const double* re, const double* im, long long n, double2* dst) {
+  for (long long i = 0; i < n; i++) dst[i] = make_double2(re[i], im ? im[i] : 0.0);
+}
+static void d2_to_split(const double2* src, long long n, double* re, double* im) {
+  for (long long i = 0; i < n; i++) {
+    re[i] = src[i].x;
+    if (im) im[i] = src[i].y;
+  }
+}
+
+static vox_status check_prec(vox_op_s* op, vox_prec prec) {
+  if (prec == VOX_C128 && !op->has_d) {
+    set_error("operator has no complex128 copy");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (prec == VOX_C64 && !op->has_f) {
+    set_error("operator has no complex64 copy");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (prec != VOX_C128 && prec != VOX_C64) {
+    set_error("unknown precision");
+    return VOX_ERR_BAD_ARG;
+  }
+  return VOX_OK;
+}
+
+// Host-buffer matvec through the staging buffers.
+static vox_status mv_host(vox_op_s* op, int mode, vox_prec prec, const double* in_re,
+                          const double* in_im, double* out_re, double* out_im) {
+  if (!op || !in_re || !out_re) {
+    set_error("NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  VOX_TRY(check_prec(op, prec));
+  DeviceGuard dg(op->device);
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  split_to_d2(in_re, in_im, n, op->h_in);
+  VOX_CUDA(cudaMemcpyAsync(op->d_in, op->h_in, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+  if (prec == VOX_C128) {
+    VOX_TRY(matvec<double>(op, mode, op->d_in, op->d_out, st, nullptr));
+  } else {
+    k_from_d2<float><<<nblk(n), 256, 0, st>>>(n, op->d_in, op->f_in);
+    VOX_TRY(matvec<float>(op, mode, op->f_in, op->f_out, st, nullptr));
+    // the complex64 copy computes A x / Gram for MV_AN (and (N-Gram)x/Gram for MV_L)
+    k_to_d2<float><<<nblk(n), 256, 0, st>>>(n, op->f_out, op->gram, op->d_out);
+  }
+  VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  d2_to_split(op->h_out, n, out_re, out_im);
+  return VOX_OK;
+}
+
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_mv_AN(vox_op_t op, int transp, vox_prec prec, const double* in_re,
+                     const double* in_im, double* out_re, double* out_im) {
+  return mv_host(op, transp ? MV_AN_T : MV_AN, prec, in_re, in_im, out_re, out_im);
+}
+
+vox_status vox_mv_L(vox_op_t op, vox_prec prec, const double* in_re, const double* in_im,
+                    double* out_re, double* out_im) {
+  return mv_host(op, MV_L, prec, in_re, in_im, out_re, out_im);
+}
+
+vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* in, void* out,
+                            void* stream) {
+  if (!op || !in || !out) {
+    set_error("NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  VOX_TRY(check_prec(op, prec));
+  DeviceGuard dg(op->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : op->stream;
+  const int mode = transp ? MV_AN_T : MV_AN;
+  if (prec == VOX_C128)
+    return matvec<double>(op, mode, (const double2*)in, (double2*)out, st, nullptr);
+  return matvec<float>(op, mode, (const float2*)in, (float2*)out, st, nullptr);
+}
+
+}  // extern "C"
+
+#include "solver.cuh"

@@ -1,0 +1,419 @@
+// Device-resident restarted GMRES (pgmres.m:70-181, pgmres_iter.m:22-150).
+//
+// Arnoldi uses classical Gram-Schmidt with one re-orthogonalisation pass
+// (CGS2).  Inner products and norms accumulate in FP64 whatever the working
+// precision R of the basis; the Hessenberg matrix, the Givens rotations and
+// the least-squares solve live on the device in FP64.  Each kernel begins by
+// reading the cycle's `done` flag, so a whole restart cycle (m iterations plus
+// the solution update) is enqueued - and captured in one CUDA graph - without
+// any host round trip; the host syncs once per cycle.
+//
+// Reductions are deterministic: every CTA writes its partial sums, and the
+// last CTA to finish (atomic ticket) adds them in block order.
+#pragma once
+
+#include "vox_common.cuh"
+
+namespace vox {
+
+constexpr int kMaxRestart = 128;
+constexpr int kRedBlocks = 296;  // 2 CTAs per SM on 148 SMs
+constexpr int kRedThreads = 256;
+
+struct GmresDev {
+  int done;          // cycle finished (converged / breakdown / m reached)
+  int k;             // iterations performed in this cycle
+  int converged;     // LS residual below tol_abs
+  int breakdown;     // H(k+1,k) == 0
+  unsigned ticket;   // last-block counter
+  int m;             // restart length
+  double tol_abs;    // tol * bnorm
+  double beta;       // ||r|| at cycle start
+  double inv_norm;   // 1/H(k+1,k) for the pending basis vector
+  double resvec[kMaxRestart];
+  double cs[kMaxRestart];
+  double2 sn[kMaxRestart];
+  double2 g[kMaxRestart + 1];
+  double2 y[kMaxRestart];
+  double2 res[kMaxRestart + 1];
+  double2 h1[kMaxRestart + 1];
+  double2 h2[kMaxRestart + 1];
+  double2 H[(kMaxRestart + 1) * kMaxRestart];   // unrotated, column-major, ld m+1
+  double2 Rm[(kMaxRestart + 1) * kMaxRestart];  // rotated (upper triangular part used)
+  double2 partial[(kMaxRestart + 1) * kRedBlocks];
+  double scal[4];    // misc reductions (norms)
+};
+
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+// Block-wide sum of one double2 per thread; result valid in thread 0.
+__device__ __forceinline__ double2 block_sum(double2 v, double2* sh) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    v = (lane < nw) ? sh[lane] : make_double2(0.0, 0.0);
+    v = warp_sum(v);
+  }
+  return v;
+}
+
+// Returns true in exactly one CTA (the last to arrive), after all partials
+// of all CTAs are visible.
+__device__ __forceinline__ bool last_block(unsigned* ticket) {
+  __shared__ bool amlast;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(ticket, 1u);
+    amlast = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (amlast) __threadfence();
+  return amlast;
+}
+
+// partial[j*nb + b] for j < nj, reduced in block order into out[j].
+__device__ __forceinline__ void reduce_partials(const double2* partial, int nj, int nb,
+                                                double2* out, double2* sh) {
+  for (int j = 0; j < nj; j++) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      v.x += partial[j * nb + b].x;
+      v.y += partial[j * nb + b].y;
+    }
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) out[j] = v;
+    __syncthreads();
+  }
+}
+
+// Per-CTA dot products of nj basis vectors with w over the CTA's grid-stride
+// elements: 4 basis vectors per sweep.
+template <typename R>
+__device__ __forceinline__ void cta_dots(const Cx<R>* __restrict__ V, long long ldv, int nj,
+                                         const Cx<R>* __restrict__ w, long long n,
+                                         double2* partial, double2* sh) {
+  for (int j0 = 0; j0 < nj; j0 += 4) {
+    double2 acc[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
+                      make_double2(0, 0)};
+    const int nb = min(4, nj - j0);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+      const double2 wi = to_d2(w[i]);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (q < nb) {
+          const double2 v = to_d2(V[(j0 + q) * ldv + i]);
+          acc[q].x += v.x * wi.x + v.y * wi.y;  // conj(v) * w
+          acc[q].y += v.x * wi.y - v.y * wi.x;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if (q < nb) {
+        const double2 s = block_sum(acc[q], sh);
+        if (threadIdx.x == 0) partial[(j0 + q) * gridDim.x + blockIdx.x] = s;
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// h1 = V(:,0..k)^H w ; H(:,k) = h1
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads) k_gs_dots(GmresDev* st, int k,
+                                                         const Cx<R>* __restrict__ V,
+                                                         long long ldv, const Cx<R>* __restrict__ w,
+                                                         long long n) {
+  __shared__ double2 sh[32];
+  if (st->done) return;
+  cta_dots<R>(V, ldv, k + 1, w, n, st->partial, sh);
+  if (last_block(&st->ticket)) {
+    reduce_partials(st->partial, k + 1, gridDim.x, st->h1, sh);
+    if (threadIdx.x == 0) st->ticket = 0;
+  }
+}
+
+// w <- w - V h_in ; then partial dots of V^H w (second CGS pass)
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads) k_gs_update_dots(GmresDev* st, int k,
+                                                                const Cx<R>* __restrict__ V,
+                                                                long long ldv, Cx<R>* w,
+                                                                long long n) {
+  __shared__ double2 sh[32];
+  __shared__ Cx<R> hs[kMaxRestart + 1];
+  if (st->done) return;
+  const int nj = k + 1;
+  for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<Cx<R>>(st->h1[j]);
+  __syncthreads();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Cx<R> wi = w[i];
+    for (int j = 0; j < nj; j++) {
+      const Cx<R> v = V[j * ldv + i];
+      const Cx<R> h = hs[j];
+      wi.x -= v.x * h.x - v.y * h.y;
+      wi.y -= v.x * h.y + v.y * h.x;
+    }
+    w[i] = wi;
+  }
+  __syncthreads();
+  cta_dots<R>(V, ldv, nj, w, n, st->partial, sh);
+  if (last_block(&st->ticket)) {
+    reduce_partials(st->partial, nj, gridDim.x, st->h2, sh);
+    if (threadIdx.x == 0) st->ticket = 0;
+  }
+}
+
+// Complex Givens rotation zeroing b in (a, b).
+__device__ __forceinline__ void givens(double2 a, double2 b, double* c, double2* s, double2* r) {
+  const double ab = hypot(b.x, b.y);
+  const double aa = hypot(a.x, a.y);
+  if (ab == 0.0) {
+    *c = 1.0;
+    *s = make_double2(0.0, 0.0);
+    *r = a;
+    return;
+  }
+  if (aa == 0.0) {
+    *c = 0.0;
+    *s = make_double2(b.x / ab, -b.y / ab);  // conj(b)/|b|
+    *r = make_double2(ab, 0.0);
+    return;
+  }
+  const double nrm = hypot(aa, ab);
+  const double2 ph = make_double2(a.x / aa, a.y / aa);
+  *c = aa / nrm;
+  // s = ph * conj(b) / nrm
+  *s = make_double2((ph.x * b.x + ph.y * b.y) / nrm, (ph.y * b.x - ph.x * b.y) / nrm);
+  *r = make_double2(ph.x * nrm, ph.y * nrm);
+}
+
+// w <- w - V h2 ; ||w||^2 ; last block: Hessenberg column, Givens, residual.
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, int k,
+                                                                const Cx<R>* __restrict__ V,
+                                                                long long ldv, Cx<R>* w,
+                                                                long long n) {
+  __shared__ double2 sh[32];
+  __shared__ Cx<R> hs[kMaxRestart + 1];
+  if (st->done) return;
+  const int nj = k + 1;
+  for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<Cx<R>>(st->h2[j]);
+  __syncthreads();
+  double2 acc = make_double2(0.0, 0.0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Cx<R> wi = w[i];
+    for (int j = 0; j < nj; j++) {
+      const Cx<R> v = V[j * ldv + i];
+      const Cx<R> h = hs[j];
+      wi.x -= v.x * h.x - v.y * h.y;
+      wi.y -= v.x * h.y + v.y * h.x;
+    }
+    w[i] = wi;
+    acc.x += (double)wi.x * wi.x + (double)wi.y * wi.y;
+  }
+  const double2 s = block_sum(acc, sh);
+  if (threadIdx.x == 0) st->partial[blockIdx.x] = s;
+  if (last_block(&st->ticket)) {
+    double2 tot[1];
+    reduce_partials(st->partial, 1, gridDim.x, tot, sh);
+    if (threadIdx.x == 0) {
+      st->ticket = 0;
+      const int m = st->m;
+      const int ld = m + 1;
+      const double nrm = sqrt(tot[0].x);
+      double2* Hc = st->H + (size_t)k * ld;
+      double2* Rc = st->Rm + (size_t)k * ld;
+      for (int j = 0; j <= k; j++) {
+        Hc[j] = make_double2(st->h1[j].x + st->h2[j].x, st->h1[j].y + st->h2[j].y);
+        Rc[j] = Hc[j];
+      }
+      Hc[k + 1] = make_double2(nrm, 0.0);
+      Rc[k + 1] = Hc[k + 1];
+      // apply previous rotations
+      for (int i = 0; i < k; i++) {
+        const double c = st->cs[i];
+        const double2 sv = st->sn[i];
+        const double2 a = Rc[i], b = Rc[i + 1];
+        // a' = c a + s b ; b' = -conj(s) a + c b
+        Rc[i] = make_double2(c * a.x + sv.x * b.x - sv.y * b.y, c * a.y + sv.x * b.y + sv.y * b.x);
+        Rc[i + 1] = make_double2(-(sv.x * a.x + sv.y * a.y) + c * b.x,
+                                 -(sv.x * a.y - sv.y * a.x) + c * b.y);
+      }
+      double c;
+      double2 sv, r;
+      givens(Rc[k], Rc[k + 1], &c, &sv, &r);
+      st->cs[k] = c;
+      st->sn[k] = sv;
+      Rc[k] = r;
+      Rc[k + 1] = make_double2(0.0, 0.0);
+      const double2 gk = st->g[k];
+      st->g[k] = make_double2(c * gk.x, c * gk.y);
+      // g(k+1) = -conj(s) g(k)
+      st->g[k + 1] = make_double2(-(sv.x * gk.x + sv.y * gk.y), -(sv.x * gk.y - sv.y * gk.x));
+      const double resid = hypot(st->g[k + 1].x, st->g[k + 1].y);
+      st->resvec[k] = resid;
+      st->k = k + 1;
+      st->inv_norm = (nrm > 0.0) ? 1.0 / nrm : 0.0;
+      if (resid < st->tol_abs) st->converged = 1;
+      if (nrm == 0.0) st->breakdown = 1;
+      if (st->converged || st->breakdown || k + 1 >= m) st->done = 1;
+    }
+  }
+}
+
+// V(:,k+1) = w * inv_norm
+template <typename R>
+__global__ void k_gs_scale(GmresDev* st, Cx<R>* __restrict__ Vnext, const Cx<R>* __restrict__ w,
+                           long long n) {
+  if (st->done) return;
+  const R s = (R)st->inv_norm;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Vnext[i] = cscale(w[i], s);
+  }
+}
+
+// ||x||^2 -> st->scal[slot] (deterministic, grid = kRedBlocks)
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads) k_norm2(GmresDev* st, const Cx<R>* __restrict__ x,
+                                                       long long n, int slot) {
+  __shared__ double2 sh[32];
+  double2 acc = make_double2(0.0, 0.0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = to_d2(x[i]);
+    acc.x += v.x * v.x + v.y * v.y;
+  }
+  const double2 s = block_sum(acc, sh);
+  if (threadIdx.x == 0) st->partial[blockIdx.x] = s;
+  if (last_block(&st->ticket)) {
+    double2 tot[1];
+    reduce_partials(st->partial, 1, gridDim.x, tot, sh);
+    if (threadIdx.x == 0) {
+      st->ticket = 0;
+      st->scal[slot] = tot[0].x;
+    }
+  }
+}
+
+// Start a cycle: beta = sqrt(scal[0]); V(:,0) = r / beta; g = beta e1.
+__global__ void k_cycle_init(GmresDev* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    st->beta = sqrt(st->scal[0]);
+    st->inv_norm = st->beta > 0.0 ? 1.0 / st->beta : 0.0;
+    st->done = 0;
+    st->k = 0;
+    st->converged = 0;
+    st->breakdown = 0;
+    for (int i = 0; i <= st->m; i++) st->g[i] = make_double2(0.0, 0.0);
+    st->g[0] = make_double2(st->beta, 0.0);
+  }
+}
+
+template <typename R>
+__global__ void k_cycle_v0(const GmresDev* st, Cx<R>* __restrict__ V0, const Cx<R>* __restrict__ r,
+                           long long n) {
+  const R s = (R)st->inv_norm;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    V0[i] = cscale(r[i], s);
+  }
+}
+
+// Least squares after the cycle: y = Rm(0:kk-1,0:kk-1) \ g(0:kk-1) (back
+// substitution), res = beta e1 - H(0:kk,0:kk-1) y  (pgmres_iter.m:117-119).
+__global__ void k_cycle_ls(GmresDev* st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int kk = st->k;
+  const int ld = st->m + 1;
+  for (int i = kk - 1; i >= 0; i--) {
+    double2 s = st->g[i];
+    for (int j = i + 1; j < kk; j++) {
+      const double2 a = st->Rm[(size_t)j * ld + i];
+      const double2 yj = st->y[j];
+      s.x -= a.x * yj.x - a.y * yj.y;
+      s.y -= a.x * yj.y + a.y * yj.x;
+    }
+    const double2 d = st->Rm[(size_t)i * ld + i];
+    const double dd = d.x * d.x + d.y * d.y;
+    st->y[i] = dd > 0.0 ? make_double2((s.x * d.x + s.y * d.y) / dd, (s.y * d.x - s.x * d.y) / dd)
+                        : make_double2(0.0, 0.0);
+  }
+  for (int i = 0; i <= kk; i++) {
+    double2 s = make_double2(i == 0 ? st->beta : 0.0, 0.0);
+    for (int j = 0; j < kk; j++) {
+      const double2 a = st->H[(size_t)j * ld + i];
+      const double2 yj = st->y[j];
+      s.x -= a.x * yj.x - a.y * yj.y;
+      s.y -= a.x * yj.y + a.y * yj.x;
+    }
+    st->res[i] = s;
+  }
+}
+
+// x += V(:,0:kk-1) y ; r = V(:,0:kk) res   (pgmres_iter.m:133-150, no right preconditioner)
+template <typename R>
+__global__ void k_cycle_update(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
+                               Cx<R>* x, Cx<R>* r, long long n) {
+  __shared__ Cx<R> ys[kMaxRestart];
+  __shared__ Cx<R> rs[kMaxRestart + 1];
+  const int kk = st->k;
+  for (int j = threadIdx.x; j <= kk; j += blockDim.x) {
+    if (j < kk) ys[j] = from_d2<Cx<R>>(st->y[j]);
+    rs[j] = from_d2<Cx<R>>(st->res[j]);
+  }
+  __syncthreads();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Cx<R> xi = x ? x[i] : czero<Cx<R>>();
+    Cx<R> ri = czero<Cx<R>>();
+    for (int j = 0; j <= kk; j++) {
+      const Cx<R> v = V[j * ldv + i];
+      if (j < kk) cfma(xi, v, ys[j]);
+      cfma(ri, v, rs[j]);
+    }
+    if (x) x[i] = xi;
+    r[i] = ri;
+  }
+}
+
+// y = V(:,0:kk-1) * ys (for the right-preconditioned update, into a temp)
+template <typename R>
+__global__ void k_cycle_vy(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
+                           Cx<R>* out, long long n) {
+  __shared__ Cx<R> ys[kMaxRestart];
+  const int kk = st->k;
+  for (int j = threadIdx.x; j < kk; j += blockDim.x) ys[j] = from_d2<Cx<R>>(st->y[j]);
+  __syncthreads();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Cx<R> acc = czero<Cx<R>>();
+    for (int j = 0; j < kk; j++) cfma(acc, V[j * ldv + i], ys[j]);
+    out[i] = acc;
+  }
+}
+
+// elementwise helpers
+template <typename R>
+__global__ void k_axpy(Cx<R>* y, const Cx<R>* __restrict__ x, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = cadd(y[i], x[i]);
+}
+
+}  // namespace vox

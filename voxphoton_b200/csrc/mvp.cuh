@@ -1,0 +1,393 @@
+// FFT-circulant matvec of the JVIE-II operator, fused into three kernels.
+//
+//   y = Gram*Mr.*J - Mc.*crop(ifftn(sum_k fN_ck .* fftn(pad(J_k))))      (mv_AN_const.m:102-134)
+//
+// Layouts in HBM (all interleaved complex, R = float or double):
+//   vector  : the unknowns at the support positions idx (length n), as in MATLAB JIn0
+//   vmap    : int32 [3][N][M][L] (column-major grid, x fastest) -> vector slot or -1
+//   T1, T2  : [Px][3][N][M]  one contiguous "plane" of 3*M*N values per x-frequency
+//   fN      : [Px][Py][Pz][6] the six unique tensor components of each padded cell
+// Px, Py, Pz are the padded lengths (>= 2L-1, 2M-1, 2N-1, 7-smooth), chosen at
+// operator creation; the circulant embedding is exact for any such length.
+//
+// Kernel 1 (k_xfwd):  per (z,c) and a tile of y: gather J pencils along x,
+//                     zero-pad to Px, forward FFT along x, write T1 planes.
+// Kernel 2 (k_plane): per kx plane: y-FFT (padded to Py) of the 3N rows, then for
+//                     chunks of ky: z-FFT (padded to Pz), 3x3 symmetric tensor
+//                     product with fN, inverse z-FFT cropped to N, then inverse
+//                     y-FFT cropped to M; write T2.
+// Kernel 3 (k_xinv):  per (z,c) and a tile of y: inverse x-FFT cropped to L,
+//                     1/P scaling, contrast Gram*Mr*J - Mc*(.), scatter to the
+//                     output vector.
+#pragma once
+
+#include "fft.cuh"
+
+namespace vox {
+
+struct OpGeom {
+  int L, M, N;
+  int Px, Py, Pz;
+  long long V;    // L*M*N
+  long long n;    // vector length
+  // launch shapes (chosen on the host)
+  int ybx;        // pencils per CTA in kernels 1/3
+  int sx;         // smem stride of an x pencil
+  int sy, sz;     // smem strides of y rows / z columns in kernel 2
+  int rc, kc;     // rows per chunk / ky columns per chunk in kernel 2
+};
+
+enum MvMode { MV_AN = 0, MV_AN_T = 1, MV_L = 2 };
+
+template <typename R>
+struct OpBuffers {
+  Cx<R>* fN = nullptr;   // [Px][Py][Pz][6]
+  Cx<R>* Mr = nullptr;   // V, nullptr when Mr == 1 everywhere
+  Cx<R>* Mc = nullptr;   // V
+  Cx<R>* twX = nullptr;  // Px
+  Cx<R>* twY = nullptr;  // Py
+  Cx<R>* twZ = nullptr;  // Pz
+  Cx<R>* T1 = nullptr;
+  Cx<R>* T2 = nullptr;
+  OpGeom geo{};          // sizes and launch shapes for this precision
+  R gram = 0;            // Gram in this precision's units
+  R out_scale = 1;       // multiplies the matvec output (1 or Gram for the scaled c64 copy)
+};
+
+inline int pad_stride(int n) { return (n % 2 == 0) ? n + 1 : n; }
+
+// ---------------------------------------------------------------- kernel 1
+template <typename R>
+__global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>* __restrict__ tw,
+                                              const Cx<R>* __restrict__ in,
+                                              const int* __restrict__ vmap,
+                                              const Cx<R>* __restrict__ Mc, int mode,
+                                              Cx<R>* __restrict__ T1, const int* skip) {
+  using C = Cx<R>;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + (size_t)g.ybx * g.sx;
+  const int y0 = blockIdx.x * g.ybx;
+  const int z = blockIdx.y;
+  const int c = blockIdx.z;
+  const int YB = g.ybx;
+  const long long cellbase = (long long)g.L * ((long long)g.M * z);
+  // gather J along x for YB pencils; zero-pad
+  for (int t = threadIdx.x; t < YB * g.Px; t += blockDim.x) {
+    const int yb = t / g.Px;
+    const int x = t - yb * g.Px;
+    const int y = y0 + yb;
+    C v = czero<C>();
+    if (x < g.L && y < g.M) {
+      const long long cell = cellbase + (long long)g.L * y + x;
+      const int m = vmap[(long long)c * g.V + cell];
+      if (m >= 0) {
+        v = in[m];
+        if (mode == MV_AN_T) v = cmul(Mc[cell], cconj(v));  // conj(conj(Mc) .* J)
+      }
+    }
+    bufA[(size_t)yb * g.sx + x] = v;
+  }
+  __syncthreads();
+  C* res = block_fft(bufA, bufB, px, YB, g.sx, tw, -1);
+  // write planes: T1[kx][c][z][y]
+  const int ny = min(YB, g.M - y0);
+  for (int t = threadIdx.x; t < YB * g.Px; t += blockDim.x) {
+    const int kx = t / YB;
+    const int yb = t - kx * YB;
+    if (yb < ny) {
+      T1[(((long long)kx * 3 + c) * g.N + z) * g.M + y0 + yb] = res[(size_t)yb * g.sx + kx];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- kernel 2
+template <typename R>
+__global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
+                                               const Cx<R>* __restrict__ twY,
+                                               const Cx<R>* __restrict__ twZ,
+                                               const Cx<R>* __restrict__ T1,
+                                               const Cx<R>* __restrict__ fN,
+                                               Cx<R>* __restrict__ T2, const int* skip) {
+  using C = Cx<R>;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int rows = 3 * g.N;
+  C* ybuf = reinterpret_cast<C*>(smem_raw);          // [3N][sy]
+  C* wA = ybuf + (size_t)rows * g.sy;
+  const int wsize = max(g.rc * g.sy, 3 * g.kc * g.sz);
+  C* wB = wA + wsize;
+  const int kx = blockIdx.x;
+  const C* tin = T1 + (long long)kx * rows * g.M;
+  C* tout = T2 + (long long)kx * rows * g.M;
+
+  // Phase A: forward y-FFT of all 3N rows
+  for (int r0 = 0; r0 < rows; r0 += g.rc) {
+    const int nr = min(g.rc, rows - r0);
+    for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
+      const int r = t / g.Py;
+      const int y = t - r * g.Py;
+      wA[(size_t)r * g.sy + y] = (y < g.M) ? tin[(long long)(r0 + r) * g.M + y] : czero<C>();
+    }
+    __syncthreads();
+    C* res = block_fft(wA, wB, py, nr, g.sy, twY, -1);
+    for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
+      const int r = t / g.Py;
+      const int y = t - r * g.Py;
+      ybuf[(size_t)(r0 + r) * g.sy + y] = res[(size_t)r * g.sy + y];
+    }
+    __syncthreads();
+  }
+
+  // Phase B: per ky chunk, z-FFT, tensor product, inverse z-FFT (crop to N)
+  const C* fplane = fN + (long long)kx * g.Py * g.Pz * 6;
+  for (int k0 = 0; k0 < g.Py; k0 += g.kc) {
+    const int nk = min(g.kc, g.Py - k0);
+    // gather columns: seq (c*nk + j), element z
+    for (int t = threadIdx.x; t < 3 * nk * g.Pz; t += blockDim.x) {
+      const int s = t / g.Pz;
+      const int zz = t - s * g.Pz;
+      const int c = s / nk;
+      const int j = s - c * nk;
+      wA[(size_t)s * g.sz + zz] =
+          (zz < g.N) ? ybuf[(size_t)(c * g.N + zz) * g.sy + k0 + j] : czero<C>();
+    }
+    __syncthreads();
+    C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, twZ, -1);
+    // tensor product (in place in res)
+    for (int t = threadIdx.x; t < nk * g.Pz; t += blockDim.x) {
+      const int j = t / g.Pz;
+      const int kz = t - j * g.Pz;
+      const C* f = fplane + ((long long)(k0 + j) * g.Pz + kz) * 6;
+      const C f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3], f4 = f[4], f5 = f[5];
+      C* p0 = res + (size_t)(0 * nk + j) * g.sz + kz;
+      C* p1 = res + (size_t)(1 * nk + j) * g.sz + kz;
+      C* p2 = res + (size_t)(2 * nk + j) * g.sz + kz;
+      const C a = *p0, b = *p1, cc = *p2;
+      C o0 = cmul(f0, a), o1 = cmul(f1, a), o2 = cmul(f2, a);
+      cfma(o0, f1, b);
+      cfma(o1, f3, b);
+      cfma(o2, f4, b);
+      cfma(o0, f2, cc);
+      cfma(o1, f4, cc);
+      cfma(o2, f5, cc);
+      *p0 = o0;
+      *p1 = o1;
+      *p2 = o2;
+    }
+    __syncthreads();
+    C* other = (res == wA) ? wB : wA;
+    C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, twZ, +1);
+    for (int t = threadIdx.x; t < 3 * nk * g.N; t += blockDim.x) {
+      const int s = t / g.N;
+      const int zz = t - s * g.N;
+      const int c = s / nk;
+      const int j = s - c * nk;
+      ybuf[(size_t)(c * g.N + zz) * g.sy + k0 + j] = res2[(size_t)s * g.sz + zz];
+    }
+    __syncthreads();
+  }
+
+  // Phase C: inverse y-FFT of the 3N rows, crop to M, write T2
+  for (int r0 = 0; r0 < rows; r0 += g.rc) {
+    const int nr = min(g.rc, rows - r0);
+    for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
+      const int r = t / g.Py;
+      const int y = t - r * g.Py;
+      wA[(size_t)r * g.sy + y] = ybuf[(size_t)(r0 + r) * g.sy + y];
+    }
+    __syncthreads();
+    C* res = block_fft(wA, wB, py, nr, g.sy, twY, +1);
+    for (int t = threadIdx.x; t < nr * g.M; t += blockDim.x) {
+      const int r = t / g.M;
+      const int y = t - r * g.M;
+      tout[(long long)(r0 + r) * g.M + y] = res[(size_t)r * g.sy + y];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- kernel 3
+template <typename R>
+__global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>* __restrict__ tw,
+                                              const Cx<R>* __restrict__ T2,
+                                              const int* __restrict__ vmap,
+                                              const Cx<R>* in, const Cx<R>* __restrict__ Mr,
+                                              const Cx<R>* __restrict__ Mc, R gram, R scale,
+                                              R out_scale, int mode, Cx<R>* out,
+                                              const int* skip) {
+  using C = Cx<R>;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + (size_t)g.ybx * g.sx;
+  const int y0 = blockIdx.x * g.ybx;
+  const int z = blockIdx.y;
+  const int c = blockIdx.z;
+  const int YB = g.ybx;
+  const int ny = min(YB, g.M - y0);
+  for (int t = threadIdx.x; t < YB * g.Px; t += blockDim.x) {
+    const int kx = t / YB;
+    const int yb = t - kx * YB;
+    bufA[(size_t)yb * g.sx + kx] =
+        (yb < ny) ? T2[(((long long)kx * 3 + c) * g.N + z) * g.M + y0 + yb] : czero<C>();
+  }
+  __syncthreads();
+  C* res = block_fft(bufA, bufB, px, YB, g.sx, tw, +1);
+  const long long cellbase = (long long)g.L * ((long long)g.M * z);
+  for (int t = threadIdx.x; t < YB * g.L; t += blockDim.x) {
+    const int yb = t / g.L;
+    const int x = t - yb * g.L;
+    if (yb >= ny) continue;
+    const long long cell = cellbase + (long long)g.L * (y0 + yb) + x;
+    const int m = vmap[(long long)c * g.V + cell];
+    if (m < 0) continue;
+    const C nj = cscale(res[(size_t)yb * g.sx + x], scale);
+    const C J = in[m];
+    C o;
+    if (mode == MV_AN) {
+      C a = cscale(J, gram);
+      if (Mr) a = cmul(Mr[cell], a);
+      o = csub(a, cmul(Mc[cell], nj));
+    } else if (mode == MV_AN_T) {
+      C a = cscale(J, gram);
+      if (Mr) a = cmul(cconj(Mr[cell]), a);
+      o = csub(a, cconj(nj));
+    } else {
+      o = csub(nj, cscale(J, gram));
+    }
+    out[m] = cscale(o, out_scale);
+  }
+}
+
+// ------------------------------------------------------------ setup kernels
+// Batched 1-D FFT of lines of a 3-D array (element (i0,i1,i2) at
+// i0*s0 + i1*s1 + i2*s2 + comp*scomp) along `axis`; `lb` adjacent lines (in the
+// other axis with the smaller stride, `axA`) per CTA for coalescing.
+struct AxisDesc {
+  int d[3];
+  long long s[3];
+  long long scomp;
+  int axis, axA, axB;
+  int lb;
+  int sstride;
+};
+
+template <typename R>
+__global__ void k_fft_axis(AxisDesc a, FftPlan p, const Cx<R>* __restrict__ tw, int sign,
+                           Cx<R>* data) {
+  using C = Cx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + (size_t)a.lb * a.sstride;
+  const int nA = a.d[a.axA];
+  const int tilesA = (nA + a.lb - 1) / a.lb;
+  const int ia0 = (blockIdx.x % tilesA) * a.lb;
+  const int ib = blockIdx.x / tilesA;
+  const int comp = blockIdx.y;
+  const int n = a.d[a.axis];
+  const int nl = min(a.lb, nA - ia0);
+  C* base = data + comp * a.scomp + (long long)ib * a.s[a.axB] + (long long)ia0 * a.s[a.axA];
+  for (int t = threadIdx.x; t < nl * n; t += blockDim.x) {
+    const int i = t / nl;
+    const int l = t - i * nl;
+    bufA[(size_t)l * a.sstride + i] = base[(long long)l * a.s[a.axA] + (long long)i * a.s[a.axis]];
+  }
+  __syncthreads();
+  C* res = block_fft(bufA, bufB, p, nl, a.sstride, tw, sign);
+  for (int t = threadIdx.x; t < nl * n; t += blockDim.x) {
+    const int i = t / nl;
+    const int l = t - i * nl;
+    base[(long long)l * a.s[a.axA] + (long long)i * a.s[a.axis]] = res[(size_t)l * a.sstride + i];
+  }
+}
+
+// Map a padded coordinate x' of the new grid (length P) to the offset d in
+// (-n, n) it represents and from there to the coordinate of the source grid of
+// length Q (Q = 2n for the MATLAB embedding, or n for a Toeplitz source with
+// sign flips).  Returns -1 for the zero band.
+__device__ __forceinline__ int embed_offset(int xp, int P, int n) {
+  if (xp < n) return xp;
+  if (xp > P - n) return xp - P;  // negative offset
+  return INT_MIN;
+}
+
+// Build the padded circulant from the MATLAB-layout circulant Gp(2L,2M,2N,6)
+// (column-major, already inverse-transformed): fill [comp][x'][y'][z'] (z fastest).
+__global__ void k_embed_from_circ(OpGeom g, const double2* __restrict__ Gp, double2* out) {
+  const long long P = (long long)g.Px * g.Py * g.Pz;
+  const int L2 = 2 * g.L, M2 = 2 * g.M, N2 = 2 * g.N;
+  const long long Q = (long long)L2 * M2 * N2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6 * P;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int comp = (int)(t / P);
+    long long r = t - comp * P;
+    const int zp = (int)(r % g.Pz);
+    r /= g.Pz;
+    const int yp = (int)(r % g.Py);
+    const int xp = (int)(r / g.Py);
+    const int dx = embed_offset(xp, g.Px, g.L);
+    const int dy = embed_offset(yp, g.Py, g.M);
+    const int dz = embed_offset(zp, g.Pz, g.N);
+    double2 v = make_double2(0.0, 0.0);
+    if (dx != INT_MIN && dy != INT_MIN && dz != INT_MIN) {
+      const int sx = (dx + L2) % L2, sy = (dy + M2) % M2, sz = (dz + N2) % N2;
+      v = Gp[comp * Q + sx + (long long)L2 * (sy + (long long)M2 * sz)];
+    }
+    out[t] = v;
+  }
+}
+
+// Build the padded circulant directly from the Toeplitz G_mn(L,M,N,6)
+// (column-major), mirroring with the per-axis parity of each component
+// (gperiodic_coeff_nop.m:4-31: 'L' [+ - - + + +], 'M' [+ - + + - +], 'N' [+ + - + - +];
+// the two- and three-axis octants take the products of these signs).
+__global__ void k_embed_from_toeplitz(OpGeom g, const double2* __restrict__ G, double2* out) {
+  const long long P = (long long)g.Px * g.Py * g.Pz;
+  const long long V = g.V;
+  const int sL[6] = {1, -1, -1, 1, 1, 1};
+  const int sM[6] = {1, -1, 1, 1, -1, 1};
+  const int sN[6] = {1, 1, -1, 1, -1, 1};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6 * P;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int comp = (int)(t / P);
+    long long r = t - comp * P;
+    const int zp = (int)(r % g.Pz);
+    r /= g.Pz;
+    const int yp = (int)(r % g.Py);
+    const int xp = (int)(r / g.Py);
+    const int dx = embed_offset(xp, g.Px, g.L);
+    const int dy = embed_offset(yp, g.Py, g.M);
+    const int dz = embed_offset(zp, g.Pz, g.N);
+    double2 v = make_double2(0.0, 0.0);
+    if (dx != INT_MIN && dy != INT_MIN && dz != INT_MIN) {
+      int s = 1;
+      if (dx < 0) s *= sL[comp];
+      if (dy < 0) s *= sM[comp];
+      if (dz < 0) s *= sN[comp];
+      const int ax = dx < 0 ? -dx : dx, ay = dy < 0 ? -dy : dy, az = dz < 0 ? -dz : dz;
+      v = G[comp * V + ax + (long long)g.L * (ay + (long long)g.M * az)];
+      v.x *= s;
+      v.y *= s;
+    }
+    out[t] = v;
+  }
+}
+
+// [comp][x][y][z] -> [x][y][z][comp], converting precision and scaling.
+template <typename R>
+__global__ void k_pack_fN(long long P, const double2* __restrict__ src, double scale,
+                          Cx<R>* dst) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6 * P;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long pt = t / 6;
+    const int comp = (int)(t - pt * 6);
+    double2 v = src[comp * P + pt];
+    v.x *= scale;
+    v.y *= scale;
+    dst[t] = from_d2<Cx<R>>(v);
+  }
+}
+
+}  // namespace vox

@@ -1,0 +1,481 @@
+// Level-1 circulant preconditioner on the device.
+//
+// Build (level_1_parallel_func_N.m:1-281 + Bragg_MOR_script.m:61-72):
+//   1. T. Chan optimal circulant of each Toeplitz component along x:
+//      c(1) = A(1), c(i) = (L+1-i)/L A(i) +/- (i-1)/L A(L-i+2)  (- for xy, xz)
+//   2. FFT along x (length L) of every (y, z, component) line
+//   3. per x-mode i: the dense 3MN x 3MN block of Toeplitz-in-y / Toeplitz-in-z
+//      sub-blocks (with the reference's sign pattern and triu symmetrisation
+//      for the xz and yz blocks), B_i = Gram*I - diag(face3)*circ_i
+//   4. batched LU with partial pivoting of all B_i (one CTA per block,
+//      right-looking, 8-column panels staged in shared memory)
+// Apply (chan_mvp_idx.m:4-16): scatter to the grid, FFT along x of every
+// (y,z,c) line, per mode P*L*U solve (blocked triangular solves, one CTA per
+// mode), inverse FFT along x (1/L), gather.  The apply reads each factor once:
+// L*(3MN)^2 complex values, the same bytes as the reference's inverse-block GEMV.
+// Caller-supplied inverse blocks (chan_mvp_idx's inv_blocks) are applied by a
+// plain per-mode GEMV instead.
+#pragma once
+
+#include "fft.cuh"
+#include "krylov.cuh"
+
+namespace vox {
+
+constexpr int kLuNb = 8;        // panel width of the batched LU
+constexpr int kTrsvNb = 32;     // diagonal block of the triangular solves
+
+struct PcGeom {
+  int L, M, N;
+  int n3;          // 3*M*N
+  long long V;
+  int ybx;         // lines per CTA in the x-FFT kernels
+  int sx;          // smem stride of a line
+};
+
+// --------------------------------------------------------------- apply: x-FFT
+template <typename R>
+__global__ void __launch_bounds__(256) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
+                                                 const Cx<R>* __restrict__ in,
+                                                 const int* __restrict__ vmap,
+                                                 Cx<R>* __restrict__ T, const int* skip) {
+  using C = Cx<R>;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + (size_t)g.ybx * g.sx;
+  const int col0 = blockIdx.x * g.ybx;
+  const int nl = min(g.ybx, g.n3 - col0);
+  for (int t = threadIdx.x; t < g.ybx * g.L; t += blockDim.x) {
+    const int l = t / g.L;
+    const int x = t - l * g.L;
+    C v = czero<C>();
+    if (l < nl) {
+      const int m = vmap[(long long)(col0 + l) * g.L + x];
+      if (m >= 0) v = in[m];
+    }
+    bufA[(size_t)l * g.sx + x] = v;
+  }
+  __syncthreads();
+  C* res = block_fft(bufA, bufB, pl, g.ybx, g.sx, tw, -1);
+  for (int t = threadIdx.x; t < nl * g.L; t += blockDim.x) {
+    const int i = t / nl;
+    const int l = t - i * nl;
+    T[(long long)i * g.n3 + col0 + l] = res[(size_t)l * g.sx + i];
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_pc_xinv(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
+                                                 const Cx<R>* __restrict__ T,
+                                                 const int* __restrict__ vmap, R scale,
+                                                 Cx<R>* out, const int* skip) {
+  using C = Cx<R>;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + (size_t)g.ybx * g.sx;
+  const int col0 = blockIdx.x * g.ybx;
+  const int nl = min(g.ybx, g.n3 - col0);
+  for (int t = threadIdx.x; t < g.ybx * g.L; t += blockDim.x) {
+    const int i = t / g.ybx;
+    const int l = t - i * g.ybx;
+    bufA[(size_t)l * g.sx + i] = (l < nl) ? T[(long long)i * g.n3 + col0 + l] : czero<C>();
+  }
+  __syncthreads();
+  C* res = block_fft(bufA, bufB, pl, g.ybx, g.sx, tw, +1);
+  for (int t = threadIdx.x; t < nl * g.L; t += blockDim.x) {
+    const int l = t / g.L;
+    const int x = t - l * g.L;
+    const int m = vmap[(long long)(col0 + l) * g.L + x];
+    if (m >= 0) out[m] = cscale(res[(size_t)l * g.sx + x], scale);
+  }
+}
+
+// --------------------------------------------------------- apply: block GEMV
+// T_i <- B_i T_i with B_i column-major n3 x n3 (explicit inverse blocks).
+template <typename R>
+__global__ void __launch_bounds__(256) k_pc_gemv(PcGeom g, const Cx<R>* __restrict__ B,
+                                                 const Cx<R>* __restrict__ Tin,
+                                                 Cx<R>* __restrict__ Tout, const int* skip) {
+  using C = Cx<R>;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* xs = reinterpret_cast<C*>(smem_raw);
+  const int n3 = g.n3;
+  const int tilesR = (n3 + blockDim.x - 1) / blockDim.x;
+  const int i = blockIdx.x / tilesR;
+  const int r = (blockIdx.x % tilesR) * blockDim.x + threadIdx.x;
+  for (int c = threadIdx.x; c < n3; c += blockDim.x) xs[c] = Tin[(long long)i * n3 + c];
+  __syncthreads();
+  if (r >= n3) return;
+  const C* Bi = B + (long long)i * n3 * n3;
+  C acc0 = czero<C>(), acc1 = czero<C>();
+  int c = 0;
+  for (; c + 1 < n3; c += 2) {
+    cfma(acc0, Bi[(long long)c * n3 + r], xs[c]);
+    cfma(acc1, Bi[(long long)(c + 1) * n3 + r], xs[c + 1]);
+  }
+  if (c < n3) cfma(acc0, Bi[(long long)c * n3 + r], xs[c]);
+  Tout[(long long)i * n3 + r] = cadd(acc0, acc1);
+}
+
+// ------------------------------------------------ apply: LU triangular solves
+// One CTA per mode: t = P t; t = L^{-1} t (unit lower); t = U^{-1} t.
+// Factors column-major in A (n3 x n3 per mode), pivots 0-based rows in piv.
+template <typename R>
+__global__ void __launch_bounds__(512) k_pc_lu_solve(PcGeom g, const Cx<R>* __restrict__ A,
+                                                     const int* __restrict__ piv, Cx<R>* T,
+                                                     const int* skip) {
+  using C = Cx<R>;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* t = reinterpret_cast<C*>(smem_raw);  // n3
+  const int n = g.n3;
+  const int i = blockIdx.x;
+  const C* Ai = A + (long long)i * n * n;
+  const int* pv = piv + (long long)i * n;
+  C* Ti = T + (long long)i * n;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) t[c] = Ti[c];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < n; k++) {
+      const int p = pv[k];
+      if (p != k) {
+        C a = t[k];
+        t[k] = t[p];
+        t[p] = a;
+      }
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // forward substitution with unit lower L, blocks of kTrsvNb columns
+  for (int k0 = 0; k0 < n; k0 += kTrsvNb) {
+    const int kb = min(kTrsvNb, n - k0);
+    if (warp == 0) {
+      // solve the diagonal block: lane r holds t[k0+r]
+      C v = (lane < kb) ? t[k0 + lane] : czero<C>();
+      for (int j = 0; j < kb; j++) {
+        C tj;
+        tj.x = __shfl_sync(0xffffffffu, v.x, j);
+        tj.y = __shfl_sync(0xffffffffu, v.y, j);
+        if (lane > j && lane < kb) {
+          const C l = Ai[(long long)(k0 + j) * n + k0 + lane];
+          v.x -= l.x * tj.x - l.y * tj.y;
+          v.y -= l.x * tj.y + l.y * tj.x;
+        }
+      }
+      if (lane < kb) t[k0 + lane] = v;
+    }
+    __syncthreads();
+    // update the rows below with the panel columns
+    for (int r = k0 + kb + threadIdx.x; r < n; r += blockDim.x) {
+      C acc = t[r];
+      for (int j = 0; j < kb; j++) {
+        const C l = Ai[(long long)(k0 + j) * n + r];
+        const C tj = t[k0 + j];
+        acc.x -= l.x * tj.x - l.y * tj.y;
+        acc.y -= l.x * tj.y + l.y * tj.x;
+      }
+      t[r] = acc;
+    }
+    __syncthreads();
+  }
+  // back substitution with U, blocks from the bottom
+  const int nblk = (n + kTrsvNb - 1) / kTrsvNb;
+  for (int bk = nblk - 1; bk >= 0; bk--) {
+    const int k0 = bk * kTrsvNb;
+    const int kb = min(kTrsvNb, n - k0);
+    if (warp == 0) {
+      C v = (lane < kb) ? t[k0 + lane] : czero<C>();
+      for (int j = kb - 1; j >= 0; j--) {
+        // v_j /= U(j,j)
+        if (lane == j) {
+          const C d = Ai[(long long)(k0 + j) * n + k0 + j];
+          const R dd = d.x * d.x + d.y * d.y;
+          C q;
+          q.x = (v.x * d.x + v.y * d.y) / dd;
+          q.y = (v.y * d.x - v.x * d.y) / dd;
+          v = q;
+        }
+        C tj;
+        tj.x = __shfl_sync(0xffffffffu, v.x, j);
+        tj.y = __shfl_sync(0xffffffffu, v.y, j);
+        if (lane < j) {
+          const C u = Ai[(long long)(k0 + j) * n + k0 + lane];
+          v.x -= u.x * tj.x - u.y * tj.y;
+          v.y -= u.x * tj.y + u.y * tj.x;
+        }
+      }
+      if (lane < kb) t[k0 + lane] = v;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < k0; r += blockDim.x) {
+      C acc = t[r];
+      for (int j = 0; j < kb; j++) {
+        const C u = Ai[(long long)(k0 + j) * n + r];
+        const C tj = t[k0 + j];
+        acc.x -= u.x * tj.x - u.y * tj.y;
+        acc.y -= u.x * tj.y + u.y * tj.x;
+      }
+      t[r] = acc;
+    }
+    __syncthreads();
+  }
+  for (int c = threadIdx.x; c < n; c += blockDim.x) Ti[c] = t[c];
+}
+
+// ------------------------------------------------------------------- build
+// Chan circulant along x of each component: src/dst [comp][z][y][x] (x fastest).
+__global__ void k_chan(int L, long long V, const double2* __restrict__ G, double2* out) {
+  const int sgn[6] = {1, -1, -1, 1, 1, 1};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6 * V;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int comp = (int)(t / V);
+    const long long r = t - comp * V;
+    const int x = (int)(r % L);
+    const long long line = r - x;  // index of (0, y, z)
+    const double2* A = G + comp * V + line;
+    double2 v;
+    if (x == 0) {
+      v = A[0];
+    } else {
+      const double a = (double)(L - x) / L, b = sgn[comp] * (double)x / L;
+      const double2 p = A[x], q = A[L - x];
+      v = make_double2(a * p.x + b * q.x, a * p.y + b * q.y);
+    }
+    out[t] = v;
+  }
+}
+
+// Dense block of mode i (column-major n3 x n3) from the x-transformed Chan
+// circulants Cf [comp][z][y][x]; B = gram*I - face3 .* circ.
+__global__ void k_assemble_blocks(int L, int M, int N, long long V, int i0, int nmodes,
+                                  const double2* __restrict__ Cf, const double* __restrict__ face3,
+                                  double gram, double2* __restrict__ B) {
+  const int MN = M * N, n3 = 3 * MN;
+  const long long per = (long long)n3 * n3;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nmodes * per;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int im = (int)(t / per);
+    const long long e = t - im * per;
+    const int col = (int)(e / n3);
+    const int row = (int)(e - (long long)col * n3);
+    const int i = i0 + im;
+    const int bp = row / MN, bq = col / MN;
+    const int p = row - bp * MN, q = col - bq * MN;
+    const int yp = p % M, zp = p / M, yq = q % M, zq = q / M;
+    const int dy = yp > yq ? yp - yq : yq - yp;
+    const int dz = zp > zq ? zp - zq : zq - zp;
+    auto C = [&](int comp, int y, int z) -> double2 {
+      return Cf[comp * V + i + (long long)L * (y + (long long)M * z)];
+    };
+    double2 v;
+    const int b0 = bp < bq ? bp : bq, b1 = bp < bq ? bq : bp;
+    if (b0 == 0 && b1 == 0) {
+      v = C(0, dy, dz);
+    } else if (b0 == 0 && b1 == 1) {
+      // toeplitz([-CC(1) CC(2:M)], -CC(1:M)): y > y' -> CC, else -CC
+      const double2 c = C(1, dy, dz);
+      v = (yp > yq) ? c : make_double2(-c.x, -c.y);
+    } else if (b0 == 0 && b1 == 2) {
+      // -C3 symmetric, then triu antisymmetrised: p<q -> -C3, p>q -> +C3, p==q -> -C3
+      const double2 c = C(2, dy, dz);
+      v = (p > q) ? c : make_double2(-c.x, -c.y);
+    } else if (b0 == 1 && b1 == 1) {
+      v = C(3, dy, dz);
+    } else if (b0 == 1 && b1 == 2) {
+      // toeplitz([C5(1) -C5(2:M)], C5(1:M)) then triu symmetrised:
+      // value of the upper entry (a<=b): y_a > y_b -> -C5, else C5
+      const int a = p < q ? p : q, b = p < q ? q : p;
+      const int ya = a % M, yb = b % M;
+      const double2 c = C(4, dy, dz);
+      v = (ya > yb) ? make_double2(-c.x, -c.y) : c;
+    } else {
+      v = C(5, dy, dz);
+    }
+    const double f = face3[row];
+    double2 o = make_double2(-f * v.x, -f * v.y);
+    if (row == col) o.x += gram;
+    B[(long long)im * per + e] = o;
+  }
+}
+
+// Batched LU with partial pivoting, one CTA per matrix (column-major n x n).
+// piv[k] = 0-based row swapped with row k at step k (LAPACK getrf order).
+template <typename R>
+__global__ void __launch_bounds__(512) k_lu_batched(int n, Cx<R>* A, int* piv, int* info) {
+  using C = Cx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* P = reinterpret_cast<C*>(smem_raw);  // panel: (n) x kLuNb, column-major, ld = n
+  __shared__ int s_piv[kLuNb];
+  __shared__ R s_best[32];
+  __shared__ int s_bidx[32];
+  C* Ai = A + (long long)blockIdx.x * n * n;
+  int* pv = piv + (long long)blockIdx.x * n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k0 = 0; k0 < n; k0 += kLuNb) {
+    const int kb = min(kLuNb, n - k0);
+    const int rows = n - k0;
+    // load panel rows k0..n-1, columns k0..k0+kb-1
+    for (int t = threadIdx.x; t < rows * kb; t += blockDim.x) {
+      const int j = t / rows, r = t - j * rows;
+      P[(size_t)j * n + r] = Ai[(long long)(k0 + j) * n + k0 + r];
+    }
+    __syncthreads();
+    for (int j = 0; j < kb; j++) {
+      // pivot search over panel rows j..rows-1 of column j
+      R best = -1;
+      int bidx = j;
+      for (int r = j + threadIdx.x; r < rows; r += blockDim.x) {
+        const C a = P[(size_t)j * n + r];
+        const R m = fabs(a.x) + fabs(a.y);
+        if (m > best) {
+          best = m;
+          bidx = r;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const R ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bidx, o);
+        if (ob > best || (ob == best && oi < bidx)) {
+          best = ob;
+          bidx = oi;
+        }
+      }
+      if (lane == 0) {
+        s_best[warp] = best;
+        s_bidx[warp] = bidx;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        R b = s_best[0];
+        int bi = s_bidx[0];
+        for (int w = 1; w < nw; w++)
+          if (s_best[w] > b || (s_best[w] == b && s_bidx[w] < bi)) {
+            b = s_best[w];
+            bi = s_bidx[w];
+          }
+        s_piv[j] = bi;
+        pv[k0 + j] = k0 + bi;
+        if (b <= 0 && info) atomicExch(info + blockIdx.x, k0 + j + 1);
+      }
+      __syncthreads();
+      const int pr = s_piv[j];
+      if (pr != j) {
+        for (int c = threadIdx.x; c < kb; c += blockDim.x) {
+          C a = P[(size_t)c * n + j];
+          P[(size_t)c * n + j] = P[(size_t)c * n + pr];
+          P[(size_t)c * n + pr] = a;
+        }
+      }
+      __syncthreads();
+      const C d = P[(size_t)j * n + j];
+      const R dd = d.x * d.x + d.y * d.y;
+      for (int r = j + 1 + threadIdx.x; r < rows; r += blockDim.x) {
+        if (dd > 0) {
+          const C a = P[(size_t)j * n + r];
+          C l;
+          l.x = (a.x * d.x + a.y * d.y) / dd;
+          l.y = (a.y * d.x - a.x * d.y) / dd;
+          P[(size_t)j * n + r] = l;
+          for (int c = j + 1; c < kb; c++) {
+            const C u = P[(size_t)c * n + j];
+            C& e = P[(size_t)c * n + r];
+            e.x -= l.x * u.x - l.y * u.y;
+            e.y -= l.x * u.y + l.y * u.x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // write the panel back
+    for (int t = threadIdx.x; t < rows * kb; t += blockDim.x) {
+      const int j = t / rows, r = t - j * rows;
+      Ai[(long long)(k0 + j) * n + k0 + r] = P[(size_t)j * n + r];
+    }
+    // row swaps on the columns outside the panel
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      if (c >= k0 && c < k0 + kb) continue;
+      C* colp = Ai + (long long)c * n;
+      for (int j = 0; j < kb; j++) {
+        const int pr = k0 + s_piv[j];
+        if (pr != k0 + j) {
+          C a = colp[k0 + j];
+          colp[k0 + j] = colp[pr];
+          colp[pr] = a;
+        }
+      }
+    }
+    __syncthreads();
+    // U12 = L11^{-1} A12 and trailing update A22 -= L21 U12, one column per thread
+    for (int c = k0 + kb + threadIdx.x; c < n; c += blockDim.x) {
+      C* colp = Ai + (long long)c * n;
+      C u[kLuNb];
+#pragma unroll
+      for (int j = 0; j < kLuNb; j++) u[j] = (j < kb) ? colp[k0 + j] : czero<C>();
+#pragma unroll
+      for (int j = 0; j < kLuNb; j++) {
+        if (j >= kb) break;
+#pragma unroll
+        for (int q = j + 1; q < kLuNb; q++) {
+          if (q < kb) {
+            const C l = P[(size_t)j * n + q];
+            u[q].x -= l.x * u[j].x - l.y * u[j].y;
+            u[q].y -= l.x * u[j].y + l.y * u[j].x;
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kLuNb; j++)
+        if (j < kb) colp[k0 + j] = u[j];
+    }
+    __syncthreads();
+    // trailing update, threads over (row) inside column sweeps: coalesced rows
+    const int r0 = k0 + kb;
+    for (int c = r0 + warp; c < n; c += nw) {
+      C* colp = Ai + (long long)c * n;
+      C u[kLuNb];
+#pragma unroll
+      for (int j = 0; j < kLuNb; j++) u[j] = (j < kb) ? colp[k0 + j] : czero<C>();
+      for (int r = r0 + lane; r < n; r += 32) {
+        C e = colp[r];
+#pragma unroll
+        for (int j = 0; j < kLuNb; j++) {
+          if (j < kb) {
+            const C l = P[(size_t)j * n + (r - k0)];
+            e.x -= l.x * u[j].x - l.y * u[j].y;
+            e.y -= l.x * u[j].y + l.y * u[j].x;
+          }
+        }
+        colp[r] = e;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename R>
+__global__ void k_cast_scale(long long n, const double2* __restrict__ src, double s, Cx<R>* dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = from_d2<Cx<R>>(make_double2(src[i].x * s, src[i].y * s));
+}
+
+// Cast LU factors to precision R, scaling the upper triangle (U, with the
+// diagonal) of every n x n column-major block by s.
+template <typename R>
+__global__ void k_cast_scale_upper(long long tot, int n, const double2* __restrict__ src, double s,
+                                   Cx<R>* dst) {
+  const long long per = (long long)n * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long e = i % per;
+    const int col = (int)(e / n), row = (int)(e - (long long)col * n);
+    const double f = row <= col ? s : 1.0;
+    dst[i] = from_d2<Cx<R>>(make_double2(src[i].x * f, src[i].y * f));
+  }
+}
+
+}  // namespace vox

@@ -1,0 +1,890 @@
+// Preconditioner handles, device GMRES driver (pgmres semantics) and the
+// complex64 + FP64-refinement solver.  Included at the end of api.cu.
+#pragma once
+
+struct vox_precond_s {
+  vox_op_s* op = nullptr;
+  PcGeom g{};
+  FftPlan pl{};
+  bool lu = true;              // LU factors (true) or explicit inverse blocks (false)
+  double2* Ad = nullptr;       // c128 blocks / factors, L * n3 * n3
+  float2* Af = nullptr;        // c64 copy (blocks scaled for the A/Gram operator)
+  int* piv = nullptr;          // L * n3
+  double2* twd = nullptr;
+  float2* twf = nullptr;
+  double2* Td = nullptr;       // L * n3 work
+  double2* Td2 = nullptr;
+  float2* Tf = nullptr;
+  float2* Tf2 = nullptr;
+  double f_scale = 1.0;        // the c64 copy applies f_scale * M^{-1}
+};
+
+namespace vox {
+
+static size_t pc_xsmem(const PcGeom& g, size_t cs) { return 2ull * g.ybx * g.sx * cs; }
+
+template <typename R> Cx<R>* pc_A(vox_precond_s* p);
+template <> double2* pc_A<double>(vox_precond_s* p) { return p->Ad; }
+template <> float2* pc_A<float>(vox_precond_s* p) { return p->Af; }
+template <typename R> Cx<R>* pc_T(vox_precond_s* p, int which);
+template <> double2* pc_T<double>(vox_precond_s* p, int w) { return w ? p->Td2 : p->Td; }
+template <> float2* pc_T<float>(vox_precond_s* p, int w) { return w ? p->Tf2 : p->Tf; }
+template <typename R> Cx<R>* pc_tw(vox_precond_s* p);
+template <> double2* pc_tw<double>(vox_precond_s* p) { return p->twd; }
+template <> float2* pc_tw<float>(vox_precond_s* p) { return p->twf; }
+
+// out = M^{-1} in (c128) or f_scale * M^{-1} in (c64 copy).  in/out length n.
+template <typename R>
+static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaStream_t st,
+                           const int* skip) {
+  const PcGeom& g = p->g;
+  const size_t cs = sizeof(Cx<R>);
+  const int nb = (g.n3 + g.ybx - 1) / g.ybx;
+  Cx<R>* T = pc_T<R>(p, 0);
+  k_pc_xfwd<R><<<nb, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip);
+  if (p->lu) {
+    k_pc_lu_solve<R><<<g.L, 512, (size_t)g.n3 * cs, st>>>(g, pc_A<R>(p), p->piv, T, skip);
+  } else {
+    Cx<R>* T2 = pc_T<R>(p, 1);
+    const int tiles = (g.n3 + 255) / 256;
+    k_pc_gemv<R><<<g.L * tiles, 256, (size_t)g.n3 * cs, st>>>(g, pc_A<R>(p), T, T2, skip);
+    T = T2;
+  }
+  k_pc_xinv<R><<<nb, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T, p->op->vmap,
+                                                  (R)(1.0 / g.L), out, skip);
+  VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
+template <typename R>
+static vox_status pc_attrs(const PcGeom& g) {
+  const size_t cs = sizeof(Cx<R>);
+  VOX_CUDA(cudaFuncSetAttribute(k_pc_xfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)pc_xsmem(g, cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_pc_xinv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)pc_xsmem(g, cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_pc_lu_solve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(g.n3 * cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_pc_gemv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(g.n3 * cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_lu_batched<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)((size_t)g.n3 * kLuNb * cs)));
+  return VOX_OK;
+}
+
+static void pc_free(vox_precond_s* p) {
+  if (!p) return;
+  cudaFree(p->Ad);
+  cudaFree(p->Af);
+  cudaFree(p->piv);
+  cudaFree(p->twd);
+  cudaFree(p->twf);
+  cudaFree(p->Td);
+  cudaFree(p->Td2);
+  cudaFree(p->Tf);
+  cudaFree(p->Tf2);
+  delete p;
+}
+
+static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
+  p->op = op;
+  PcGeom& g = p->g;
+  g.L = op->g.L;
+  g.M = op->g.M;
+  g.N = op->g.N;
+  g.n3 = 3 * g.M * g.N;
+  g.V = op->g.V;
+  if (!make_fft_plan(g.L, &p->pl)) {
+    set_error("preconditioner: FFT length L has a prime factor above 64");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  g.sx = pad_stride(g.L);
+  const size_t per = 2ull * g.sx * sizeof(double2);
+  g.ybx = (int)std::max<size_t>(1, std::min<size_t>(8, kSmemBudget / per));
+  if (per > 220 * 1024) {
+    set_error("preconditioner: L too long for the shared-memory FFT");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  if ((size_t)g.n3 * kLuNb * sizeof(double2) > 220 * 1024) {
+    set_error("preconditioner: 3*M*N too large for the batched LU panel");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  std::vector<double2> tw = twiddles(g.L);
+  std::vector<float2> twf(g.L);
+  for (int i = 0; i < g.L; i++) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+  VOX_TRY(dalloc(&p->twd, g.L));
+  VOX_TRY(dalloc(&p->twf, g.L));
+  VOX_CUDA(cudaMemcpy(p->twd, tw.data(), g.L * sizeof(double2), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpy(p->twf, twf.data(), g.L * sizeof(float2), cudaMemcpyHostToDevice));
+  const long long LT = (long long)g.L * g.n3;
+  VOX_TRY(dalloc(&p->Td, LT));
+  VOX_TRY(dalloc(&p->Td2, LT));
+  VOX_TRY(dalloc(&p->Tf, LT));
+  VOX_TRY(dalloc(&p->Tf2, LT));
+  VOX_TRY(pc_attrs<double>(g));
+  VOX_TRY(pc_attrs<float>(g));
+  return VOX_OK;
+}
+
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const double* G_im,
+                                     const double* face3, vox_precond_t* out) {
+  if (!op || !G_re || !face3 || !out) {
+    set_error("vox_precond_create_level1: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  DeviceGuard dg(op->device);
+  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
+  VOX_TRY(pc_common(op, p.get()));
+  const PcGeom& g = p->g;
+  cudaStream_t st = op->stream;
+  const long long V = g.V;
+  // Toeplitz -> Chan circulants -> FFT along x
+  std::vector<double2> G(6 * V);
+  for (long long i = 0; i < 6 * V; i++) G[i] = make_double2(G_re[i], G_im ? G_im[i] : 0.0);
+  double2 *dG, *dC;
+  VOX_TRY(dalloc(&dG, 6 * V));
+  std::unique_ptr<double2, decltype(&cudaFree)> gG(dG, cudaFree);
+  VOX_TRY(dalloc(&dC, 6 * V));
+  std::unique_ptr<double2, decltype(&cudaFree)> gC(dC, cudaFree);
+  VOX_CUDA(cudaMemcpy(dG, G.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice));
+  k_chan<<<nblk(6 * V), 256, 0, st>>>(g.L, V, dG, dC);
+  VOX_CUDA(cudaGetLastError());
+  VOX_TRY(fft_axis_d(dC, g.L, g.M, g.N, 1, g.L, (long long)g.L * g.M, V, 6, 0, -1, st));
+  double* dface;
+  VOX_TRY(dalloc(&dface, g.n3));
+  std::unique_ptr<double, decltype(&cudaFree)> gF(dface, cudaFree);
+  VOX_CUDA(cudaMemcpy(dface, face3, g.n3 * sizeof(double), cudaMemcpyHostToDevice));
+  // blocks and LU
+  const long long per = (long long)g.n3 * g.n3;
+  VOX_TRY(dalloc(&p->Ad, g.L * per));
+  VOX_TRY(dalloc(&p->piv, (long long)g.L * g.n3));
+  k_assemble_blocks<<<nblk(g.L * per), 256, 0, st>>>(g.L, g.M, g.N, V, 0, g.L, dC, dface,
+                                                      op->gram, p->Ad);
+  VOX_CUDA(cudaGetLastError());
+  int* dinfo;
+  VOX_TRY(dalloc(&dinfo, g.L));
+  std::unique_ptr<int, decltype(&cudaFree)> gI(dinfo, cudaFree);
+  VOX_CUDA(cudaMemsetAsync(dinfo, 0, g.L * sizeof(int), st));
+  k_lu_batched<double><<<g.L, 512, (size_t)g.n3 * kLuNb * sizeof(double2), st>>>(g.n3, p->Ad,
+                                                                                 p->piv, dinfo);
+  VOX_CUDA(cudaGetLastError());
+  std::vector<int> info(g.L);
+  VOX_CUDA(cudaMemcpyAsync(info.data(), dinfo, g.L * sizeof(int), cudaMemcpyDeviceToHost, st));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < g.L; i++)
+    if (info[i]) {
+      set_error("vox_precond_create_level1: block " + std::to_string(i) + " is singular");
+      return VOX_ERR_BAD_ARG;
+    }
+  // c64 copy: factors of B/Gram (the c64 operator is A/Gram): L unchanged, U / Gram,
+  // so the copy applies Gram * M^{-1}
+  p->lu = true;
+  p->f_scale = op->gram;
+  if (op->has_f) {
+    VOX_TRY(dalloc(&p->Af, g.L * per));
+    k_cast_scale_upper<float><<<nblk(g.L * per), 256, 0, st>>>(g.L * per, g.n3, p->Ad,
+                                                               1.0 / op->gram, p->Af);
+    VOX_CUDA(cudaGetLastError());
+  }
+  VOX_CUDA(cudaStreamSynchronize(st));
+  op->pcs.push_back(p.get());
+  *out = p.release();
+  return VOX_OK;
+}
+
+vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const double* blk_im,
+                                     vox_precond_t* out) {
+  if (!op || !blk_re || !out) {
+    set_error("vox_precond_create_blocks: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  DeviceGuard dg(op->device);
+  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
+  VOX_TRY(pc_common(op, p.get()));
+  const PcGeom& g = p->g;
+  const long long tot = (long long)g.L * g.n3 * g.n3;
+  std::vector<double2> B(tot);
+  for (long long i = 0; i < tot; i++) B[i] = make_double2(blk_re[i], blk_im ? blk_im[i] : 0.0);
+  VOX_TRY(dalloc(&p->Ad, tot));
+  VOX_CUDA(cudaMemcpy(p->Ad, B.data(), tot * sizeof(double2), cudaMemcpyHostToDevice));
+  p->lu = false;
+  p->f_scale = op->gram;
+  if (op->has_f) {
+    VOX_TRY(dalloc(&p->Af, tot));
+    k_cast_scale<float><<<nblk(tot), 256, 0, op->stream>>>(tot, p->Ad, op->gram, p->Af);
+    VOX_CUDA(cudaGetLastError());
+  }
+  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  op->pcs.push_back(p.get());
+  *out = p.release();
+  return VOX_OK;
+}
+
+void vox_precond_destroy(vox_precond_t p) {
+  if (!p) return;
+  pc_release(p);
+}
+
+}  // extern "C"
+
+namespace vox {
+
+// Unregister from the operator, drop cached GMRES graphs that captured this
+// preconditioner and free it.
+static void pc_release(vox_precond_s* p) {
+  vox_op_s* op = p->op;
+  DeviceGuard dg(op->device);
+  cudaDeviceSynchronize();
+  op->pcs.erase(std::remove(op->pcs.begin(), op->pcs.end(), p), op->pcs.end());
+  // drop cached GMRES graphs that captured this preconditioner
+  for (auto it = op->wd.graphs.begin(); it != op->wd.graphs.end();) {
+    if (it->first.first == (void*)p) {
+      cudaGraphExecDestroy(it->second);
+      it = op->wd.graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  for (auto it = op->wf.graphs.begin(); it != op->wf.graphs.end();) {
+    if (it->first.first == (void*)p) {
+      cudaGraphExecDestroy(it->second);
+      it = op->wf.graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  pc_free(p);
+}
+
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_precond_apply(vox_precond_t p, vox_prec prec, const double* in_re,
+                             const double* in_im, double* out_re, double* out_im) {
+  if (!p || !in_re || !out_re) {
+    set_error("vox_precond_apply: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  vox_op_s* op = p->op;
+  VOX_TRY(check_prec(op, prec));
+  DeviceGuard dg(op->device);
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  split_to_d2(in_re, in_im, n, op->h_in);
+  VOX_CUDA(cudaMemcpyAsync(op->d_in, op->h_in, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+  if (prec == VOX_C128) {
+    VOX_TRY(pc_apply<double>(p, op->d_in, op->d_out, st, nullptr));
+  } else {
+    k_from_d2<float><<<nblk(n), 256, 0, st>>>(n, op->d_in, op->f_in);
+    VOX_TRY(pc_apply<float>(p, op->f_in, op->f_out, st, nullptr));
+    k_to_d2<float><<<nblk(n), 256, 0, st>>>(n, op->f_out, 1.0 / p->f_scale, op->d_out);
+  }
+  VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  d2_to_split(op->h_out, n, out_re, out_im);
+  return VOX_OK;
+}
+
+}  // extern "C"
+
+namespace vox {
+
+// ------------------------------------------------------------ GMRES driver
+template <typename R>
+static vox_status ensure_work(vox_op_s* op, int m) {
+  GmresWork<R>& w = work<R>(op);
+  if (w.m == m && w.V) return VOX_OK;
+  w.release();
+  const long long n = op->g.n;
+  VOX_TRY(dalloc(&w.V, (long long)(m + 1) * n));
+  VOX_TRY(dalloc(&w.w, n));
+  VOX_TRY(dalloc(&w.t, n));
+  VOX_TRY(dalloc(&w.r, n));
+  VOX_TRY(dalloc(&w.x, n));
+  VOX_TRY(dalloc(&w.b, n));
+  VOX_TRY(dalloc(&w.st, 1));
+  VOX_CUDA(cudaMallocHost((void**)&w.hst, sizeof(GmresDev)));
+  VOX_CUDA(cudaMemset(w.st, 0, sizeof(GmresDev)));
+  w.m = m;
+  return VOX_OK;
+}
+
+// Enqueue one restart cycle (pgmres_iter.m) on stream st.
+template <typename R>
+static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, cudaStream_t st) {
+  GmresWork<R>& w = work<R>(op);
+  const long long n = op->g.n;
+  const int m = w.m;
+  GmresDev* d = w.st;
+  const int* skip = &d->done;
+  const int nb = nblk(n);
+  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, w.r, n, 0);
+  k_cycle_init<<<1, 32, 0, st>>>(d);
+  k_cycle_v0<R><<<nb, 256, 0, st>>>(d, w.V, w.r, n);
+  for (int k = 0; k < m; k++) {
+    Cx<R>* vk = w.V + (long long)k * n;
+    const Cx<R>* src = vk;
+    if (side == VOX_PREC_RIGHT && pc) {
+      VOX_TRY(pc_apply<R>(pc, vk, w.t, st, skip));
+      src = w.t;
+    }
+    VOX_TRY(matvec<R>(op, MV_AN, src, w.w, st, skip));
+    Cx<R>* wv = w.w;
+    if (side == VOX_PREC_LEFT && pc) {
+      VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, skip));
+      wv = w.t;
+    }
+    k_gs_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
+    k_gs_update_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
+    k_gs_update_norm<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
+    k_gs_scale<R><<<nb, 256, 0, st>>>(d, w.V + (long long)(k + 1) * n, wv, n);
+  }
+  k_cycle_ls<<<1, 32, 0, st>>>(d);
+  if (side == VOX_PREC_RIGHT && pc) {
+    k_cycle_vy<R><<<nb, 256, 0, st>>>(d, w.V, n, w.w, n);
+    VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, nullptr));
+    k_axpy<R><<<nb, 256, 0, st>>>(w.x, w.t, n);
+    k_cycle_update<R><<<nb, 256, 0, st>>>(d, w.V, n, (Cx<R>*)nullptr, w.r, n);
+  } else {
+    k_cycle_update<R><<<nb, 256, 0, st>>>(d, w.V, n, w.x, w.r, n);
+  }
+  VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
+template <typename R>
+static vox_status get_cycle_graph(vox_op_s* op, vox_precond_s* pc, int side,
+                                  cudaGraphExec_t* out) {
+  GmresWork<R>& w = work<R>(op);
+  auto key = std::make_pair((void*)pc, side);
+  auto it = w.graphs.find(key);
+  if (it != w.graphs.end()) {
+    *out = it->second;
+    return VOX_OK;
+  }
+  cudaStream_t st = op->stream;
+  cudaGraph_t graph;
+  VOX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  vox_status s = enqueue_cycle<R>(op, pc, side, st);
+  cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (s != VOX_OK) return s;
+  if (e != cudaSuccess) {
+    set_error(std::string("graph capture: ") + cudaGetErrorString(e));
+    return VOX_ERR_CUDA;
+  }
+  size_t nnodes = 0;
+  cudaGraphGetNodes(graph, nullptr, &nnodes);
+  cudaGraphExec_t exec;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  op->graph_nodes[exec] = (int)nnodes;
+  if (e != cudaSuccess) {
+    set_error(std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return VOX_ERR_CUDA;
+  }
+  w.graphs[key] = exec;
+  *out = exec;
+  return VOX_OK;
+}
+
+template <typename R>
+__global__ void k_sub(long long n, const Cx<R>* __restrict__ b, const Cx<R>* __restrict__ ax,
+                      Cx<R>* r) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    r[i] = csub(b[i], ax[i]);
+}
+
+template <typename R>
+static vox_status read_scal(vox_op_s* op, int slot, double* v) {
+  GmresWork<R>& w = work<R>(op);
+  VOX_CUDA(cudaMemcpyAsync(v, &w.st->scal[slot], sizeof(double), cudaMemcpyDeviceToHost,
+                           op->stream));
+  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  return VOX_OK;
+}
+
+// pgmres.m:70-181 on device vectors already in w.b; solution in w.x.
+// The preconditioned-residual history (relative) is appended to resvec.
+template <typename R>
+static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, double tol, int maxit,
+                             vox_gmres_info* info, std::vector<double>* resvec) {
+  GmresWork<R>& w = work<R>(op);
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  const int nb = nblk(n);
+  if (side != VOX_PREC_NONE && !pc) side = VOX_PREC_NONE;
+  // x0 = 0 -> r = b ; left preconditioning: r = M^{-1} b, bnorm = ||M^{-1} b||
+  VOX_CUDA(cudaMemsetAsync(w.x, 0, n * sizeof(Cx<R>), st));
+  if (side == VOX_PREC_LEFT) {
+    VOX_TRY(pc_apply<R>(pc, w.b, w.r, st, nullptr));
+  } else {
+    VOX_CUDA(cudaMemcpyAsync(w.r, w.b, n * sizeof(Cx<R>), cudaMemcpyDeviceToDevice, st));
+  }
+  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.r, n, 1);
+  op->launches += (side == VOX_PREC_LEFT) ? 4 : 1;
+  double bn2;
+  VOX_TRY(read_scal<R>(op, 1, &bn2));
+  const double bnorm = std::sqrt(bn2);
+  if (bnorm == 0.0) {
+    info->flag = 0;
+    info->relres = 0.0;
+    info->iter_inner = info->iter_outer = 0;
+    if (resvec) resvec->push_back(0.0);
+    return VOX_OK;
+  }
+  // reset the header fields (everything before resvec) of the device state
+  std::vector<unsigned char> hdr(offsetof(GmresDev, resvec), 0);
+  GmresDev* init = reinterpret_cast<GmresDev*>(hdr.data());
+  init->m = w.m;
+  init->tol_abs = tol * bnorm;
+  VOX_CUDA(cudaMemcpyAsync(w.st, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  cudaGraphExec_t cyc;
+  VOX_TRY(get_cycle_graph<R>(op, pc, side, &cyc));
+  double rel = 1.0;  // ||r0|| / bnorm with x0 = 0
+  if (resvec) resvec->push_back(rel);
+  int outit = 0, p = 0;
+  while (rel > tol && outit < maxit) {
+    outit++;
+    VOX_CUDA(cudaGraphLaunch(cyc, st));
+    op->launches += op->graph_nodes[cyc];
+    VOX_CUDA(cudaMemcpyAsync(w.hst, w.st, offsetof(GmresDev, sn), cudaMemcpyDeviceToHost, st));
+    VOX_CUDA(cudaStreamSynchronize(st));
+    p = w.hst->k;
+    for (int i = 0; i < p; i++)
+      if (resvec) resvec->push_back(w.hst->resvec[i] / bnorm);
+    info->total_iters += p;
+    rel = (p > 0) ? w.hst->resvec[p - 1] / bnorm : rel;
+    if (w.hst->breakdown && !w.hst->converged) {
+      // exact breakdown: the Krylov space is invariant, the LS solution is exact
+      break;
+    }
+  }
+  info->iter_inner = p;
+  info->iter_outer = outit;
+  return VOX_OK;
+}
+
+// relres = ||b - A x|| / ||b|| in the given precision's vectors (x, b in work)
+template <typename R>
+static vox_status true_relres(vox_op_s* op, double* relres) {
+  GmresWork<R>& w = work<R>(op);
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  VOX_TRY(matvec<R>(op, MV_AN, w.x, w.w, st, nullptr));
+  k_sub<R><<<nblk(n), 256, 0, st>>>(n, w.b, w.w, w.t);
+  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.t, n, 2);
+  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.b, n, 3);
+  op->launches += 6;
+  double a, b;
+  VOX_TRY(read_scal<R>(op, 2, &a));
+  VOX_TRY(read_scal<R>(op, 3, &b));
+  *relres = b > 0 ? std::sqrt(a / b) : 0.0;
+  return VOX_OK;
+}
+
+static void fill_resvec(vox_gmres_info* info, const std::vector<double>& rv) {
+  if (!info) return;
+  info->n_resvec = (long long)rv.size();
+  if (info->resvec && info->resvec_cap > 0) {
+    const long long c = std::min<long long>(info->resvec_cap, (long long)rv.size());
+    std::memcpy(info->resvec, rv.data(), c * sizeof(double));
+  }
+}
+
+template <typename R>
+static vox_status pgmres_entry(vox_op_s* op, vox_precond_s* pc, int side, const double2* b_dev,
+                               int restart, double tol, int maxit, double2* x_dev,
+                               vox_gmres_info* info) {
+  if (restart < 1 || restart > kMaxRestart) {
+    set_error("restart must be in 1.." + std::to_string(kMaxRestart));
+    return VOX_ERR_BAD_ARG;
+  }
+  VOX_TRY(ensure_work<R>(op, restart));
+  GmresWork<R>& w = work<R>(op);
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  // b in the working precision (the c64 operator is A/Gram: scale b by 1/Gram)
+  const double bscale = std::is_same<R, float>::value ? 1.0 / op->gram : 1.0;
+  k_cast_scale<R><<<nblk(n), 256, 0, st>>>(n, b_dev, bscale, w.b);
+  std::vector<double> rv;
+  info->total_iters = 0;
+  VOX_TRY(pgmres_dev<R>(op, pc, side, tol, maxit, info, &rv));
+  double relres;
+  VOX_TRY(true_relres<R>(op, &relres));
+  info->relres = relres;
+  info->flag = relres <= tol ? 0 : 1;
+  k_to_d2<R><<<nblk(n), 256, 0, st>>>(n, w.x, 1.0, x_dev);
+  op->launches += 2;
+  VOX_CUDA(cudaStreamSynchronize(st));
+  fill_resvec(info, rv);
+  return VOX_OK;
+}
+
+__global__ void k_axpy_d2_from(long long n, const float2* __restrict__ d, double s, double2* x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    x[i].x += s * (double)d[i].x;
+    x[i].y += s * (double)d[i].y;
+  }
+}
+
+// complex64 GMRES inside FP64 iterative refinement.
+static vox_status refined_entry(vox_op_s* op, vox_precond_s* pc, int side, const double2* b_dev,
+                                double tol, int restart, int maxit_inner, double inner_tol,
+                                int max_refine, double2* x_dev, vox_gmres_info* info) {
+  if (!op->has_d || !op->has_f) {
+    set_error("refined solve needs both complex128 and complex64 operator copies");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (restart < 1 || restart > kMaxRestart) {
+    set_error("restart must be in 1.." + std::to_string(kMaxRestart));
+    return VOX_ERR_BAD_ARG;
+  }
+  if (inner_tol <= 0) inner_tol = 1e-3;
+  if (max_refine < 1) max_refine = 10;
+  VOX_TRY(ensure_work<float>(op, restart));
+  if (!op->wd.V) VOX_TRY(ensure_work<double>(op, 1));
+  GmresWork<float>& wf = op->wf;
+  GmresWork<double>& wd = op->wd;
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  const int nb = nblk(n);
+  // FP64 state: x = 0, r = b
+  VOX_CUDA(cudaMemsetAsync(x_dev, 0, n * sizeof(double2), st));
+  VOX_CUDA(cudaMemcpyAsync(wd.b, b_dev, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  VOX_CUDA(cudaMemcpyAsync(wd.r, b_dev, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  k_norm2<double><<<kRedBlocks, kRedThreads, 0, st>>>(wd.st, wd.b, n, 3);
+  op->launches += 1;
+  double bn2;
+  VOX_TRY(read_scal<double>(op, 3, &bn2));
+  const double bn = std::sqrt(bn2);
+  info->total_iters = 0;
+  info->refinements = 0;
+  std::vector<double> rv;
+  if (bn == 0.0) {
+    info->flag = 0;
+    info->relres = 0;
+    fill_resvec(info, rv);
+    return VOX_OK;
+  }
+  double rel = 1.0;
+  int outer_total = 0, last_inner = 0;
+  for (int it = 0; it < max_refine && rel > tol; it++) {
+    const double rn = rel * bn;
+    // inner right-hand side: r / ||r|| in complex64 (operator copy is A/Gram)
+    k_cast_scale<float><<<nb, 256, 0, st>>>(n, wd.r, 1.0 / rn, wf.b);
+    vox_gmres_info ii{};
+    // tolerance relative to ||r||; never ask for less than what reaches tol
+    const double itol = std::min(0.5, std::max(inner_tol, 0.5 * tol * bn / rn));
+    VOX_TRY(pgmres_dev<float>(op, pc, side, itol, maxit_inner, &ii, &rv));
+    info->total_iters += ii.total_iters;
+    outer_total += ii.iter_outer;
+    last_inner = ii.iter_inner;
+    // x += (||r|| / Gram) * d   (d solves (A/Gram) d = r/||r||)
+    k_axpy_d2_from<<<nb, 256, 0, st>>>(n, wf.x, rn / op->gram, x_dev);
+    // r = b - A x in FP64
+    VOX_TRY(matvec<double>(op, MV_AN, x_dev, wd.w, st, nullptr));
+    k_sub<double><<<nb, 256, 0, st>>>(n, wd.b, wd.w, wd.r);
+    k_norm2<double><<<kRedBlocks, kRedThreads, 0, st>>>(wd.st, wd.r, n, 2);
+    op->launches += 7;
+    double r2;
+    VOX_TRY(read_scal<double>(op, 2, &r2));
+    rel = std::sqrt(r2) / bn;
+    info->refinements = it + 1;
+  }
+  info->relres = rel;
+  info->flag = rel <= tol ? 0 : 1;
+  info->iter_inner = last_inner;
+  info->iter_outer = outer_total;
+  fill_resvec(info, rv);
+  return VOX_OK;
+}
+
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_pgmres_device(vox_op_t op, vox_precond_t pc, int side, vox_prec prec,
+                             const void* b, int restart, double tol, int maxit, void* x,
+                             vox_gmres_info* info) {
+  if (!op || !b || !x) {
+    set_error("vox_pgmres_device: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  VOX_TRY(check_prec(op, prec));
+  DeviceGuard dg(op->device);
+  vox_gmres_info local{};
+  if (!info) info = &local;
+  auto t0 = std::chrono::steady_clock::now();
+  vox_status s = prec == VOX_C128
+                     ? pgmres_entry<double>(op, pc, side, (const double2*)b, restart, tol, maxit,
+                                            (double2*)x, info)
+                     : pgmres_entry<float>(op, pc, side, (const double2*)b, restart, tol, maxit,
+                                           (double2*)x, info);
+  info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return s;
+}
+
+vox_status vox_solve_refined_device(vox_op_t op, vox_precond_t pc, int side, const void* b,
+                                    double tol, int restart, int maxit_inner, double inner_tol,
+                                    int max_refine, void* x, vox_gmres_info* info) {
+  if (!op || !b || !x) {
+    set_error("vox_solve_refined_device: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  DeviceGuard dg(op->device);
+  vox_gmres_info local{};
+  if (!info) info = &local;
+  auto t0 = std::chrono::steady_clock::now();
+  vox_status s = refined_entry(op, pc, side, (const double2*)b, tol, restart, maxit_inner,
+                               inner_tol, max_refine, (double2*)x, info);
+  info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return s;
+}
+
+static vox_status host_solve(vox_op_t op, const double* b_re, const double* b_im, double* x_re,
+                             double* x_im, vox_gmres_info* info,
+                             const std::function<vox_status(const double2*, double2*)>& fn) {
+  if (!op || !b_re || !x_re) {
+    set_error("NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  DeviceGuard dg(op->device);
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  split_to_d2(b_re, b_im, n, op->h_in);
+  VOX_CUDA(cudaMemcpyAsync(op->d_in, op->h_in, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+  VOX_TRY(fn(op->d_in, op->d_out));
+  VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  d2_to_split(op->h_out, n, x_re, x_im);
+  if (info)
+    info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return VOX_OK;
+}
+
+vox_status vox_pgmres(vox_op_t op, vox_precond_t pc, int side, vox_prec prec, const double* b_re,
+                      const double* b_im, int restart, double tol, int maxit, double* x_re,
+                      double* x_im, vox_gmres_info* info) {
+  if (op) {
+    vox_status s = check_prec(op, prec);
+    if (s != VOX_OK) return s;
+  }
+  vox_gmres_info local{};
+  vox_gmres_info* inf = info ? info : &local;
+  return host_solve(op, b_re, b_im, x_re, x_im, inf, [&](const double2* b, double2* x) {
+    return prec == VOX_C128 ? pgmres_entry<double>(op, pc, side, b, restart, tol, maxit, x, inf)
+                            : pgmres_entry<float>(op, pc, side, b, restart, tol, maxit, x, inf);
+  });
+}
+
+vox_status vox_solve_refined(vox_op_t op, vox_precond_t pc, int side, const double* b_re,
+                             const double* b_im, double tol, int restart, int maxit_inner,
+                             double inner_tol, int max_refine, double* x_re, double* x_im,
+                             vox_gmres_info* info) {
+  vox_gmres_info local{};
+  vox_gmres_info* inf = info ? info : &local;
+  return host_solve(op, b_re, b_im, x_re, x_im, inf, [&](const double2* b, double2* x) {
+    return refined_entry(op, pc, side, b, tol, restart, maxit_inner, inner_tol, max_refine, x,
+                         inf);
+  });
+}
+
+vox_status vox_jvie_rhs(int L, int M, int N, const double* er_re, const double* er_im,
+                        const double* Einc_re, const double* Einc_im, double gram, double freq,
+                        const double* idx, long long n_idx, double* out_re, double* out_im) {
+  if (!er_re || !Einc_re || !idx || !out_re || L < 1 || M < 1 || N < 1) {
+    set_error("vox_jvie_rhs: bad argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  const double mu = 4e-7 * M_PI, co = 299792458.0;
+  const double eo = 1.0 / (co * co) / mu;
+  const double omega = 2.0 * M_PI * freq;
+  const long long V = (long long)L * M * N;
+  for (long long i = 0; i < n_idx; i++) {
+    const long long p = (long long)idx[i] - 1;
+    if (p < 0 || p >= 3 * V) {
+      set_error("vox_jvie_rhs: idx out of range");
+      return VOX_ERR_BAD_ARG;
+    }
+    const long long cell = p % V;
+    const double er_r = er_re[cell], er_i = er_im ? er_im[cell] : 0.0;
+    // tau = j omega eo (e_r - 1); Vrhs = Gram tau Einc / e_r
+    const double tr = -omega * eo * er_i, ti = omega * eo * (er_r - 1.0);
+    const double er = Einc_re[p], ei = Einc_im ? Einc_im[p] : 0.0;
+    double vr = gram * (tr * er - ti * ei), vi = gram * (tr * ei + ti * er);
+    const double dd = er_r * er_r + er_i * er_i;
+    out_re[i] = (vr * er_r + vi * er_i) / dd;
+    if (out_im) out_im[i] = (vi * er_r - vr * er_i) / dd;
+  }
+  return VOX_OK;
+}
+
+}  // extern "C"
+
+namespace vox {
+
+template <typename R>
+__global__ void k_fill(long long n, R v, Cx<R>* x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = mkc<R>(v, (R)0.5 * v);
+}
+
+// Average device time (ms) of each kernel of one GMRES iteration, measured with
+// CUDA events on the operator's stream: out[0..2] matvec (x-forward, plane,
+// x-inverse), out[3..5] preconditioner (x-forward, per-mode solve, x-inverse),
+// out[6..9] Gram-Schmidt (dots, update+dots, update+norm, scale) at basis size
+// kgs+1.  Entries that do not apply are 0.
+template <typename R>
+static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, int kgs, int reps,
+                                 double* out) {
+  VOX_TRY(ensure_work<R>(op, restart));
+  GmresWork<R>& w = work<R>(op);
+  OpBuffers<R>& b = bufs<R>(op);
+  const OpGeom& g = b.geo;
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  const size_t cs = sizeof(Cx<R>);
+  k_fill<R><<<nblk((long long)(restart + 1) * n), 256, 0, st>>>((long long)(restart + 1) * n,
+                                                               (R)1e-3, w.V);
+  k_fill<R><<<nblk(n), 256, 0, st>>>(n, (R)1e-3, w.w);
+  k_fill<R><<<nblk(n), 256, 0, st>>>(n, (R)1e-3, w.t);
+  cudaEvent_t e0, e1;
+  VOX_CUDA(cudaEventCreate(&e0));
+  VOX_CUDA(cudaEventCreate(&e1));
+  auto timeit = [&](auto&& launch) -> double {
+    launch();  // warm-up
+    VOX_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; r++) launch();
+    VOX_CUDA(cudaEventRecord(e1, st));
+    VOX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / reps;
+  };
+  for (int i = 0; i < 10; i++) out[i] = 0;
+  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3);
+  const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
+  out[0] = timeit([&] {
+    k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, w.V, op->vmap, b.Mc, MV_AN, b.T1,
+                                              nullptr);
+  });
+  out[1] = timeit([&] {
+    k_plane<R><<<g.Px, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, b.T1, b.fN,
+                                                 b.T2, nullptr);
+  });
+  out[2] = timeit([&] {
+    k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, w.V, b.Mr, b.Mc,
+                                              b.gram, scale, b.out_scale, MV_AN, w.w, nullptr);
+  });
+  if (pc) {
+    const PcGeom& pg = pc->g;
+    const int nb = (pg.n3 + pg.ybx - 1) / pg.ybx;
+    Cx<R>* T = pc_T<R>(pc, 0);
+    out[3] = timeit([&] {
+      k_pc_xfwd<R><<<nb, 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), w.V, op->vmap,
+                                                       T, nullptr);
+    });
+    out[4] = timeit([&] {
+      if (pc->lu)
+        k_pc_lu_solve<R><<<pg.L, 512, (size_t)pg.n3 * cs, st>>>(pg, pc_A<R>(pc), pc->piv, T,
+                                                                nullptr);
+      else
+        k_pc_gemv<R><<<pg.L * ((pg.n3 + 255) / 256), 256, (size_t)pg.n3 * cs, st>>>(
+            pg, pc_A<R>(pc), T, pc_T<R>(pc, 1), nullptr);
+    });
+    out[5] = timeit([&] {
+      k_pc_xinv<R><<<nb, 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), T, op->vmap,
+                                                       (R)(1.0 / pg.L), w.t, nullptr);
+    });
+  }
+  // Gram-Schmidt at basis size kgs+1 (done flag cleared before every launch)
+  const int k = std::min(kgs, restart - 1);
+  const int nb = nblk(n);
+  int zero = 0;
+  auto clear = [&] {
+    cudaMemcpyAsync(&w.st->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+  };
+  {
+    // state header with m and a huge tolerance so no iteration "converges"
+    std::vector<unsigned char> hdr(offsetof(GmresDev, resvec), 0);
+    GmresDev* init = reinterpret_cast<GmresDev*>(hdr.data());
+    init->m = restart;
+    init->tol_abs = -1.0;
+    VOX_CUDA(cudaMemcpyAsync(w.st, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
+    VOX_CUDA(cudaStreamSynchronize(st));
+  }
+  out[6] = timeit([&] { k_gs_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, k, w.V, n, w.w, n); });
+  out[7] = timeit([&] {
+    k_gs_update_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, k, w.V, n, w.w, n);
+  });
+  // update_norm sets done at the last column; time it at k < m-1 and clear after
+  double tn = 0;
+  for (int r = 0; r < reps + 1; r++) {
+    clear();
+    VOX_CUDA(cudaEventRecord(e0, st));
+    k_gs_update_norm<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, k, w.V, n, w.w, n);
+    VOX_CUDA(cudaEventRecord(e1, st));
+    VOX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0) tn += ms;
+  }
+  out[8] = tn / reps;
+  clear();
+  out[9] = timeit([&] {
+    k_gs_scale<R><<<nb, 256, 0, st>>>(w.st, w.V + (long long)(k + 1) * n, w.w, n);
+  });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  VOX_CUDA(cudaGetLastError());
+  VOX_CUDA(cudaStreamSynchronize(st));
+  return VOX_OK;
+}
+
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_op_set_stream(vox_op_t op, void* stream) {
+  if (!op) {
+    set_error("vox_op_set_stream: NULL operator");
+    return VOX_ERR_BAD_ARG;
+  }
+  op->stream = stream ? (cudaStream_t)stream : op->own_stream;
+  return VOX_OK;
+}
+
+vox_status vox_op_stats(vox_op_t op, long long* launches) {
+  if (!op || !launches) {
+    set_error("vox_op_stats: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *launches = op->launches;
+  return VOX_OK;
+}
+
+vox_status vox_profile_stages(vox_op_t op, vox_precond_t pc, vox_prec prec, int restart, int kgs,
+                              int reps, double* ms_out) {
+  if (!op || !ms_out || reps < 1 || restart < 1 || restart > kMaxRestart) {
+    set_error("vox_profile_stages: bad argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  VOX_TRY(check_prec(op, prec));
+  DeviceGuard dg(op->device);
+  return prec == VOX_C128 ? profile_stages<double>(op, pc, restart, kgs, reps, ms_out)
+                          : profile_stages<float>(op, pc, restart, kgs, reps, ms_out);
+}
+
+}  // extern "C"

@@ -1,0 +1,344 @@
+"""MATLAB-facing mirror of VoxPhoton's VIE hot path over libvox.
+
+Names, argument meaning and return values follow the reference functions:
+
+* ``Operator(...)``           -- the device-resident operator behind the
+  ``mv_AN_const(JIn0, fN, Mr, Mc, Gram, transp_flag, idx, GPU_flag)`` handle
+  (piecewise_constant/src_vie/src_mvp/mv_AN_const.m:1); the one-time upload of
+  JVIE_Solver_const.m:277-284.
+* ``mv_AN_const(...)``        -- one-shot call with the reference signature.
+* ``mv_L_const(...)``         -- mv_L_const.m:1.
+* ``Preconditioner.level1``   -- level_1_parallel_func_N.m:1 + Bragg_MOR_script.m:61-72.
+* ``chan_mvp_idx(...)``       -- chan_mvp_idx.m:2.
+* ``pgmres(...)``             -- pgmres.m:70, returning (x, flag, relres, iter, resvec).
+
+All compute runs in libvox (hand-written sm_100a CUDA); this module only
+marshals MATLAB-layout arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import weakref
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, fortran_flat, lib, split
+
+
+def _idx_array(idx):
+    a = np.ascontiguousarray(np.asarray(idx, dtype=np.float64).reshape(-1))
+    return a
+
+
+class Operator:
+    """Device-resident JVIE-II operator A = Gram*Mr - Mc*N (one per wavelength).
+
+    Give either ``fN`` (2L x 2M x 2N x 6, the circulant FFT from
+    getOPERATORS_SAM) or ``G`` (L x M x N x 6 Toeplitz, opToeplitz).
+    ``Mr=None`` means Mr == 1 (the JVIE-II form).
+    """
+
+    def __init__(self, Mc, Gram, idx, fN=None, G=None, Mr=None, precisions=("c128", "c64"),
+                 device=0):
+        Mc = np.asarray(Mc)
+        if Mc.ndim != 3:
+            raise ValueError("Mc must be L x M x N")
+        L, M, N = Mc.shape
+        self.shape = (L, M, N)
+        self.Gram = float(Gram)
+        self._keep = []
+        d = _lib.OpDesc()
+        d.L, d.M, d.N = L, M, N
+        if (fN is None) == (G is None):
+            raise ValueError("give exactly one of fN or G")
+        if fN is not None:
+            fN = np.asarray(fN)
+            d.LfN, d.MfN, d.NfN = fN.shape[:3]
+            re, im = split(fortran_flat(fN))
+            d.fN_re, d.fN_im = dptr(re), dptr(im)
+            self._keep += [re, im]
+        else:
+            G = np.asarray(G)
+            if G.shape != (L, M, N, 6):
+                raise ValueError("G must be L x M x N x 6")
+            re, im = split(fortran_flat(G))
+            d.G_re, d.G_im = dptr(re), dptr(im)
+            self._keep += [re, im]
+        if Mr is not None:
+            re, im = split(fortran_flat(Mr))
+            d.Mr_re, d.Mr_im = dptr(re), dptr(im)
+            self._keep += [re, im]
+        re, im = split(fortran_flat(Mc))
+        d.Mc_re, d.Mc_im = dptr(re), dptr(im)
+        self._keep += [re, im]
+        d.gram = self.Gram
+        ia = _idx_array(idx)
+        d.idx, d.n_idx = dptr(ia), ia.size
+        self._keep.append(ia)
+        d.precisions = (1 if "c128" in precisions else 0) | (2 if "c64" in precisions else 0)
+        d.device = device
+        h = ctypes.c_void_p()
+        check(lib().vox_op_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self._keep = []
+        self._pcs = weakref.WeakSet()
+        self.n = ia.size
+        self.idx = ia
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        px, py, pz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        n = ctypes.c_longlong()
+        check(lib().vox_op_info(self._h, ctypes.byref(px), ctypes.byref(py), ctypes.byref(pz),
+                                ctypes.byref(n)))
+        return {"Px": px.value, "Py": py.value, "Pz": pz.value, "n": n.value}
+
+    def close(self):
+        """Free the device operator (and the preconditioners built on it)."""
+        if getattr(self, "_h", None):
+            for pc in list(getattr(self, "_pcs", ())):
+                pc.close()
+            lib().vox_op_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _mv(self, fn, x, *pre):
+        re, im = split(x, self.n)
+        ore = np.empty(self.n)
+        oim = np.empty(self.n)
+        check(fn(self._h, *pre, dptr(re), dptr(im), dptr(ore), dptr(oim)))
+        return ore + 1j * oim
+
+    def mv_AN(self, JIn0, transp_flag="notransp", prec="c128"):
+        t = {"notransp": 0, "transp": 1}[transp_flag]
+        return self._mv(lib().vox_mv_AN, JIn0, t, _lib.PREC[prec])
+
+    def mv_L(self, JIn0, prec="c128"):
+        return self._mv(lib().vox_mv_L, JIn0, _lib.PREC[prec])
+
+    def __call__(self, JIn0):
+        return self.mv_AN(JIn0)
+
+    # ----------------------------------------------- device-resident calls
+    def set_stream(self, stream_ptr):
+        """Run on the caller's cudaStream_t (an int handle; 0 restores the op's)."""
+        check(lib().vox_op_set_stream(self._h, ctypes.c_void_p(stream_ptr or None)))
+
+    def launches(self):
+        v = ctypes.c_longlong()
+        check(lib().vox_op_stats(self._h, ctypes.byref(v)))
+        return v.value
+
+    def profile_stages(self, pc=None, prec="c64", restart=50, kgs=25, reps=20):
+        """Per-kernel device ms of one GMRES iteration (see vox_profile_stages)."""
+        out = np.zeros(10)
+        check(lib().vox_profile_stages(self._h, pc.handle if pc else None, _lib.PREC[prec],
+                                       restart, kgs, reps, dptr(out)))
+        names = ["mv_xfwd", "mv_plane", "mv_xinv", "pc_xfwd", "pc_solve", "pc_xinv",
+                 "gs_dots", "gs_update_dots", "gs_update_norm", "gs_scale"]
+        return dict(zip(names, out.tolist()))
+
+    def solve_refined_device(self, b_ptr, x_ptr, pc=None, side=None, tol=1e-5, restart=50,
+                             maxit_inner=20, inner_tol=1e-3, max_refine=10):
+        """vox_solve_refined_device on device pointers (interleaved complex128)."""
+        info = _lib.GmresInfo()
+        check(lib().vox_solve_refined_device(
+            self._h, pc.handle if pc else None, _lib.SIDE[side] if pc else 0,
+            ctypes.c_void_p(b_ptr), tol, restart, maxit_inner, inner_tol, max_refine,
+            ctypes.c_void_p(x_ptr), ctypes.byref(info)))
+        return info
+
+    def pgmres_device(self, b_ptr, x_ptr, pc=None, side=None, prec="c128", restart=50,
+                      tol=1e-5, maxit=20):
+        """vox_pgmres_device on device pointers (interleaved complex128 in/out)."""
+        info = _lib.GmresInfo()
+        check(lib().vox_pgmres_device(
+            self._h, pc.handle if pc else None, _lib.SIDE[side] if pc else 0, _lib.PREC[prec],
+            ctypes.c_void_p(b_ptr), restart, tol, maxit, ctypes.c_void_p(x_ptr),
+            ctypes.byref(info)))
+        return info
+
+
+def mv_AN_const(JIn0, fN, Mr, Mc, Gram, transp_flag, idx, GPU_flag=1, prec="c128"):
+    """mv_AN_const.m:1 with the reference's arguments (uploads fN each call;
+    keep an ``Operator`` for repeated products)."""
+    Mr_arg = None if np.all(np.asarray(Mr) == 1) else Mr
+    op = Operator(Mc, Gram, idx, fN=fN, Mr=Mr_arg, precisions=(prec,))
+    try:
+        return op.mv_AN(JIn0, transp_flag, prec)
+    finally:
+        op.close()
+
+
+def mv_L_const(JIn0, fN, r, Gram, idx, GPU_flag=1, prec="c128"):
+    """mv_L_const.m:1: (N - Gram) J at the positions idx."""
+    L, M, N = np.asarray(r).shape[:3]
+    op = Operator(np.ones((L, M, N)), Gram, idx, fN=fN, precisions=(prec,))
+    try:
+        return op.mv_L(JIn0, prec)
+    finally:
+        op.close()
+
+
+def face3_from_Mr(Mr):
+    """Bragg_MOR_script.m:64-66: face = (m-1)/m, m = real(mean over x of Mr)."""
+    Mr = np.asarray(Mr)
+    hey = np.real(Mr.sum(axis=0) / Mr.shape[0])
+    f = ((hey - 1) / hey).reshape(-1, order="F")
+    return np.ascontiguousarray(np.concatenate([f, f, f]), dtype=np.float64)
+
+
+class Preconditioner:
+    """Level-1 circulant preconditioner on the device (chan_mvp_idx)."""
+
+    def __init__(self, op: Operator, handle):
+        self.op = op
+        self._h = handle
+        op._pcs.add(self)
+
+    @classmethod
+    def level1(cls, op: Operator, G, Mr_mean_source):
+        """Build from the Toeplitz tensor G (L x M x N x 6) and the permittivity
+        Mr used for the x-averaged face factor (Bragg_MOR_script.m:61-72)."""
+        re, im = split(fortran_flat(G))
+        f3 = face3_from_Mr(Mr_mean_source)
+        h = ctypes.c_void_p()
+        check(lib().vox_precond_create_level1(op.handle, dptr(re), dptr(im), dptr(f3),
+                                              ctypes.byref(h)))
+        return cls(op, h)
+
+    @classmethod
+    def from_blocks(cls, op: Operator, inv_blocks):
+        """chan_mvp_idx with caller-supplied inverse blocks (list of L matrices)."""
+        B = np.stack([np.asarray(b) for b in inv_blocks])  # L x n3 x n3
+        flat = np.concatenate([fortran_flat(b) for b in B])
+        re, im = split(flat)
+        h = ctypes.c_void_p()
+        check(lib().vox_precond_create_blocks(op.handle, dptr(re), dptr(im), ctypes.byref(h)))
+        return cls(op, h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def apply(self, JIn, prec="c128"):
+        re, im = split(JIn, self.op.n)
+        ore = np.empty(self.op.n)
+        oim = np.empty(self.op.n)
+        check(lib().vox_precond_apply(self._h, _lib.PREC[prec], dptr(re), dptr(im), dptr(ore),
+                                      dptr(oim)))
+        return ore + 1j * oim
+
+    __call__ = apply
+
+    def close(self):
+        if getattr(self, "_h", None):
+            if getattr(self.op, "_h", None):
+                lib().vox_precond_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def chan_mvp_idx(inv_blocks, JIn, L, M, N, idx, op=None):
+    """chan_mvp_idx.m:2 (builds a temporary preconditioner from inv_blocks)."""
+    if op is None:
+        raise ValueError("an Operator on the same grid/idx is required for the index map")
+    pc = Preconditioner.from_blocks(op, inv_blocks)
+    try:
+        return pc.apply(JIn)
+    finally:
+        pc.close()
+
+
+def _info(resvec_cap):
+    info = _lib.GmresInfo()
+    buf = np.zeros(max(1, resvec_cap))
+    info.resvec = dptr(buf)
+    info.resvec_cap = buf.size
+    return info, buf
+
+
+def pgmres(A: Operator, b, restart=None, tol=None, maxit=None, L1=None, R1=None, prec="c128"):
+    """pgmres.m:70 on the device: returns (x, flag, relres, iter, resvec).
+
+    ``L1`` / ``R1`` are left / right preconditioners (``Preconditioner``)."""
+    restart = 50 if restart is None else int(restart)
+    tol = 1e-3 if tol is None else float(tol)
+    maxit = 10 if maxit is None else int(maxit)
+    if L1 is not None and R1 is not None:
+        raise ValueError("give at most one of L1 or R1")
+    pc = L1 if L1 is not None else R1
+    side = 1 if L1 is not None else (2 if R1 is not None else 0)
+    re, im = split(b, A.n)
+    xre = np.empty(A.n)
+    xim = np.empty(A.n)
+    info, buf = _info(restart * maxit + 1)
+    check(lib().vox_pgmres(A.handle, pc.handle if pc else None, side, _lib.PREC[prec], dptr(re),
+                           dptr(im), restart, tol, maxit, dptr(xre), dptr(xim),
+                           ctypes.byref(info)))
+    resvec = buf[:min(info.n_resvec, buf.size)].copy()
+    return (xre + 1j * xim, info.flag, info.relres, [info.iter_inner, info.iter_outer], resvec)
+
+
+def solve_refined(A: Operator, b, tol=1e-5, restart=50, maxit_inner=20, inner_tol=1e-3,
+                  max_refine=10, L1=None, R1=None):
+    """complex64 GMRES inside FP64 iterative refinement; returns (x, info dict)."""
+    pc = L1 if L1 is not None else R1
+    side = 1 if L1 is not None else (2 if R1 is not None else 0)
+    re, im = split(b, A.n)
+    xre = np.empty(A.n)
+    xim = np.empty(A.n)
+    info, buf = _info(restart * maxit_inner * max_refine + max_refine + 1)
+    check(lib().vox_solve_refined(A.handle, pc.handle if pc else None, side, dptr(re), dptr(im),
+                                  tol, restart, maxit_inner, inner_tol, max_refine, dptr(xre),
+                                  dptr(xim), ctypes.byref(info)))
+    return xre + 1j * xim, {
+        "flag": info.flag, "relres": info.relres, "iters": info.total_iters,
+        "refinements": info.refinements, "seconds": info.seconds,
+        "resvec": buf[:min(info.n_resvec, buf.size)].copy()}
+
+
+def jvie_rhs(e_r, Einc, Gram, freq, idx):
+    """JVIE_Solver_const.m:151-157 + :243-251: Vrhs at the positions idx."""
+    e_r = np.asarray(e_r)
+    L, M, N = e_r.shape
+    er_re, er_im = split(fortran_flat(e_r))
+    e_re, e_im = split(fortran_flat(Einc))
+    ia = _idx_array(idx)
+    ore = np.empty(ia.size)
+    oim = np.empty(ia.size)
+    check(lib().vox_jvie_rhs(L, M, N, dptr(er_re), dptr(er_im), dptr(e_re), dptr(e_im),
+                             float(Gram), float(freq), dptr(ia), ia.size, dptr(ore), dptr(oim)))
+    return ore + 1j * oim
+
+
+def assemble_toeplitz(shape3, ko, dx, nthreads=0):
+    """assembly_nop_const(r, ko, dx, 'DEMCEM') on the host (C++): G (L x M x N x 6)."""
+    L, M, N = shape3
+    V = L * M * N
+    re = np.empty(6 * V)
+    im = np.empty(6 * V)
+    check(lib().vox_assemble_toeplitz(L, M, N, float(ko), float(dx), int(nthreads), dptr(re),
+                                      dptr(im)))
+    return (re + 1j * im).reshape((L, M, N, 6), order="F")
+
+
+def singular_integrals(ko, dx, order=32):
+    """(ST, EAc, EAo, VAc, VAo) face-pair integrals of exp(-j ko R)/R."""
+    out = np.empty(10)
+    check(lib().vox_singular_integrals(float(ko), float(dx), int(order), dptr(out)))
+    return tuple(out[0::2] + 1j * out[1::2])
