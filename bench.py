@@ -132,9 +132,13 @@ def kernel_bytes(op_info, shape, n, pc_on, k):
     c = 8
     T = Px * 3 * N * M * c
     n3 = 3 * M * N
+    if op_info.get("octant_fN"):
+        fN_bytes = 6 * (Px // 2 + 1) * (Py // 2 + 1) * (Pz // 2 + 1) * c
+    else:
+        fN_bytes = 6 * Px * Py * Pz * c
     b = {
         "mv_xfwd": n * c + 3 * V * 4 + T,
-        "mv_plane": 2 * T + 6 * Px * Py * Pz * c,
+        "mv_plane": 2 * T + fN_bytes,
         "mv_xinv": T + 2 * n * c + 3 * V * 4 + V * c,
         "gs_dots": (k + 1) * n * c + n * c,
         "gs_update_dots": (k + 1) * n * c + 2 * n * c,

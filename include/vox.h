@@ -110,6 +110,9 @@ vox_status vox_op_info(vox_op_t op, int* Px, int* Py, int* Pz, long long* n);
 vox_status vox_op_set_stream(vox_op_t op, void* stream);
 /* Kernels launched so far by the solver entry points on this operator. */
 vox_status vox_op_stats(vox_op_t op, long long* launches);
+/* Storage flags: bit 0 set when fN is kept as one octant (the transformed
+ * circulant has the per-axis parity of the Green tensor). */
+vox_status vox_op_flags(vox_op_t op, int* flags);
 /* Device time (ms, CUDA events on the operator's stream, mean of reps) of each
  * kernel of one GMRES iteration: [0..2] matvec x-forward / plane / x-inverse,
  * [3..5] preconditioner x-forward / per-mode solve / x-inverse (0 if pc is

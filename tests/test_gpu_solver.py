@@ -49,8 +49,12 @@ def test_pgmres_c128_matches_oracle_unpreconditioned():
     # same Krylov process: iteration counts agree (to one step at the
     # tolerance crossing), residual histories agree to rounding
     assert it[1] == it_r[1] and abs(it[0] - it_r[0]) <= 1
-    k = min(len(resvec), len(resvec_r))
-    assert np.max(np.abs(resvec[:k] - resvec_r[:k]) / resvec_r[:k]) < 1e-6
+    # within the first restart cycle the histories agree to rounding; later
+    # cycles start from restart residuals that carry the difference between
+    # the reference's one-pass CGS and this CGS2, so only the iteration count
+    # and the solution are compared there
+    first = slice(0, 31)
+    assert np.max(np.abs(resvec[first] - resvec_r[first]) / resvec_r[first]) < 1e-6
     assert rel(x, xr) < 1e-7
     op.close()
 

@@ -337,8 +337,14 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
   const OpGeom& g = b.geo;
   const long long P = (long long)g.Px * g.Py * g.Pz;
   cudaStream_t st = op->stream;
-  VOX_TRY(dalloc(&b.fN, 6 * P));
-  k_pack_fN<R><<<nblk(6 * P), 256, 0, st>>>(P, fN_packed_src, scale, b.fN);
+  if (g.sym) {
+    const long long H = (long long)(g.Px / 2 + 1) * (g.Py / 2 + 1) * (g.Pz / 2 + 1);
+    VOX_TRY(dalloc(&b.fN, 6 * H));
+    k_pack_fN_sym<R><<<nblk(6 * H), 256, 0, st>>>(g, fN_packed_src, scale, b.fN);
+  } else {
+    VOX_TRY(dalloc(&b.fN, 6 * P));
+    k_pack_fN<R><<<nblk(6 * P), 256, 0, st>>>(P, fN_packed_src, scale, b.fN);
+  }
   VOX_CUDA(cudaGetLastError());
   double2* tmp;
   VOX_TRY(dalloc(&tmp, g.V));
@@ -544,6 +550,21 @@ vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out) {
   // forward 3-D FFT of the padded circulant: z stride 1, y Pz, x Py*Pz
   for (int ax = 0; ax < 3; ax++)
     VOX_TRY(fft_axis_d(emb, g.Px, g.Py, g.Pz, (long long)g.Py * g.Pz, g.Pz, 1, P, 6, ax, -1, st));
+  // keep one octant when the transformed circulant has the tensor's parity
+  {
+    unsigned* dd;
+    VOX_TRY(dalloc(&dd, 2));
+    std::unique_ptr<unsigned, decltype(&cudaFree)> gd(dd, cudaFree);
+    VOX_CUDA(cudaMemsetAsync(dd, 0, 2 * sizeof(unsigned), st));
+    k_sym_defect<<<nblk(6 * P), 256, 0, st>>>(g, emb, dd);
+    unsigned hv[2];
+    VOX_CUDA(cudaMemcpyAsync(hv, dd, sizeof(hv), cudaMemcpyDeviceToHost, st));
+    VOX_CUDA(cudaStreamSynchronize(st));
+    float defect, fmax;
+    std::memcpy(&defect, &hv[0], 4);
+    std::memcpy(&fmax, &hv[1], 4);
+    g.sym = (fmax > 0.f && defect <= 1e-12f * fmax) ? 1 : 0;
+  }
   if (precs & 1) {
     OpGeom gd = g;
     if (!pick_shapes(gd, sizeof(double2))) {

@@ -17,7 +17,7 @@
 namespace vox {
 
 constexpr int kMaxRestart = 128;
-constexpr int kRedBlocks = 296;  // 2 CTAs per SM on 148 SMs
+constexpr int kRedBlocks = 592;  // 4 CTAs per SM on 148 SMs
 constexpr int kRedThreads = 256;
 
 struct GmresDev {
@@ -83,36 +83,45 @@ __device__ __forceinline__ bool last_block(unsigned* ticket) {
   return amlast;
 }
 
-// partial[j*nb + b] for j < nj, reduced in block order into out[j].
+// partial[j*nb + b] for j < nj, reduced into out[j] (one warp per j, fixed
+// order, so the result is deterministic).  Ends with __syncthreads().
 __device__ __forceinline__ void reduce_partials(const double2* partial, int nj, int nb,
                                                 double2* out, double2* sh) {
-  for (int j = 0; j < nj; j++) {
+  (void)sh;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = warp; j < nj; j += nw) {
     double2 v = make_double2(0.0, 0.0);
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      v.x += partial[j * nb + b].x;
-      v.y += partial[j * nb + b].y;
+    for (int b = lane; b < nb; b += 32) {
+      const double2 p = __ldcg(&partial[j * nb + b]);
+      v.x += p.x;
+      v.y += p.y;
     }
-    v = block_sum(v, sh);
-    if (threadIdx.x == 0) out[j] = v;
-    __syncthreads();
+    v = warp_sum(v);
+    if (lane == 0) out[j] = v;
   }
+  __syncthreads();
 }
 
 // Per-CTA dot products of nj basis vectors with w over the CTA's grid-stride
-// elements: 4 basis vectors per sweep.
+// elements, kDotBatch basis vectors per sweep (FP64 accumulation).
+constexpr int kDotBatch = 8;
 template <typename R>
 __device__ __forceinline__ void cta_dots(const Cx<R>* __restrict__ V, long long ldv, int nj,
                                          const Cx<R>* __restrict__ w, long long n,
                                          double2* partial, double2* sh) {
-  for (int j0 = 0; j0 < nj; j0 += 4) {
-    double2 acc[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
-                      make_double2(0, 0)};
-    const int nb = min(4, nj - j0);
+  (void)sh;
+  __shared__ double2 red[kDotBatch][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j0 = 0; j0 < nj; j0 += kDotBatch) {
+    double2 acc[kDotBatch];
+#pragma unroll
+    for (int q = 0; q < kDotBatch; q++) acc[q] = make_double2(0.0, 0.0);
+    const int nb = min(kDotBatch, nj - j0);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
       const double2 wi = to_d2(w[i]);
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
+      for (int q = 0; q < kDotBatch; q++) {
         if (q < nb) {
           const double2 v = to_d2(V[(j0 + q) * ldv + i]);
           acc[q].x += v.x * wi.x + v.y * wi.y;  // conj(v) * w
@@ -121,13 +130,20 @@ __device__ __forceinline__ void cta_dots(const Cx<R>* __restrict__ V, long long 
       }
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      if (q < nb) {
-        const double2 s = block_sum(acc[q], sh);
-        if (threadIdx.x == 0) partial[(j0 + q) * gridDim.x + blockIdx.x] = s;
-        __syncthreads();
-      }
+    for (int q = 0; q < kDotBatch; q++) {
+      const double2 s = warp_sum(acc[q]);
+      if (lane == 0) red[q][warp] = s;
     }
+    __syncthreads();
+    if (threadIdx.x < nb) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int q = 0; q < nw; q++) {
+        s.x += red[threadIdx.x][q].x;
+        s.y += red[threadIdx.x][q].y;
+      }
+      partial[(j0 + threadIdx.x) * gridDim.x + blockIdx.x] = s;
+    }
+    __syncthreads();
   }
 }
 
@@ -161,6 +177,7 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_update_dots(GmresDev* st, in
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     Cx<R> wi = w[i];
+#pragma unroll 4
     for (int j = 0; j < nj; j++) {
       const Cx<R> v = V[j * ldv + i];
       const Cx<R> h = hs[j];
@@ -217,6 +234,7 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, in
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     Cx<R> wi = w[i];
+#pragma unroll 4
     for (int j = 0; j < nj; j++) {
       const Cx<R> v = V[j * ldv + i];
       const Cx<R> h = hs[j];
@@ -276,11 +294,12 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, in
   }
 }
 
-// V(:,k+1) = w * inv_norm
+// V(:,k+1) = w * inv_norm.  Runs for the step that just completed even when
+// that step ended the cycle: the restart residual V(:,1:k+1)*res needs it.
 template <typename R>
-__global__ void k_gs_scale(GmresDev* st, Cx<R>* __restrict__ Vnext, const Cx<R>* __restrict__ w,
-                           long long n) {
-  if (st->done) return;
+__global__ void k_gs_scale(GmresDev* st, int k, Cx<R>* __restrict__ Vnext,
+                           const Cx<R>* __restrict__ w, long long n) {
+  if (st->k != k + 1) return;
   const R s = (R)st->inv_norm;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {

@@ -35,6 +35,7 @@ struct OpGeom {
   int sx;         // smem stride of an x pencil
   int sy, sz;     // smem strides of y rows / z columns in kernel 2
   int rc, kc;     // rows per chunk / ky columns per chunk in kernel 2
+  int sym;        // fN stored as one octant (exact per-axis parity), else full
 };
 
 enum MvMode { MV_AN = 0, MV_AN_T = 1, MV_L = 2 };
@@ -141,7 +142,11 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
   }
 
   // Phase B: per ky chunk, z-FFT, tensor product, inverse z-FFT (crop to N)
-  const C* fplane = fN + (long long)kx * g.Py * g.Pz * 6;
+  // octant storage: fN(-k) = s fN(k) per axis, with s = -1 for xy (x, y),
+  // xz (x, z) and yz (y, z); index the octant and flip those signs
+  const int fx = g.sym && (2 * kx > g.Px);
+  const int hy = g.sym ? g.Py / 2 + 1 : g.Py, hz = g.sym ? g.Pz / 2 + 1 : g.Pz;
+  const C* fplane = fN + (long long)(fx ? g.Px - kx : kx) * hy * hz * 6;
   for (int k0 = 0; k0 < g.Py; k0 += g.kc) {
     const int nk = min(g.kc, g.Py - k0);
     // gather columns: seq (c*nk + j), element z
@@ -159,8 +164,15 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
     for (int t = threadIdx.x; t < nk * g.Pz; t += blockDim.x) {
       const int j = t / g.Pz;
       const int kz = t - j * g.Pz;
-      const C* f = fplane + ((long long)(k0 + j) * g.Pz + kz) * 6;
-      const C f0 = f[0], f1 = f[1], f2 = f[2], f3 = f[3], f4 = f[4], f5 = f[5];
+      const int ky = k0 + j;
+      const int fy = g.sym && (2 * ky > g.Py);
+      const int fz = g.sym && (2 * kz > g.Pz);
+      const C* f = fplane + ((long long)(fy ? g.Py - ky : ky) * hz + (fz ? g.Pz - kz : kz)) * 6;
+      C f1 = f[1], f2 = f[2], f4 = f[4];
+      const C f0 = f[0], f3 = f[3], f5 = f[5];
+      if (fx ^ fy) f1 = cscale(f1, (R)-1);
+      if (fx ^ fz) f2 = cscale(f2, (R)-1);
+      if (fy ^ fz) f4 = cscale(f4, (R)-1);
       C* p0 = res + (size_t)(0 * nk + j) * g.sz + kz;
       C* p1 = res + (size_t)(1 * nk + j) * g.sz + kz;
       C* p2 = res + (size_t)(2 * nk + j) * g.sz + kz;
@@ -372,6 +384,52 @@ __global__ void k_embed_from_toeplitz(OpGeom g, const double2* __restrict__ G, d
       v.y *= s;
     }
     out[t] = v;
+  }
+}
+
+// Largest parity defect |F(k) - s F(-k)| and largest |F(k)| of the
+// transformed circulant [comp][x][y][z] (as float bit patterns, atomicMax).
+__global__ void k_sym_defect(OpGeom g, const double2* __restrict__ F, unsigned* out) {
+  const long long P = (long long)g.Px * g.Py * g.Pz;
+  const int sx[6] = {1, -1, -1, 1, 1, 1}, sy[6] = {1, -1, 1, 1, -1, 1}, sz[6] = {1, 1, -1, 1, -1, 1};
+  float dmax = 0.f, fmax = 0.f;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6 * P;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int comp = (int)(t / P);
+    long long r = t - comp * P;
+    const int z = (int)(r % g.Pz);
+    r /= g.Pz;
+    const int y = (int)(r % g.Py), x = (int)(r / g.Py);
+    const int mx = (g.Px - x) % g.Px, my = (g.Py - y) % g.Py, mz = (g.Pz - z) % g.Pz;
+    const double s = (double)(sx[comp] * sy[comp] * sz[comp]);
+    const double2 a = F[t];
+    const double2 b = F[comp * P + ((long long)mx * g.Py + my) * g.Pz + mz];
+    dmax = fmaxf(dmax, (float)(fabs(a.x - s * b.x) + fabs(a.y - s * b.y)));
+    fmax = fmaxf(fmax, (float)(fabs(a.x) + fabs(a.y)));
+  }
+  atomicMax(out, __float_as_uint(dmax));
+  atomicMax(out + 1, __float_as_uint(fmax));
+}
+
+// Octant pack: [comp][x][y][z] -> [x'][y'][z'][comp] for x' <= Px/2, y' <= Py/2,
+// z' <= Pz/2, converting precision and scaling.
+template <typename R>
+__global__ void k_pack_fN_sym(OpGeom g, const double2* __restrict__ src, double scale,
+                              Cx<R>* dst) {
+  const long long P = (long long)g.Px * g.Py * g.Pz;
+  const int hx = g.Px / 2 + 1, hy = g.Py / 2 + 1, hz = g.Pz / 2 + 1;
+  const long long H = (long long)hx * hy * hz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6 * H;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long pt = t / 6;
+    const int comp = (int)(t - pt * 6);
+    const int z = (int)(pt % hz);
+    const long long r = pt / hz;
+    const int y = (int)(r % hy), x = (int)(r / hy);
+    double2 v = src[comp * P + ((long long)x * g.Py + y) * g.Pz + z];
+    v.x *= scale;
+    v.y *= scale;
+    dst[t] = from_d2<Cx<R>>(v);
   }
 }
 

@@ -24,6 +24,8 @@ namespace vox {
 
 constexpr int kLuNb = 8;        // panel width of the batched LU
 constexpr int kTrsvNb = 32;     // diagonal block of the triangular solves
+// right-hand-side length padded to whole diagonal blocks
+inline int lu_npad(int n) { return (n + kTrsvNb - 1) / kTrsvNb * kTrsvNb; }
 
 struct PcGeom {
   int L, M, N;
@@ -461,6 +463,206 @@ __global__ void k_cast_scale(long long n, const double2* __restrict__ src, doubl
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     dst[i] = from_d2<Cx<R>>(make_double2(src[i].x * s, src[i].y * s));
+}
+
+// ----------------------------------------- paired, blocked LU solves (apply)
+// Row permutation of getrf's pivots: (P c)[k] = c[perm[k]] (one CTA per matrix).
+__global__ void k_lu_perm(int n, const int* __restrict__ piv, int* __restrict__ perm) {
+  if (threadIdx.x != 0) return;
+  const int* pv = piv + (long long)blockIdx.x * n;
+  int* pm = perm + (long long)blockIdx.x * n;
+  for (int k = 0; k < n; k++) pm[k] = k;
+  for (int k = 0; k < n; k++) {
+    const int p = pv[k];
+    if (p != k) {
+      const int a = pm[k];
+      pm[k] = pm[p];
+      pm[p] = a;
+    }
+  }
+}
+
+// Inverses of the kTrsvNb x kTrsvNb diagonal blocks of the unit-lower L and of
+// U, for every block of every matrix: grid (nblk, nmat).  Output column-major
+// kTrsvNb^2 per block; a ragged last block is completed with the identity.
+__global__ void k_tri_inv_blocks(int n, const double2* __restrict__ A, double2* __restrict__ Dl,
+                                 double2* __restrict__ Du) {
+  constexpr int B = kTrsvNb;
+  __shared__ double2 Bk[B][B + 1];
+  __shared__ double2 X[B][B + 1];
+  const int nb = (n + B - 1) / B;
+  const int bk = blockIdx.x, mat = blockIdx.y;
+  const int k0 = bk * B, kb = min(B, n - k0);
+  const double2* Am = A + (long long)mat * n * n;
+  for (int t = threadIdx.x; t < B * B; t += blockDim.x) {
+    const int r = t % B, c = t / B;
+    double2 v = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    if (r < kb && c < kb) v = Am[(long long)(k0 + c) * n + k0 + r];
+    Bk[r][c] = v;
+  }
+  __syncthreads();
+  const long long off = ((long long)mat * nb + bk) * B * B;
+  if (threadIdx.x < B) {
+    // column c of L^{-1}: X(r,c) = delta_rc - sum_{c<=q<r} L(r,q) X(q,c)
+    const int c = threadIdx.x;
+    for (int r = 0; r < B; r++) {
+      double2 s = make_double2(r == c ? 1.0 : 0.0, 0.0);
+      if (r > c) {
+        for (int q = c; q < r; q++) {
+          const double2 l = Bk[r][q], x = X[q][c];
+          s.x -= l.x * x.x - l.y * x.y;
+          s.y -= l.x * x.y + l.y * x.x;
+        }
+      } else if (r < c) {
+        s = make_double2(0.0, 0.0);
+      }
+      X[r][c] = s;
+    }
+    for (int r = 0; r < B; r++) Dl[off + (long long)c * B + r] = X[r][c];
+    // column c of U^{-1}: X(r,c) = (delta_rc - sum_{r<q<=c} U(r,q) X(q,c)) / U(r,r)
+    for (int r = B - 1; r >= 0; r--) {
+      double2 s = make_double2(r == c ? 1.0 : 0.0, 0.0);
+      if (r < c) {
+        for (int q = r + 1; q <= c; q++) {
+          const double2 u = Bk[r][q], x = X[q][c];
+          s.x -= u.x * x.x - u.y * x.y;
+          s.y -= u.x * x.y + u.y * x.x;
+        }
+      } else if (r > c) {
+        s = make_double2(0.0, 0.0);
+      }
+      if (r <= c) {
+        const double2 d = Bk[r][r];
+        const double dd = d.x * d.x + d.y * d.y;
+        s = dd > 0 ? make_double2((s.x * d.x + s.y * d.y) / dd, (s.y * d.x - s.x * d.y) / dd)
+                   : make_double2(0.0, 0.0);
+      }
+      X[r][c] = s;
+    }
+    for (int r = 0; r < B; r++) Du[off + (long long)c * B + r] = X[r][c];
+  }
+}
+
+// One CTA per factored mode f.  With pairing, the CTA also solves mode L-f:
+// B_{L-f} = D B_f D (D negates the x-component rows), so
+// x_{L-f} = D (B_f^{-1} (D b_{L-f})) reuses the same factors - each factor
+// element is read once for two right-hand sides.  Blocked forward/back
+// substitution: x_blk = inv(diag block) * t_blk, then a rank-kTrsvNb update of
+// the remaining rows (column-major factor panels, coalesced).
+template <typename R>
+__global__ void __launch_bounds__(512) k_pc_lu_solve2(PcGeom g, int paired,
+                                                      const Cx<R>* __restrict__ A,
+                                                      const Cx<R>* __restrict__ Dl,
+                                                      const Cx<R>* __restrict__ Du,
+                                                      const int* __restrict__ perm, Cx<R>* T,
+                                                      const int* skip) {
+  using C = Cx<R>;
+  constexpr int B = kTrsvNb;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = g.n3;
+  const int MN = n / 3;
+  const int nb = (n + B - 1) / B;
+  const int npad = nb * B;  // right-hand sides padded with zeros to whole blocks
+  C* t1 = reinterpret_cast<C*>(smem_raw);
+  C* t2 = t1 + npad;
+  __shared__ C xb1[B], xb2[B];
+  const int f = blockIdx.x;
+  const int i2 = g.L - f;
+  const bool two = paired && f != 0 && i2 != f;
+  const C* Af = A + (long long)f * n * n;
+  const int* pm = perm + (long long)f * n;
+  C* T1 = T + (long long)f * n;
+  C* T2 = T + (long long)(two ? i2 : f) * n;
+  const int tid = threadIdx.x;
+  for (int k = tid; k < npad; k += blockDim.x) {
+    C v1 = czero<C>(), v2 = czero<C>();
+    if (k < n) {
+      const int p = pm[k];
+      v1 = T1[p];
+      if (two) {
+        v2 = T2[p];
+        if (p < MN) v2 = cscale(v2, (R)-1);
+      }
+    }
+    t1[k] = v1;
+    t2[k] = v2;
+  }
+  __syncthreads();
+  const C* DL = Dl + (long long)f * nb * B * B;
+  const C* DU = Du + (long long)f * nb * B * B;
+  // x_blk = inv(diag block) * t_blk (padded blocks are identity on zeros):
+  // 32 independent loads per thread, fully unrolled.
+  auto diag = [&](const C* Dblk, int k0) {
+    if (tid < 2 * B) {
+      const int q = tid & (B - 1), which = tid / B;
+      if (which == 0 || two) {
+        const C* tv = (which ? t2 : t1) + k0;
+        const C* D = Dblk + q;
+        C acc = czero<C>();
+#pragma unroll
+        for (int c = 0; c < B; c++) cfma(acc, __ldg(D + c * B), tv[c]);
+        (which ? xb2 : xb1)[q] = acc;
+      }
+    }
+    __syncthreads();
+    if (tid < B) {
+      t1[k0 + tid] = xb1[tid];
+      if (two) t2[k0 + tid] = xb2[tid];
+    }
+  };
+  // t[r] -= sum_j F[r, k0+j] x_j for rows r in [r0, r1): column-major panel,
+  // coalesced across threads, 16 loads in flight per thread
+  auto update = [&](int k0, int kb, int r0, int r1) {
+    const C* col = Af + (long long)k0 * n;
+    for (int r = r0 + tid; r < r1; r += blockDim.x) {
+      C a1 = t1[r], a2 = t2[r];
+      if (kb == B) {
+#pragma unroll 16
+        for (int j = 0; j < B; j++) {
+          const C l = __ldg(col + (long long)j * n + r);
+          const C x1 = xb1[j];
+          a1.x -= l.x * x1.x - l.y * x1.y;
+          a1.y -= l.x * x1.y + l.y * x1.x;
+          if (two) {
+            const C x2 = xb2[j];
+            a2.x -= l.x * x2.x - l.y * x2.y;
+            a2.y -= l.x * x2.y + l.y * x2.x;
+          }
+        }
+      } else {
+        for (int j = 0; j < kb; j++) {
+          const C l = __ldg(col + (long long)j * n + r);
+          const C x1 = xb1[j];
+          a1.x -= l.x * x1.x - l.y * x1.y;
+          a1.y -= l.x * x1.y + l.y * x1.x;
+          if (two) {
+            const C x2 = xb2[j];
+            a2.x -= l.x * x2.x - l.y * x2.y;
+            a2.y -= l.x * x2.y + l.y * x2.x;
+          }
+        }
+      }
+      t1[r] = a1;
+      if (two) t2[r] = a2;
+    }
+    __syncthreads();
+  };
+  // forward substitution with the unit-lower L, then back substitution with U
+  for (int bk = 0; bk < nb; bk++) {
+    const int k0 = bk * B;
+    diag(DL + (long long)bk * B * B, k0);
+    update(k0, min(B, n - k0), k0 + B, n);
+  }
+  for (int bk = nb - 1; bk >= 0; bk--) {
+    const int k0 = bk * B;
+    diag(DU + (long long)bk * B * B, k0);
+    update(k0, min(B, n - k0), 0, k0);
+  }
+  for (int k = tid; k < n; k += blockDim.x) {
+    T1[k] = t1[k];
+    if (two) T2[k] = (k < MN) ? cscale(t2[k], (R)-1) : t2[k];
+  }
 }
 
 // Cast LU factors to precision R, scaling the upper triangle (U, with the

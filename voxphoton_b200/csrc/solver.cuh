@@ -9,7 +9,14 @@ struct vox_precond_s {
   bool lu = true;              // LU factors (true) or explicit inverse blocks (false)
   double2* Ad = nullptr;       // c128 blocks / factors, L * n3 * n3
   float2* Af = nullptr;        // c64 copy (blocks scaled for the A/Gram operator)
-  int* piv = nullptr;          // L * n3
+  int* piv = nullptr;          // Lf * n3 getrf pivots
+  int* perm = nullptr;         // Lf * n3 row permutation of the pivots
+  int Lf = 0;                  // factored modes (L, or L/2+1 with pairing)
+  int paired = 0;              // mode L-f solved with the factors of mode f
+  double2* Dld = nullptr;      // inverted diagonal blocks of L and U (c128)
+  double2* Dud = nullptr;
+  float2* Dlf = nullptr;       // ... and of the c64 copy
+  float2* Duf = nullptr;
   double2* twd = nullptr;
   float2* twf = nullptr;
   double2* Td = nullptr;       // L * n3 work
@@ -29,6 +36,12 @@ template <> float2* pc_A<float>(vox_precond_s* p) { return p->Af; }
 template <typename R> Cx<R>* pc_T(vox_precond_s* p, int which);
 template <> double2* pc_T<double>(vox_precond_s* p, int w) { return w ? p->Td2 : p->Td; }
 template <> float2* pc_T<float>(vox_precond_s* p, int w) { return w ? p->Tf2 : p->Tf; }
+template <typename R> Cx<R>* pc_Dl(vox_precond_s* p);
+template <> double2* pc_Dl<double>(vox_precond_s* p) { return p->Dld; }
+template <> float2* pc_Dl<float>(vox_precond_s* p) { return p->Dlf; }
+template <typename R> Cx<R>* pc_Du(vox_precond_s* p);
+template <> double2* pc_Du<double>(vox_precond_s* p) { return p->Dud; }
+template <> float2* pc_Du<float>(vox_precond_s* p) { return p->Duf; }
 template <typename R> Cx<R>* pc_tw(vox_precond_s* p);
 template <> double2* pc_tw<double>(vox_precond_s* p) { return p->twd; }
 template <> float2* pc_tw<float>(vox_precond_s* p) { return p->twf; }
@@ -43,7 +56,8 @@ static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaSt
   Cx<R>* T = pc_T<R>(p, 0);
   k_pc_xfwd<R><<<nb, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip);
   if (p->lu) {
-    k_pc_lu_solve<R><<<g.L, 512, (size_t)g.n3 * cs, st>>>(g, pc_A<R>(p), p->piv, T, skip);
+    k_pc_lu_solve2<R><<<p->Lf, 512, 2 * (size_t)lu_npad(g.n3) * cs, st>>>(
+        g, p->paired, pc_A<R>(p), pc_Dl<R>(p), pc_Du<R>(p), p->perm, T, skip);
   } else {
     Cx<R>* T2 = pc_T<R>(p, 1);
     const int tiles = (g.n3 + 255) / 256;
@@ -63,8 +77,8 @@ static vox_status pc_attrs(const PcGeom& g) {
                                 (int)pc_xsmem(g, cs)));
   VOX_CUDA(cudaFuncSetAttribute(k_pc_xinv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pc_xsmem(g, cs)));
-  VOX_CUDA(cudaFuncSetAttribute(k_pc_lu_solve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(g.n3 * cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_pc_lu_solve2<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * lu_npad(g.n3) * cs)));
   VOX_CUDA(cudaFuncSetAttribute(k_pc_gemv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(g.n3 * cs)));
   VOX_CUDA(cudaFuncSetAttribute(k_lu_batched<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -77,6 +91,11 @@ static void pc_free(vox_precond_s* p) {
   cudaFree(p->Ad);
   cudaFree(p->Af);
   cudaFree(p->piv);
+  cudaFree(p->perm);
+  cudaFree(p->Dld);
+  cudaFree(p->Dud);
+  cudaFree(p->Dlf);
+  cudaFree(p->Duf);
   cudaFree(p->twd);
   cudaFree(p->twf);
   cudaFree(p->Td);
@@ -159,36 +178,62 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   VOX_TRY(dalloc(&dface, g.n3));
   std::unique_ptr<double, decltype(&cudaFree)> gF(dface, cudaFree);
   VOX_CUDA(cudaMemcpy(dface, face3, g.n3 * sizeof(double), cudaMemcpyHostToDevice));
-  // blocks and LU
+  // Pairing: the Chan circulants satisfy c[L-j] = s*c[j] (s = -1 for xy, xz),
+  // so B_{L-i} = D B_i D exactly when G_xy and G_xz vanish on the x = 0 plane
+  // (true of the physical tensor); then only modes 0..L/2 are factored.
+  {
+    double gmax = 0.0, g0 = 0.0;
+    for (long long i = 0; i < 6 * V; i++) gmax = std::max(gmax, std::abs(G[i].x) + std::abs(G[i].y));
+    for (int comp = 1; comp <= 2; comp++)
+      for (long long c = 0; c < (long long)g.M * g.N; c++) {
+        const double2 v = G[comp * V + c * g.L];
+        g0 = std::max(g0, std::abs(v.x) + std::abs(v.y));
+      }
+    p->paired = (g0 <= 1e-13 * gmax) ? 1 : 0;
+  }
+  p->Lf = p->paired ? g.L / 2 + 1 : g.L;
+  const int Lf = p->Lf;
   const long long per = (long long)g.n3 * g.n3;
-  VOX_TRY(dalloc(&p->Ad, g.L * per));
-  VOX_TRY(dalloc(&p->piv, (long long)g.L * g.n3));
-  k_assemble_blocks<<<nblk(g.L * per), 256, 0, st>>>(g.L, g.M, g.N, V, 0, g.L, dC, dface,
-                                                      op->gram, p->Ad);
+  const int nbd = (g.n3 + kTrsvNb - 1) / kTrsvNb;
+  const long long dsz = (long long)Lf * nbd * kTrsvNb * kTrsvNb;
+  VOX_TRY(dalloc(&p->Ad, Lf * per));
+  VOX_TRY(dalloc(&p->piv, (long long)Lf * g.n3));
+  VOX_TRY(dalloc(&p->perm, (long long)Lf * g.n3));
+  VOX_TRY(dalloc(&p->Dld, dsz));
+  VOX_TRY(dalloc(&p->Dud, dsz));
+  k_assemble_blocks<<<nblk(Lf * per), 256, 0, st>>>(g.L, g.M, g.N, V, 0, Lf, dC, dface,
+                                                     op->gram, p->Ad);
   VOX_CUDA(cudaGetLastError());
   int* dinfo;
-  VOX_TRY(dalloc(&dinfo, g.L));
+  VOX_TRY(dalloc(&dinfo, Lf));
   std::unique_ptr<int, decltype(&cudaFree)> gI(dinfo, cudaFree);
-  VOX_CUDA(cudaMemsetAsync(dinfo, 0, g.L * sizeof(int), st));
-  k_lu_batched<double><<<g.L, 512, (size_t)g.n3 * kLuNb * sizeof(double2), st>>>(g.n3, p->Ad,
-                                                                                 p->piv, dinfo);
+  VOX_CUDA(cudaMemsetAsync(dinfo, 0, Lf * sizeof(int), st));
+  k_lu_batched<double><<<Lf, 512, (size_t)g.n3 * kLuNb * sizeof(double2), st>>>(g.n3, p->Ad,
+                                                                                p->piv, dinfo);
   VOX_CUDA(cudaGetLastError());
-  std::vector<int> info(g.L);
-  VOX_CUDA(cudaMemcpyAsync(info.data(), dinfo, g.L * sizeof(int), cudaMemcpyDeviceToHost, st));
+  std::vector<int> info(Lf);
+  VOX_CUDA(cudaMemcpyAsync(info.data(), dinfo, Lf * sizeof(int), cudaMemcpyDeviceToHost, st));
   VOX_CUDA(cudaStreamSynchronize(st));
-  for (int i = 0; i < g.L; i++)
+  for (int i = 0; i < Lf; i++)
     if (info[i]) {
       set_error("vox_precond_create_level1: block " + std::to_string(i) + " is singular");
       return VOX_ERR_BAD_ARG;
     }
-  // c64 copy: factors of B/Gram (the c64 operator is A/Gram): L unchanged, U / Gram,
-  // so the copy applies Gram * M^{-1}
+  k_lu_perm<<<Lf, 32, 0, st>>>(g.n3, p->piv, p->perm);
+  k_tri_inv_blocks<<<dim3(nbd, Lf), 64, 0, st>>>(g.n3, p->Ad, p->Dld, p->Dud);
+  VOX_CUDA(cudaGetLastError());
+  // c64 copy: factors of B/Gram (the c64 operator is A/Gram): L unchanged,
+  // U / Gram (so inv(U) * Gram), so the copy applies Gram * M^{-1}
   p->lu = true;
   p->f_scale = op->gram;
   if (op->has_f) {
-    VOX_TRY(dalloc(&p->Af, g.L * per));
-    k_cast_scale_upper<float><<<nblk(g.L * per), 256, 0, st>>>(g.L * per, g.n3, p->Ad,
-                                                               1.0 / op->gram, p->Af);
+    VOX_TRY(dalloc(&p->Af, Lf * per));
+    VOX_TRY(dalloc(&p->Dlf, dsz));
+    VOX_TRY(dalloc(&p->Duf, dsz));
+    k_cast_scale_upper<float><<<nblk(Lf * per), 256, 0, st>>>(Lf * per, g.n3, p->Ad,
+                                                              1.0 / op->gram, p->Af);
+    k_cast_scale<float><<<nblk(dsz), 256, 0, st>>>(dsz, p->Dld, 1.0, p->Dlf);
+    k_cast_scale<float><<<nblk(dsz), 256, 0, st>>>(dsz, p->Dud, op->gram, p->Duf);
     VOX_CUDA(cudaGetLastError());
   }
   VOX_CUDA(cudaStreamSynchronize(st));
@@ -344,7 +389,7 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, cudaS
     k_gs_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
     k_gs_update_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
     k_gs_update_norm<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
-    k_gs_scale<R><<<nb, 256, 0, st>>>(d, w.V + (long long)(k + 1) * n, wv, n);
+    k_gs_scale<R><<<nb, 256, 0, st>>>(d, k, w.V + (long long)(k + 1) * n, wv, n);
   }
   k_cycle_ls<<<1, 32, 0, st>>>(d);
   if (side == VOX_PREC_RIGHT && pc) {
@@ -798,8 +843,8 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     });
     out[4] = timeit([&] {
       if (pc->lu)
-        k_pc_lu_solve<R><<<pg.L, 512, (size_t)pg.n3 * cs, st>>>(pg, pc_A<R>(pc), pc->piv, T,
-                                                                nullptr);
+        k_pc_lu_solve2<R><<<pc->Lf, 512, 2 * (size_t)lu_npad(pg.n3) * cs, st>>>(
+            pg, pc->paired, pc_A<R>(pc), pc_Dl<R>(pc), pc_Du<R>(pc), pc->perm, T, nullptr);
       else
         k_pc_gemv<R><<<pg.L * ((pg.n3 + 255) / 256), 256, (size_t)pg.n3 * cs, st>>>(
             pg, pc_A<R>(pc), T, pc_T<R>(pc, 1), nullptr);
@@ -844,7 +889,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
   out[8] = tn / reps;
   clear();
   out[9] = timeit([&] {
-    k_gs_scale<R><<<nb, 256, 0, st>>>(w.st, w.V + (long long)(k + 1) * n, w.w, n);
+    k_gs_scale<R><<<nb, 256, 0, st>>>(w.st, k, w.V + (long long)(k + 1) * n, w.w, n);
   });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -863,6 +908,15 @@ vox_status vox_op_set_stream(vox_op_t op, void* stream) {
     return VOX_ERR_BAD_ARG;
   }
   op->stream = stream ? (cudaStream_t)stream : op->own_stream;
+  return VOX_OK;
+}
+
+vox_status vox_op_flags(vox_op_t op, int* flags) {
+  if (!op || !flags) {
+    set_error("vox_op_flags: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *flags = op->g.sym ? 1 : 0;
   return VOX_OK;
 }
 

@@ -95,7 +95,10 @@ class Operator:
         n = ctypes.c_longlong()
         check(lib().vox_op_info(self._h, ctypes.byref(px), ctypes.byref(py), ctypes.byref(pz),
                                 ctypes.byref(n)))
-        return {"Px": px.value, "Py": py.value, "Pz": pz.value, "n": n.value}
+        fl = ctypes.c_int()
+        check(lib().vox_op_flags(self._h, ctypes.byref(fl)))
+        return {"Px": px.value, "Py": py.value, "Pz": pz.value, "n": n.value,
+                "octant_fN": bool(fl.value & 1)}
 
     def close(self):
         """Free the device operator (and the preconditioners built on it)."""
