@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--precond", default="none", choices=["none", "level1"])
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--restart", type=int, default=50)
+    ap.add_argument("--inner-tol", type=float, default=0.0,
+                    help="complex64 inner GMRES tolerance (0: aim at the target directly)")
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -124,7 +126,7 @@ def build_problem(name):
     return p, G, idx, b, t_asm
 
 
-def kernel_bytes(op_info, shape, n, pc_on, k):
+def kernel_bytes(op_info, shape, n, pc_info, k):
     """Algorithmic bytes per launch of each stage, complex64 (8 B per value)."""
     L, M, N = shape
     V = L * M * N
@@ -145,9 +147,14 @@ def kernel_bytes(op_info, shape, n, pc_on, k):
         "gs_update_norm": (k + 1) * n * c + 2 * n * c,
         "gs_scale": 2 * n * c,
     }
-    if pc_on:
+    if pc_info:
+        # factors of the factored modes (each read once for both paired modes),
+        # the inverted 32x32 diagonal blocks, the transformed vectors in and out
+        nf, ld = pc_info["n_factored"], pc_info["ld"]
+        nblk = ld // 32
         b["pc_xfwd"] = n * c + 3 * V * 4 + L * n3 * c
-        b["pc_solve"] = L * n3 * n3 * c + 2 * L * n3 * c + L * n3 * 4
+        b["pc_solve"] = nf * ld * ld * c + 2 * nf * nblk * 32 * 32 * c + 2 * L * n3 * c \
+            + nf * n3 * 4
         b["pc_xinv"] = L * n3 * c + 3 * V * 4 + n * c
     return b
 
@@ -259,7 +266,8 @@ def main():
     def solve_mixed():
         return op.solve_refined_device(b_dev.data_ptr(), x_dev.data_ptr(), pc=pc, side=side,
                                        tol=args.tol, restart=args.restart,
-                                       maxit_inner=maxit_inner, inner_tol=1e-3, max_refine=10)
+                                       maxit_inner=maxit_inner, inner_tol=args.inner_tol,
+                                       max_refine=10)
 
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -323,7 +331,8 @@ def main():
         def host_solve():
             _lib.check(lib.vox_solve_refined(
                 op.handle, pc.handle if pc else None, 1 if pc else 0, _lib.dptr(bre),
-                _lib.dptr(bim), args.tol, args.restart, maxit_inner, 1e-3, 10, _lib.dptr(xre),
+                _lib.dptr(bim), args.tol, args.restart, maxit_inner, args.inner_tol, 10,
+                _lib.dptr(xre),
                 _lib.dptr(xim), ctypes.byref(inf)))
         host_solve()
         torch.cuda.synchronize()
@@ -344,7 +353,7 @@ def main():
     # roofline of the dominant kernel, from live CUDA-event timing of each stage
     k_avg = max(1, min(args.restart - 1, int(np.mean(iters) // 2) if iters else 25))
     stages = op.profile_stages(pc, "c64", restart=args.restart, kgs=min(k_avg, 25), reps=20)
-    nbytes = kernel_bytes(op.info(), p.shape, n, pc is not None, min(k_avg, 25))
+    nbytes = kernel_bytes(op.info(), p.shape, n, pc.info() if pc else None, min(k_avg, 25))
     dom = max((k for k in nbytes if stages.get(k, 0) > 0), key=lambda k: stages[k])
     peak, peak_kind = peaks()
     achieved = nbytes[dom] / (stages[dom] * 1e-3) / 1e9

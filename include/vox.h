@@ -143,6 +143,10 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
 vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const double* blk_im,
                                      vox_precond_t* out);
 void vox_precond_destroy(vox_precond_t p);
+/* Factored modes (L, or L/2+1 when modes L-i reuse the factors of mode i),
+ * the factor leading dimension, and whether the blocks are LU factors (1) or
+ * caller-supplied explicit inverses (0). */
+vox_status vox_precond_info(vox_precond_t p, int* n_factored, int* ld, int* is_lu);
 /* mvp = chan_mvp_idx(inv_blocks, JIn, L, M, N, idx), host buffers of length n_idx. */
 vox_status vox_precond_apply(vox_precond_t p, vox_prec prec, const double* in_re,
                              const double* in_im, double* out_re, double* out_im);
@@ -155,7 +159,8 @@ vox_status vox_pgmres(vox_op_t op, vox_precond_t pc, int side, vox_prec prec, co
 /* complex64 GMRES (matvec, preconditioner, Krylov basis in FP32; inner
  * products, norms and Givens in FP64) inside FP64 iterative refinement:
  * repeat { r = b - A x (FP64); d = GMRES_c64(A, r/|r|, inner_tol); x += |r| d }
- * until ||b - A x|| / ||b|| <= tol.  inner_tol <= 0 picks 1e-3. */
+ * until ||b - A x|| / ||b|| <= tol.  inner_tol <= 0 aims each inner solve at
+ * the remaining target directly (0.3 * tol * ||b|| / ||r||). */
 vox_status vox_solve_refined(vox_op_t op, vox_precond_t pc, int side, const double* b_re,
                              const double* b_im, double tol, int restart, int maxit_inner,
                              double inner_tol, int max_refine, double* x_re, double* x_im,

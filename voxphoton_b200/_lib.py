@@ -112,6 +112,9 @@ SIGNATURES = [
     ("vox_op_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("vox_op_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("vox_op_flags", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    ("vox_precond_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]),
     ("vox_profile_stages", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]),
 ]

@@ -196,10 +196,19 @@ __device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restri
   const int nR = n / R;
   const int total = nseq * nR;
   const int twstep = n / (Ns * R);
+  // butterfly t = b*nR + j, j = jq*Ns + k: start from t = tid and advance by
+  // nthr with carries, so the loop body has no integer division
+  const int nq = nR / Ns;
+  int b = tid / nR;
+  const int j0 = tid - b * nR;
+  int jq = j0 / Ns;
+  int k = j0 - jq * Ns;
+  const int db = nthr / nR;
+  const int dj = nthr - db * nR;
+  const int dq = dj / Ns;
+  const int dk = dj - dq * Ns;
   for (int t = tid; t < total; t += nthr) {
-    const int b = t / nR;
-    const int j = t - b * nR;
-    const int k = j % Ns;
+    const int j = jq * Ns + k;
     const C* s = src + (size_t)b * sstride;
     C* d = dst + (size_t)b * sstride;
     C v[R];
@@ -210,9 +219,20 @@ __device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restri
       for (int r = 1; r < R; r++) v[r] = cmul(v[r], tw_get(tw, r * k * twstep, sign));
     }
     dft_small<R>(v, sign, tw, nR);
-    const int idxD = (j / Ns) * Ns * R + k;
+    const int idxD = jq * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; r++) d[idxD + r * Ns] = v[r];
+    k += dk;
+    jq += dq;
+    b += db;
+    if (k >= Ns) {
+      k -= Ns;
+      jq++;
+    }
+    if (jq >= nq) {
+      jq -= nq;
+      b++;
+    }
   }
 }
 

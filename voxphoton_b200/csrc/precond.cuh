@@ -253,7 +253,7 @@ __global__ void k_chan(int L, long long V, const double2* __restrict__ G, double
 
 // Dense block of mode i (column-major n3 x n3) from the x-transformed Chan
 // circulants Cf [comp][z][y][x]; B = gram*I - face3 .* circ.
-__global__ void k_assemble_blocks(int L, int M, int N, long long V, int i0, int nmodes,
+__global__ void k_assemble_blocks(int L, int M, int N, long long V, int i0, int nmodes, int ld,
                                   const double2* __restrict__ Cf, const double* __restrict__ face3,
                                   double gram, double2* __restrict__ B) {
   const int MN = M * N, n3 = 3 * MN;
@@ -300,21 +300,21 @@ __global__ void k_assemble_blocks(int L, int M, int N, long long V, int i0, int 
     const double f = face3[row];
     double2 o = make_double2(-f * v.x, -f * v.y);
     if (row == col) o.x += gram;
-    B[(long long)im * per + e] = o;
+    B[(long long)im * ld * ld + (long long)col * ld + row] = o;
   }
 }
 
 // Batched LU with partial pivoting, one CTA per matrix (column-major n x n).
 // piv[k] = 0-based row swapped with row k at step k (LAPACK getrf order).
 template <typename R>
-__global__ void __launch_bounds__(512) k_lu_batched(int n, Cx<R>* A, int* piv, int* info) {
+__global__ void __launch_bounds__(512) k_lu_batched(int n, int ld, Cx<R>* A, int* piv, int* info) {
   using C = Cx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* P = reinterpret_cast<C*>(smem_raw);  // panel: (n) x kLuNb, column-major, ld = n
   __shared__ int s_piv[kLuNb];
   __shared__ R s_best[32];
   __shared__ int s_bidx[32];
-  C* Ai = A + (long long)blockIdx.x * n * n;
+  C* Ai = A + (long long)blockIdx.x * ld * ld;  // column-major, leading dimension ld
   int* pv = piv + (long long)blockIdx.x * n;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k0 = 0; k0 < n; k0 += kLuNb) {
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(512) k_lu_batched(int n, Cx<R>* A, int* piv, i
     // load panel rows k0..n-1, columns k0..k0+kb-1
     for (int t = threadIdx.x; t < rows * kb; t += blockDim.x) {
       const int j = t / rows, r = t - j * rows;
-      P[(size_t)j * n + r] = Ai[(long long)(k0 + j) * n + k0 + r];
+      P[(size_t)j * n + r] = Ai[(long long)(k0 + j) * ld + k0 + r];
     }
     __syncthreads();
     for (int j = 0; j < kb; j++) {
@@ -395,12 +395,12 @@ __global__ void __launch_bounds__(512) k_lu_batched(int n, Cx<R>* A, int* piv, i
     // write the panel back
     for (int t = threadIdx.x; t < rows * kb; t += blockDim.x) {
       const int j = t / rows, r = t - j * rows;
-      Ai[(long long)(k0 + j) * n + k0 + r] = P[(size_t)j * n + r];
+      Ai[(long long)(k0 + j) * ld + k0 + r] = P[(size_t)j * n + r];
     }
     // row swaps on the columns outside the panel
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
       if (c >= k0 && c < k0 + kb) continue;
-      C* colp = Ai + (long long)c * n;
+      C* colp = Ai + (long long)c * ld;
       for (int j = 0; j < kb; j++) {
         const int pr = k0 + s_piv[j];
         if (pr != k0 + j) {
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(512) k_lu_batched(int n, Cx<R>* A, int* piv, i
     __syncthreads();
     // U12 = L11^{-1} A12 and trailing update A22 -= L21 U12, one column per thread
     for (int c = k0 + kb + threadIdx.x; c < n; c += blockDim.x) {
-      C* colp = Ai + (long long)c * n;
+      C* colp = Ai + (long long)c * ld;
       C u[kLuNb];
 #pragma unroll
       for (int j = 0; j < kLuNb; j++) u[j] = (j < kb) ? colp[k0 + j] : czero<C>();
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(512) k_lu_batched(int n, Cx<R>* A, int* piv, i
     // trailing update, threads over (row) inside column sweeps: coalesced rows
     const int r0 = k0 + kb;
     for (int c = r0 + warp; c < n; c += nw) {
-      C* colp = Ai + (long long)c * n;
+      C* colp = Ai + (long long)c * ld;
       C u[kLuNb];
 #pragma unroll
       for (int j = 0; j < kLuNb; j++) u[j] = (j < kb) ? colp[k0 + j] : czero<C>();
@@ -485,19 +485,19 @@ __global__ void k_lu_perm(int n, const int* __restrict__ piv, int* __restrict__ 
 // Inverses of the kTrsvNb x kTrsvNb diagonal blocks of the unit-lower L and of
 // U, for every block of every matrix: grid (nblk, nmat).  Output column-major
 // kTrsvNb^2 per block; a ragged last block is completed with the identity.
-__global__ void k_tri_inv_blocks(int n, const double2* __restrict__ A, double2* __restrict__ Dl,
-                                 double2* __restrict__ Du) {
+__global__ void k_tri_inv_blocks(int n, int ld, const double2* __restrict__ A,
+                                 double2* __restrict__ Dl, double2* __restrict__ Du) {
   constexpr int B = kTrsvNb;
   __shared__ double2 Bk[B][B + 1];
   __shared__ double2 X[B][B + 1];
   const int nb = (n + B - 1) / B;
   const int bk = blockIdx.x, mat = blockIdx.y;
   const int k0 = bk * B, kb = min(B, n - k0);
-  const double2* Am = A + (long long)mat * n * n;
+  const double2* Am = A + (long long)mat * ld * ld;
   for (int t = threadIdx.x; t < B * B; t += blockDim.x) {
     const int r = t % B, c = t / B;
     double2 v = make_double2(r == c ? 1.0 : 0.0, 0.0);
-    if (r < kb && c < kb) v = Am[(long long)(k0 + c) * n + k0 + r];
+    if (r < kb && c < kb) v = Am[(long long)(k0 + c) * ld + k0 + r];
     Bk[r][c] = v;
   }
   __syncthreads();
@@ -659,6 +659,248 @@ __global__ void __launch_bounds__(512) k_pc_lu_solve2(PcGeom g, int paired,
     diag(DU + (long long)bk * B * B, k0);
     update(k0, min(B, n - k0), 0, k0);
   }
+  for (int k = tid; k < n; k += blockDim.x) {
+    T1[k] = t1[k];
+    if (two) T2[k] = (k < MN) ? cscale(t2[k], (R)-1) : t2[k];
+  }
+}
+
+// ------------------------------------------ streamed LU solves (the apply)
+// The factors are static, so their 32 x 32 tiles are streamed through a ring
+// of shared-memory slots with cp.async, kRing-1 tiles in flight, in exactly
+// the order the substitution consumes them; only the arithmetic waits on the
+// dependency chain.  Tile order: forward [Dl(k), L(c,k) for c > k] for
+// k = 0..nb-1, then backward [Du(k), U(c,k) for c < k] for k = nb-1..0.
+// Factor storage is padded to ld = nb*32 (zero rows/columns), so every tile
+// column is 32 contiguous, 16-byte aligned values.
+constexpr int kTileLd = 36;  // smem column stride of a tile (bank-conflict free)
+
+template <typename R> struct RingDepth;
+// ring depth: 4 slots keep 3 tiles in flight and fit 4 CTAs (c64) per SM, so
+// up to 592 factored modes run in a single wave on 148 SMs
+template <> struct RingDepth<float> { static constexpr int value = 4; };
+template <> struct RingDepth<double> { static constexpr int value = 3; };
+
+template <typename R>
+constexpr size_t lu_stream_smem(int npad) {
+  return (size_t)RingDepth<R>::value * kTrsvNb * kTileLd * sizeof(Cx<R>) +
+         2 * (size_t)npad * sizeof(Cx<R>);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Position in the tile sequence: phase 0 forward / 1 backward, block column
+// k, block row c (c = -1: the inverted diagonal block).
+struct TileIt {
+  int phase, k, c;
+};
+__device__ __forceinline__ void tile_next(TileIt& it, int nb) {
+  if (it.phase == 0) {
+    const int c = (it.c < 0) ? it.k + 1 : it.c + 1;
+    if (c < nb) {
+      it.c = c;
+    } else if (it.k + 1 < nb) {
+      it.k++;
+      it.c = -1;
+    } else {
+      it.phase = 1;
+      it.k = nb - 1;
+      it.c = -1;
+    }
+  } else {
+    const int c = it.c + 1;
+    if (c < it.k) {
+      it.c = c;
+    } else {
+      it.k--;
+      it.c = -1;
+    }
+  }
+}
+
+// Number of tiles per mode in consumption order, and the (phase, k, c) of
+// tile i (closed-form group search, O(nb)).
+__host__ __device__ inline int lu_tiles(int nb) { return nb * (nb + 1); }
+__device__ inline TileIt tile_at(int i, int nb) {
+  TileIt it;
+  const int half = nb * (nb + 1) / 2;
+  if (i < half) {
+    int k = 0, start = 0;
+    while (i >= start + (nb - k)) {
+      start += nb - k;
+      k++;
+    }
+    it.phase = 0;
+    it.k = k;
+    it.c = (i == start) ? -1 : k + (i - start);
+  } else {
+    int i2 = i - half, k = nb - 1, start = 0;
+    while (i2 >= start + (k + 1)) {
+      start += k + 1;
+      k--;
+    }
+    it.phase = 1;
+    it.k = k;
+    it.c = (i2 == start) ? -1 : (i2 - start - 1);
+  }
+  return it;
+}
+
+// Repack LU factors (ld-padded, column-major, c128) and the inverted diagonal
+// blocks into per-mode tile streams in consumption order: tile i of mode f at
+// out[(f * lu_tiles(nb) + i) * 1024], each 32 x 32 column-major.  U tiles and
+// inverted U diagonal blocks are scaled by su (the c64 copy holds factors of
+// B/Gram: U/Gram and Gram*inv(U_kk)).  grid (lu_tiles(nb), Lf).
+template <typename R>
+__global__ void k_tile_pack(int nb, int ld, const double2* __restrict__ A,
+                            const double2* __restrict__ Dl, const double2* __restrict__ Du,
+                            double su_panel, double su_diag, Cx<R>* __restrict__ out) {
+  constexpr int B = kTrsvNb;
+  const int i = blockIdx.x, f = blockIdx.y;
+  const TileIt it = tile_at(i, nb);
+  Cx<R>* o = out + ((long long)f * lu_tiles(nb) + i) * B * B;
+  for (int e = threadIdx.x; e < B * B; e += blockDim.x) {
+    const int j = e / B, q = e - j * B;
+    double2 v;
+    double s = 1.0;
+    if (it.c < 0) {
+      const double2* D = (it.phase == 0 ? Dl : Du) + ((long long)f * nb + it.k) * B * B;
+      v = D[e];
+      if (it.phase == 1) s = su_diag;
+    } else {
+      v = A[(long long)f * ld * ld + (long long)(it.k * B + j) * ld + it.c * B + q];
+      if (it.phase == 1) s = su_panel;
+    }
+    o[e] = from_d2<Cx<R>>(make_double2(v.x * s, v.y * s));
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_pc_lu_stream(PcGeom g, int paired,
+                                                      const Cx<R>* __restrict__ tiles,
+                                                      const int* __restrict__ perm, Cx<R>* T,
+                                                      const int* skip) {
+  using C = Cx<R>;
+  constexpr int B = kTrsvNb;
+  constexpr int S = RingDepth<R>::value;
+  constexpr int SLOT = B * kTileLd;
+  constexpr int PPC = B * (int)sizeof(C) / 16;  // 16-byte pieces per tile column
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* ring = reinterpret_cast<C*>(smem_raw);
+  const int n = g.n3;
+  const int MN = n / 3;
+  const int nb = (n + B - 1) / B;
+  const int npad = nb * B;
+  C* t1 = ring + S * SLOT;
+  C* t2 = t1 + npad;
+  __shared__ C xb[2][B];
+  const int f = blockIdx.x;
+  const int i2 = g.L - f;
+  const bool two = paired && f != 0 && i2 != f;
+  const int total = lu_tiles(nb);
+  const C* tf = tiles + (long long)f * total * B * B;  // this mode's tile stream
+  const int* pm = perm + (long long)f * n;
+  C* T1 = T + (long long)f * n;
+  C* T2 = T + (long long)(two ? i2 : f) * n;
+  const int tid = threadIdx.x;
+
+  // tile i is 32*32 contiguous values: coalesced 16-byte pieces
+  auto issue = [&](int i, C* slot) {
+    const C* src = tf + (long long)i * B * B;
+    constexpr int per = 16 / (int)sizeof(C);
+    for (int p = tid; p < B * PPC; p += blockDim.x) {
+      const int j = p / PPC, q = p - j * PPC;
+      cp_async16(slot + j * kTileLd + q * per, src + j * B + q * per);
+    }
+  };
+
+  // right-hand sides: t = P (D b) for the paired mode
+  for (int k = tid; k < npad; k += blockDim.x) {
+    C v1 = czero<C>(), v2 = czero<C>();
+    if (k < n) {
+      const int p = pm[k];
+      v1 = T1[p];
+      if (two) {
+        v2 = T2[p];
+        if (p < MN) v2 = cscale(v2, (R)-1);
+      }
+    }
+    t1[k] = v1;
+    t2[k] = v2;
+  }
+
+  TileIt cons{0, 0, -1};
+  for (int s = 0; s < S - 1; s++) {
+    if (s < total) issue(s, ring + s * SLOT);
+    cp_async_commit();
+  }
+  // thread mapping for a tile: warp w -> right-hand side w>>2 and rows
+  // (w&3)*8 + (lane&7); lane>>3 picks 8 of the 32 tile columns
+  const int lane = tid & 31, w = tid >> 5;
+  const int which = w >> 2;
+  const int q = (w & 3) * 8 + (lane & 7);
+  const int jp = lane >> 3;
+  const bool active = which == 0 || two;
+  C* tv = which ? t2 : t1;
+  __syncthreads();
+  for (int ci = 0; ci < total; ci++) {
+    const int pi = ci + S - 1;
+    if (pi < total) issue(pi, ring + (pi % S) * SLOT);
+    cp_async_commit();
+    cp_async_wait<S - 1>();
+    __syncthreads();
+    const C* tile = ring + (ci % S) * SLOT;
+    const int k0 = cons.k * B;
+    if (cons.c < 0) {
+      // x_blk = inv(diag block) * t_blk
+      C acc = czero<C>();
+      if (active) {
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) {
+          const int j = jj * 4 + jp;
+          cfma(acc, tile[j * kTileLd + q], tv[k0 + j]);
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 8);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 8);
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 16);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 16);
+      if (active && jp == 0) xb[which][q] = acc;
+      __syncthreads();
+      if (active && jp == 0) tv[k0 + q] = acc;
+    } else {
+      // t_rows(c) -= tile * x_blk
+      C acc = czero<C>();
+      if (active) {
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) {
+          const int j = jj * 4 + jp;
+          cfma(acc, tile[j * kTileLd + q], xb[which][j]);
+        }
+      }
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 8);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 8);
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 16);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 16);
+      if (active && jp == 0) {
+        const int r = cons.c * B + q;
+        tv[r] = csub(tv[r], acc);
+      }
+    }
+    tile_next(cons, nb);
+    __syncthreads();
+  }
+  cp_async_wait<0>();
   for (int k = tid; k < n; k += blockDim.x) {
     T1[k] = t1[k];
     if (two) T2[k] = (k < MN) ? cscale(t2[k], (R)-1) : t2[k];

@@ -17,6 +17,8 @@ struct vox_precond_s {
   double2* Dud = nullptr;
   float2* Dlf = nullptr;       // ... and of the c64 copy
   float2* Duf = nullptr;
+  double2* tiles_d = nullptr;  // per-mode LU tile streams (c128, c64)
+  float2* tiles_f = nullptr;
   double2* twd = nullptr;
   float2* twf = nullptr;
   double2* Td = nullptr;       // L * n3 work
@@ -36,6 +38,9 @@ template <> float2* pc_A<float>(vox_precond_s* p) { return p->Af; }
 template <typename R> Cx<R>* pc_T(vox_precond_s* p, int which);
 template <> double2* pc_T<double>(vox_precond_s* p, int w) { return w ? p->Td2 : p->Td; }
 template <> float2* pc_T<float>(vox_precond_s* p, int w) { return w ? p->Tf2 : p->Tf; }
+template <typename R> Cx<R>* pc_tiles(vox_precond_s* p);
+template <> double2* pc_tiles<double>(vox_precond_s* p) { return p->tiles_d; }
+template <> float2* pc_tiles<float>(vox_precond_s* p) { return p->tiles_f; }
 template <typename R> Cx<R>* pc_Dl(vox_precond_s* p);
 template <> double2* pc_Dl<double>(vox_precond_s* p) { return p->Dld; }
 template <> float2* pc_Dl<float>(vox_precond_s* p) { return p->Dlf; }
@@ -56,8 +61,8 @@ static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaSt
   Cx<R>* T = pc_T<R>(p, 0);
   k_pc_xfwd<R><<<nb, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip);
   if (p->lu) {
-    k_pc_lu_solve2<R><<<p->Lf, 512, 2 * (size_t)lu_npad(g.n3) * cs, st>>>(
-        g, p->paired, pc_A<R>(p), pc_Dl<R>(p), pc_Du<R>(p), p->perm, T, skip);
+    k_pc_lu_stream<R><<<p->Lf, 256, lu_stream_smem<R>(lu_npad(g.n3)), st>>>(
+        g, p->paired, pc_tiles<R>(p), p->perm, T, skip);
   } else {
     Cx<R>* T2 = pc_T<R>(p, 1);
     const int tiles = (g.n3 + 255) / 256;
@@ -77,8 +82,8 @@ static vox_status pc_attrs(const PcGeom& g) {
                                 (int)pc_xsmem(g, cs)));
   VOX_CUDA(cudaFuncSetAttribute(k_pc_xinv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)pc_xsmem(g, cs)));
-  VOX_CUDA(cudaFuncSetAttribute(k_pc_lu_solve2<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(2 * lu_npad(g.n3) * cs)));
+  VOX_CUDA(cudaFuncSetAttribute(k_pc_lu_stream<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)lu_stream_smem<R>(lu_npad(g.n3))));
   VOX_CUDA(cudaFuncSetAttribute(k_pc_gemv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(g.n3 * cs)));
   VOX_CUDA(cudaFuncSetAttribute(k_lu_batched<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -96,6 +101,8 @@ static void pc_free(vox_precond_s* p) {
   cudaFree(p->Dud);
   cudaFree(p->Dlf);
   cudaFree(p->Duf);
+  cudaFree(p->tiles_d);
+  cudaFree(p->tiles_f);
   cudaFree(p->twd);
   cudaFree(p->twf);
   cudaFree(p->Td);
@@ -193,22 +200,27 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   }
   p->Lf = p->paired ? g.L / 2 + 1 : g.L;
   const int Lf = p->Lf;
+  // factors kept column-major with leading dimension ld = 3MN rounded up to
+  // whole 32-blocks (zero padding) for the streamed triangular solves
+  const int ld = lu_npad(g.n3);
   const long long per = (long long)g.n3 * g.n3;
+  const long long perp = (long long)ld * ld;
   const int nbd = (g.n3 + kTrsvNb - 1) / kTrsvNb;
   const long long dsz = (long long)Lf * nbd * kTrsvNb * kTrsvNb;
-  VOX_TRY(dalloc(&p->Ad, Lf * per));
+  VOX_TRY(dalloc(&p->Ad, Lf * perp));
+  VOX_CUDA(cudaMemsetAsync(p->Ad, 0, Lf * perp * sizeof(double2), st));
   VOX_TRY(dalloc(&p->piv, (long long)Lf * g.n3));
   VOX_TRY(dalloc(&p->perm, (long long)Lf * g.n3));
   VOX_TRY(dalloc(&p->Dld, dsz));
   VOX_TRY(dalloc(&p->Dud, dsz));
-  k_assemble_blocks<<<nblk(Lf * per), 256, 0, st>>>(g.L, g.M, g.N, V, 0, Lf, dC, dface,
+  k_assemble_blocks<<<nblk(Lf * per), 256, 0, st>>>(g.L, g.M, g.N, V, 0, Lf, ld, dC, dface,
                                                      op->gram, p->Ad);
   VOX_CUDA(cudaGetLastError());
   int* dinfo;
   VOX_TRY(dalloc(&dinfo, Lf));
   std::unique_ptr<int, decltype(&cudaFree)> gI(dinfo, cudaFree);
   VOX_CUDA(cudaMemsetAsync(dinfo, 0, Lf * sizeof(int), st));
-  k_lu_batched<double><<<Lf, 512, (size_t)g.n3 * kLuNb * sizeof(double2), st>>>(g.n3, p->Ad,
+  k_lu_batched<double><<<Lf, 512, (size_t)g.n3 * kLuNb * sizeof(double2), st>>>(g.n3, ld, p->Ad,
                                                                                 p->piv, dinfo);
   VOX_CUDA(cudaGetLastError());
   std::vector<int> info(Lf);
@@ -220,23 +232,31 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
       return VOX_ERR_BAD_ARG;
     }
   k_lu_perm<<<Lf, 32, 0, st>>>(g.n3, p->piv, p->perm);
-  k_tri_inv_blocks<<<dim3(nbd, Lf), 64, 0, st>>>(g.n3, p->Ad, p->Dld, p->Dud);
+  k_tri_inv_blocks<<<dim3(nbd, Lf), 64, 0, st>>>(g.n3, ld, p->Ad, p->Dld, p->Dud);
   VOX_CUDA(cudaGetLastError());
   // c64 copy: factors of B/Gram (the c64 operator is A/Gram): L unchanged,
   // U / Gram (so inv(U) * Gram), so the copy applies Gram * M^{-1}
   p->lu = true;
   p->f_scale = op->gram;
+  // repack into per-mode tile streams in consumption order; the c64 stream
+  // holds U/Gram and Gram*inv(U_kk), so it applies Gram * M^{-1}
+  const long long tsz = (long long)Lf * lu_tiles(nbd) * kTrsvNb * kTrsvNb;
+  VOX_TRY(dalloc(&p->tiles_d, tsz));
+  k_tile_pack<double><<<dim3(lu_tiles(nbd), Lf), 256, 0, st>>>(nbd, ld, p->Ad, p->Dld, p->Dud,
+                                                               1.0, 1.0, p->tiles_d);
   if (op->has_f) {
-    VOX_TRY(dalloc(&p->Af, Lf * per));
-    VOX_TRY(dalloc(&p->Dlf, dsz));
-    VOX_TRY(dalloc(&p->Duf, dsz));
-    k_cast_scale_upper<float><<<nblk(Lf * per), 256, 0, st>>>(Lf * per, g.n3, p->Ad,
-                                                              1.0 / op->gram, p->Af);
-    k_cast_scale<float><<<nblk(dsz), 256, 0, st>>>(dsz, p->Dld, 1.0, p->Dlf);
-    k_cast_scale<float><<<nblk(dsz), 256, 0, st>>>(dsz, p->Dud, op->gram, p->Duf);
-    VOX_CUDA(cudaGetLastError());
+    VOX_TRY(dalloc(&p->tiles_f, tsz));
+    k_tile_pack<float><<<dim3(lu_tiles(nbd), Lf), 256, 0, st>>>(
+        nbd, ld, p->Ad, p->Dld, p->Dud, 1.0 / op->gram, op->gram, p->tiles_f);
   }
+  VOX_CUDA(cudaGetLastError());
   VOX_CUDA(cudaStreamSynchronize(st));
+  cudaFree(p->Ad);
+  cudaFree(p->Dld);
+  cudaFree(p->Dud);
+  p->Ad = nullptr;
+  p->Dld = p->Dud = nullptr;
+  (void)dsz;
   op->pcs.push_back(p.get());
   *out = p.release();
   return VOX_OK;
@@ -594,7 +614,10 @@ static vox_status refined_entry(vox_op_s* op, vox_precond_s* pc, int side, const
     set_error("restart must be in 1.." + std::to_string(kMaxRestart));
     return VOX_ERR_BAD_ARG;
   }
-  if (inner_tol <= 0) inner_tol = 1e-3;
+  // inner_tol <= 0: aim each inner solve at the remaining target directly
+  // (0.3 * tol * ||b|| / ||r||, the factor leaving room for the gap between the
+  // preconditioned residual GMRES minimises and the true residual)
+  const bool auto_tol = inner_tol <= 0;
   if (max_refine < 1) max_refine = 10;
   VOX_TRY(ensure_work<float>(op, restart));
   if (!op->wd.V) VOX_TRY(ensure_work<double>(op, 1));
@@ -629,7 +652,8 @@ static vox_status refined_entry(vox_op_s* op, vox_precond_s* pc, int side, const
     k_cast_scale<float><<<nb, 256, 0, st>>>(n, wd.r, 1.0 / rn, wf.b);
     vox_gmres_info ii{};
     // tolerance relative to ||r||; never ask for less than what reaches tol
-    const double itol = std::min(0.5, std::max(inner_tol, 0.5 * tol * bn / rn));
+    const double itol = auto_tol ? std::min(0.5, 0.3 * tol * bn / rn)
+                                 : std::min(0.5, std::max(inner_tol, 0.5 * tol * bn / rn));
     VOX_TRY(pgmres_dev<float>(op, pc, side, itol, maxit_inner, &ii, &rv));
     info->total_iters += ii.total_iters;
     outer_total += ii.iter_outer;
@@ -843,8 +867,9 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     });
     out[4] = timeit([&] {
       if (pc->lu)
-        k_pc_lu_solve2<R><<<pc->Lf, 512, 2 * (size_t)lu_npad(pg.n3) * cs, st>>>(
-            pg, pc->paired, pc_A<R>(pc), pc_Dl<R>(pc), pc_Du<R>(pc), pc->perm, T, nullptr);
+        k_pc_lu_stream<R><<<pc->Lf, 256, lu_stream_smem<R>(lu_npad(pg.n3)), st>>>(
+            pg, pc->paired, pc_tiles<R>(pc), pc->perm, T,
+            nullptr);
       else
         k_pc_gemv<R><<<pg.L * ((pg.n3 + 255) / 256), 256, (size_t)pg.n3 * cs, st>>>(
             pg, pc_A<R>(pc), T, pc_T<R>(pc, 1), nullptr);
@@ -908,6 +933,17 @@ vox_status vox_op_set_stream(vox_op_t op, void* stream) {
     return VOX_ERR_BAD_ARG;
   }
   op->stream = stream ? (cudaStream_t)stream : op->own_stream;
+  return VOX_OK;
+}
+
+vox_status vox_precond_info(vox_precond_t p, int* n_factored, int* ld, int* is_lu) {
+  if (!p) {
+    set_error("vox_precond_info: NULL preconditioner");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (n_factored) *n_factored = p->lu ? p->Lf : p->g.L;
+  if (ld) *ld = p->lu ? lu_npad(p->g.n3) : p->g.n3;
+  if (is_lu) *is_lu = p->lu ? 1 : 0;
   return VOX_OK;
 }
 

@@ -233,6 +233,12 @@ class Preconditioner:
     def handle(self):
         return self._h
 
+    def info(self):
+        nf, ld, lu = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().vox_precond_info(self._h, ctypes.byref(nf), ctypes.byref(ld),
+                                     ctypes.byref(lu)))
+        return {"n_factored": nf.value, "ld": ld.value, "lu": bool(lu.value)}
+
     def apply(self, JIn, prec="c128"):
         re, im = split(JIn, self.op.n)
         ore = np.empty(self.op.n)
