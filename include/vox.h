@@ -132,6 +132,19 @@ vox_status vox_mv_L(vox_op_t op, vox_prec prec, const double* in_re, const doubl
  * device pointers of length n; stream is a cudaStream_t (NULL = the op's). */
 vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* in, void* out,
                             void* stream);
+/* Same product as vox_mv_AN_device, but allocating nothing: for callers that
+ * cannot call cudaMalloc where they need the product (an external memory
+ * manager owns all device memory, or allocation is forbidden in that region).
+ * No counterpart in the reference.  The two plane intermediates live in a
+ * fixed 64 MiB device array inside libvox (held by every GPU that loads the
+ * library until exit), so operators needing more than 64 MiB of intermediates
+ * (2 * Px * 3MN complex values) are rejected with VOX_ERR_BAD_ARG.  The first
+ * call on a device looks up the array's device address; make that call before
+ * any stream capture.  Every call shares the array: calls that overlap on the
+ * GPU (different streams or threads) race.  Each call overwrites what it reads,
+ * so nothing carries over from the previous call. */
+vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, const void* in, void* out,
+                             void* stream);
 
 /* Level-1 circulant preconditioner (T. Chan circulant along x, per-mode dense
  * blocks inv(Gram*I - diag(face3)*circ_i)); face3 = (m-1)/m with m the x-mean of

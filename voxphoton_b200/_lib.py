@@ -80,6 +80,8 @@ SIGNATURES = [
     ("vox_mv_L", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp]),
     ("vox_mv_AN_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("vox_mv_AN_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("vox_precond_create_level1", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp,
                                                  ctypes.POINTER(ctypes.c_void_p)]),
     ("vox_precond_create_blocks", ctypes.c_int, [ctypes.c_void_p, _dp, _dp,

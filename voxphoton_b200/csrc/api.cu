@@ -718,3 +718,90 @@ vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* 
 }  // extern "C"
 
 #include "solver.cuh"
+
+// ------------------------------------------------ matvec without allocation
+// Some callers cannot call cudaMalloc at the point where they need a product:
+// code running under an external memory manager that owns every device
+// allocation, or inside a callback/region where allocating is forbidden.
+// vox_mv_AN_noalloc runs the fused matvec on an operator prepared earlier with
+// the two plane intermediates placed in this fixed, file-scope device array
+// instead of the operator's own buffers.  The array is part of the module:
+// every GPU that loads libvox holds it until the process exits.
+namespace vox {
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // 64 MiB: T1 and T2 together
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static std::map<int, void*> g_noalloc_addr;  // device ordinal -> array address
+
+// Device address of the array on `dev` (which must be current).  Looked up
+// once per device; a host-side reference to the symbol is not a device address.
+static vox_status noalloc_scratch(int dev, void** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  auto it = g_noalloc_addr.find(dev);
+  if (it != g_noalloc_addr.end()) {
+    *out = it->second;
+    return VOX_OK;
+  }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    cudaGetLastError();
+    set_error(std::string("vox_mv_AN_noalloc: cudaGetSymbolAddress failed: ") +
+              cudaGetErrorString(e));
+    return VOX_ERR_CUDA;
+  }
+  g_noalloc_addr[dev] = p;
+  *out = p;
+  return VOX_OK;
+}
+
+template <typename R>
+static vox_status matvec_noalloc(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out,
+                                 cudaStream_t st, Cx<R>* T1, Cx<R>* T2) {
+  OpBuffers<R>& b = bufs<R>(op);
+  const OpGeom& g = b.geo;
+  const size_t cs = sizeof(Cx<R>);
+  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3);
+  const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
+  k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1,
+                                            nullptr);
+  k_plane<R><<<g.Px, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1, b.fN, T2,
+                                               nullptr);
+  k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
+                                            b.gram, scale, b.out_scale, mode, out, nullptr);
+  VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
+}  // namespace vox
+
+extern "C" vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, const void* in,
+                                        void* out, void* stream) {
+  if (!op || !in || !out) {
+    set_error("vox_mv_AN_noalloc: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  VOX_TRY(check_prec(op, prec));
+  DeviceGuard dg(op->device);
+  const OpGeom& g = prec == VOX_C128 ? op->d.geo : op->f.geo;
+  const size_t cs = prec == VOX_C128 ? sizeof(double2) : sizeof(float2);
+  const size_t half = ((size_t)g.Px * 3 * g.N * g.M * cs + 255) / 256 * 256;
+  if (2 * half > kNoAllocScratchBytes) {
+    set_error("vox_mv_AN_noalloc: this operator needs " + std::to_string(2 * half) +
+              " bytes of scratch; the fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
+              " bytes (use vox_mv_AN_device)");
+    return VOX_ERR_BAD_ARG;
+  }
+  void* base = nullptr;
+  VOX_TRY(noalloc_scratch(op->device, &base));
+  cudaStream_t st = stream ? (cudaStream_t)stream : op->stream;
+  const int mode = transp ? MV_AN_T : MV_AN;
+  unsigned char* b8 = static_cast<unsigned char*>(base);
+  if (prec == VOX_C128)
+    return matvec_noalloc<double>(op, mode, (const double2*)in, (double2*)out, st,
+                                  (double2*)b8, (double2*)(b8 + half));
+  return matvec_noalloc<float>(op, mode, (const float2*)in, (float2*)out, st, (float2*)b8,
+                               (float2*)(b8 + half));
+}
