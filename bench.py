@@ -38,7 +38,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vox", choices=["vox", "reference"])
     ap.add_argument("--workload", default="bragg20")
-    ap.add_argument("--precond", default="none", choices=["none", "level1"])
+    ap.add_argument("--precond", default="level1", choices=["none", "level1"])
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--inner-tol", type=float, default=0.0,
@@ -46,6 +46,18 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
+    ap.add_argument("--no-stages", action="store_true", help="skip per-kernel timing")
+    ap.add_argument("--sweep-periods", default="20,40,60,80,100")
+    ap.add_argument("--sweep-lambdas", type=int, default=201)
+    ap.add_argument("--sweep-rate", type=float, default=200.0,
+                    help="Poisson arrival rate (requests/s) of the sweep stream")
+    ap.add_argument("--sweep-slots", type=int, default=4)
+    ap.add_argument("--sweep-fp64", type=int, default=10,
+                    help="requests solved one at a time in plain complex128 for the baseline")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-clocks", action="store_true",
+                    help="do not spawn the nvidia-smi clock sampler (profiler runs)")
     return ap.parse_args()
 
 
@@ -113,6 +125,22 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def measured_traffic(kernel, alg_bytes):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/ncu_kernels_bragg.md, line 'traffic_ratio <kernel> <r>' = measured
+    dram bytes / algorithmic bytes on the captured case), scaled to this launch's
+    algorithmic bytes; None when no capture covers the kernel."""
+    path = os.path.join(ROOT, "profiles", "ncu_kernels_bragg.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "traffic_ratio" and parts[1] == kernel:
+                return float(parts[2]) * alg_bytes
+    return None
+
+
 def build_problem(name):
     from voxphoton_b200 import geometry as geo
     import voxphoton_b200 as vb
@@ -153,8 +181,9 @@ def kernel_bytes(op_info, shape, n, pc_info, k):
         nf, ld = pc_info["n_factored"], pc_info["ld"]
         nblk = ld // 32
         b["pc_xfwd"] = n * c + 3 * V * 4 + L * n3 * c
-        b["pc_solve"] = nf * ld * ld * c + 2 * nf * nblk * 32 * 32 * c + 2 * L * n3 * c \
-            + nf * n3 * 4
+        # the tile stream: nb*(nb+1) 32x32 tiles per factored mode (L and U
+        # off-diagonal tiles plus the two inverted diagonal blocks per block row)
+        b["pc_solve"] = nf * nblk * (nblk + 1) * 32 * 32 * c + 2 * L * n3 * c + nf * n3 * 4
         b["pc_xinv"] = L * n3 * c + 3 * V * 4 + n * c
     return b
 
@@ -234,6 +263,90 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_sweep(args, world, rank, local):
+    """Mixed-length Bragg sweep served as a Poisson request stream (one GPU per
+    rank; ranks take disjoint shares of the stream)."""
+    import torch
+    from voxphoton_b200 import geometry as geo
+    from voxphoton_b200 import serving as sv
+    torch.cuda.set_device(local)
+    periods = [int(x) for x in args.sweep_periods.split(",")]
+    band = (1500e-9, 1600e-9)
+    lams = np.linspace(band[0], band[1], args.sweep_lambdas)
+    t = time.time()
+    fams = [sv.Family(pr, geo.bragg(periods=pr, M=30), band, nG=5, device=local)
+            for pr in periods]
+    setup_s = time.time() - t
+    # admission by HBM footprint: slots per family from one slot's bytes
+    free0, total = torch.cuda.mem_get_info()
+    fams[-1].add_slot()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    slot_bytes = max(free0 - free1, 1)
+    budget = 0.6 * free1
+    nslots = int(max(1, min(args.sweep_slots, budget // (slot_bytes * len(fams)))))
+    for f in fams:
+        while len(f.slots) < nslots:
+            f.add_slot()
+    mine = sv.shard_requests([(pr, lam) for pr in periods for lam in lams], world, rank)
+    reqs = sv.poisson_stream(mine, rate=args.sweep_rate, seed=args.seed + rank)
+    # warm-up: one solve per family (graph capture, caches)
+    warm = [sv.Request(-1 - i, f.key, lams[len(lams) // 2], 0.0) for i, f in enumerate(fams)]
+    sv.SweepServer(fams).serve(warm, realtime=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res, wall = sv.SweepServer(fams, sv.ServeConfig(tol=args.tol)).serve(reqs, realtime=True)
+    torch.cuda.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    dev_s = e0.elapsed_time(e1) / 1e3
+    summ = sv.summarize(res, wall)
+    # plain complex128 GMRES, one solve at a time, on a seeded subset
+    rng = np.random.default_rng(args.seed)
+    sub = [reqs[i] for i in rng.choice(len(reqs), size=min(len(reqs), args.sweep_fp64), replace=False)]
+    for f in fams:
+        for op, pc in f.slots[1:]:
+            pc.close()
+            op.close()
+        del f.slots[1:]
+    res64, wall64 = sv.SweepServer(fams, sv.ServeConfig(tol=args.tol, mode="fp64")).serve(
+        sub, realtime=False)
+    fp64 = sv.summarize(res64, wall64)
+    fp64_serial = len(res64) / sum(r.done - r.start for r in res64)
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([dev_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_s = float(tt.item())
+    value = len(res) * world / dev_s
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+                "steps": len(res), "warmup": len(warm), "ms_per_step": 1e3 * dev_s / len(res),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "c64", "data": "synthetic",
+                "config": {"workload": f"mixed-length Bragg sweep: periods {periods} (grids "
+                                       f"{[f.p.shape for f in fams]}), {len(lams)} wavelengths "
+                                       f"in 1500-1600 nm each, Poisson arrivals "
+                                       f"{args.sweep_rate}/s (seed {args.seed})",
+                           "tol": args.tol, "slots_per_length": nslots,
+                           "slot_bytes": int(slot_bytes), "setup_s": round(setup_s, 1),
+                           "operator": "Lagrange interpolation over 5 Legendre wavelengths",
+                           "precond": "level1 at band centre, shared per length"},
+                "latency_ms": {"p50": summ["p50_ms"], "p99": summ["p99_ms"]},
+                "serving": summ,
+                "fp64_plain_serial": {"solves_per_s": fp64_serial, "sampled": len(res64),
+                                      "mean_iters": fp64["mean_iters"],
+                                      "max_relres": fp64["max_relres"]},
+                "speedup_vs_fp64_serial": value / world / fp64_serial,
+                "e2e": {"value": value, "unit": "solves/s",
+                        "h2d_bytes_per_step": int(np.mean([f.idx.size for f in fams]) * 16),
+                        "d2h_bytes_per_step": int(np.mean([f.idx.size for f in fams]) * 16)}}
+        print(json.dumps(line), flush=True)
+    for f in fams:
+        f.close()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -241,6 +354,19 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "sweep":
+        if world > 1:
+            import torch
+            import torch.distributed as dist
+            from datetime import timedelta
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        run_sweep(args, world, rank, local)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
         return
     import torch
     import torch.distributed as dist
@@ -275,8 +401,9 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = Clocks(local)
-    clocks.start()
+    clocks = None if args.no_clocks else Clocks(local)
+    if clocks:
+        clocks.start()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     launches0 = op.launches()
     torch.cuda.synchronize()
@@ -289,7 +416,8 @@ def main():
         relres.append(info.relres)
     torch.cuda.synchronize()
     launches = op.launches() - launches0
-    ck = clocks.stop()
+    ck = clocks.stop() if clocks else {"sm_mhz": None, "sm_max_mhz": None,
+                                       "reasons": ["not sampled (--no-clocks)"]}
     lat = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)])
     total_ms = float(ev[0].elapsed_time(ev[-1]))
     if world > 1:
@@ -318,7 +446,7 @@ def main():
 
     # end to end through the C-ABI with host buffers (H2D of b, D2H of x per step)
     e2e = None
-    if args.steps > 0:
+    if args.steps > 0 and not args.no_e2e:
         import ctypes
         from voxphoton_b200 import _lib
         bre = np.ascontiguousarray(b.real)
@@ -351,16 +479,19 @@ def main():
                "h2d_bytes_per_step": int(2 * n * 8), "d2h_bytes_per_step": int(2 * n * 8)}
 
     # roofline of the dominant kernel, from live CUDA-event timing of each stage
-    k_avg = max(1, min(args.restart - 1, int(np.mean(iters) // 2) if iters else 25))
-    stages = op.profile_stages(pc, "c64", restart=args.restart, kgs=min(k_avg, 25), reps=20)
-    nbytes = kernel_bytes(op.info(), p.shape, n, pc.info() if pc else None, min(k_avg, 25))
-    dom = max((k for k in nbytes if stages.get(k, 0) > 0), key=lambda k: stages[k])
-    peak, peak_kind = peaks()
-    achieved = nbytes[dom] / (stages[dom] * 1e-3) / 1e9
-    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-            "bytes_per_launch": nbytes[dom], "ms_per_launch": stages[dom],
-            "stage_ms": stages}
+    roof = None
+    if not args.no_stages:
+        k_avg = max(1, min(args.restart - 1, int(np.mean(iters) // 2) if iters else 25))
+        stages = op.profile_stages(pc, "c64", restart=args.restart, kgs=min(k_avg, 25), reps=20)
+        nbytes = kernel_bytes(op.info(), p.shape, n, pc.info() if pc else None, min(k_avg, 25))
+        dom = max((k for k in nbytes if stages.get(k, 0) > 0), key=lambda k: stages[k])
+        peak, peak_kind = peaks()
+        achieved = nbytes[dom] / (stages[dom] * 1e-3) / 1e9
+        traffic = measured_traffic(dom, nbytes[dom])
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_kind, "bytes_per_launch": nbytes[dom],
+                "ms_per_launch": stages[dom], "stage_ms": stages}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

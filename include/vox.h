@@ -110,6 +110,12 @@ vox_status vox_op_info(vox_op_t op, int* Px, int* Py, int* Pz, long long* n);
 vox_status vox_op_set_stream(vox_op_t op, void* stream);
 /* Kernels launched so far by the solver entry points on this operator. */
 vox_status vox_op_stats(vox_op_t op, long long* launches);
+/* dst.fN = sum_i w[i] * srcs[i].fN on the device (all operators on one grid,
+ * padding, storage and precisions): lagrange_int(fN, S, s) of
+ * piecewise_constant/src_photonics/lagrange_int.m:1-12, the reference's
+ * wavelength interpolation of the operator between Legendre nodes.  Enqueued
+ * on dst's stream; Mr, Mc, Gram and idx of dst are unchanged. */
+vox_status vox_op_interp(vox_op_t dst, const vox_op_t* srcs, const double* w, int n);
 /* Storage flags: bit 0 set when fN is kept as one octant (the transformed
  * circulant has the per-axis parity of the Green tensor). */
 vox_status vox_op_flags(vox_op_t op, int* flags);
@@ -156,6 +162,12 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
 vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const double* blk_im,
                                      vox_precond_t* out);
 void vox_precond_destroy(vox_precond_t p);
+/* A second handle on the same factors, bound to `op` (same grid and support
+ * idx as the source's operator), with its own work buffers: lets solves on
+ * different operators/streams (e.g. the wavelengths of a sweep of one device)
+ * apply one preconditioner concurrently.  The factors live until the last
+ * handle sharing them is destroyed.  No reference counterpart. */
+vox_status vox_precond_share(vox_precond_t src, vox_op_t op, vox_precond_t* out);
 /* Factored modes (L, or L/2+1 when modes L-i reuse the factors of mode i),
  * the factor leading dimension, and whether the blocks are LU factors (1) or
  * caller-supplied explicit inverses (0). */

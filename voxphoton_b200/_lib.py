@@ -114,6 +114,10 @@ SIGNATURES = [
     ("vox_op_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("vox_op_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("vox_op_flags", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    ("vox_op_interp", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), _dp,
+                                     ctypes.c_int]),
+    ("vox_precond_share", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
     ("vox_precond_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]),

@@ -26,6 +26,10 @@ struct vox_precond_s {
   float2* Tf = nullptr;
   float2* Tf2 = nullptr;
   double f_scale = 1.0;        // the c64 copy applies f_scale * M^{-1}
+  // Owner of the factor arrays above (Ad/Af/piv/perm/D*/tiles/tw): set once
+  // construction succeeds; views made by vox_precond_share hold a copy, and the
+  // arrays are freed with the last holder.  Work buffers T* are per handle.
+  std::shared_ptr<void> factors;
 };
 
 namespace vox {
@@ -91,20 +95,45 @@ static vox_status pc_attrs(const PcGeom& g) {
   return VOX_OK;
 }
 
+// Hand the factor arrays to a shared owner (called once a handle is complete).
+static void pc_seal(vox_precond_s* p) {
+  double2 *Ad = p->Ad, *Dld = p->Dld, *Dud = p->Dud, *td = p->tiles_d, *twd = p->twd;
+  float2 *Af = p->Af, *Dlf = p->Dlf, *Duf = p->Duf, *tf = p->tiles_f, *twf = p->twf;
+  int *piv = p->piv, *perm = p->perm;
+  p->factors = std::shared_ptr<void>(nullptr, [=](void*) {
+    cudaFree(Ad);
+    cudaFree(Af);
+    cudaFree(piv);
+    cudaFree(perm);
+    cudaFree(Dld);
+    cudaFree(Dud);
+    cudaFree(Dlf);
+    cudaFree(Duf);
+    cudaFree(td);
+    cudaFree(tf);
+    cudaFree(twd);
+    cudaFree(twf);
+  });
+}
+
 static void pc_free(vox_precond_s* p) {
   if (!p) return;
-  cudaFree(p->Ad);
-  cudaFree(p->Af);
-  cudaFree(p->piv);
-  cudaFree(p->perm);
-  cudaFree(p->Dld);
-  cudaFree(p->Dud);
-  cudaFree(p->Dlf);
-  cudaFree(p->Duf);
-  cudaFree(p->tiles_d);
-  cudaFree(p->tiles_f);
-  cudaFree(p->twd);
-  cudaFree(p->twf);
+  if (p->factors) {
+    p->factors.reset();
+  } else {  // construction did not complete: the arrays are still this handle's
+    cudaFree(p->Ad);
+    cudaFree(p->Af);
+    cudaFree(p->piv);
+    cudaFree(p->perm);
+    cudaFree(p->Dld);
+    cudaFree(p->Dud);
+    cudaFree(p->Dlf);
+    cudaFree(p->Duf);
+    cudaFree(p->tiles_d);
+    cudaFree(p->tiles_f);
+    cudaFree(p->twd);
+    cudaFree(p->twf);
+  }
   cudaFree(p->Td);
   cudaFree(p->Td2);
   cudaFree(p->Tf);
@@ -257,6 +286,7 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   p->Ad = nullptr;
   p->Dld = p->Dud = nullptr;
   (void)dsz;
+  pc_seal(p.get());
   op->pcs.push_back(p.get());
   *out = p.release();
   return VOX_OK;
@@ -286,6 +316,7 @@ vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const do
     VOX_CUDA(cudaGetLastError());
   }
   VOX_CUDA(cudaStreamSynchronize(op->stream));
+  pc_seal(p.get());
   op->pcs.push_back(p.get());
   *out = p.release();
   return VOX_OK;
@@ -512,15 +543,26 @@ static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, double t
   init->tol_abs = tol * bnorm;
   VOX_CUDA(cudaMemcpyAsync(w.st, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
   VOX_CUDA(cudaStreamSynchronize(st));
-  cudaGraphExec_t cyc;
-  VOX_TRY(get_cycle_graph<R>(op, pc, side, &cyc));
+  // VOX_GRAPHS=0 enqueues each cycle's kernels directly instead of replaying
+  // the captured graph (same kernels and order; for profilers that cannot
+  // follow stream capture)
+  static const bool use_graphs = [] {
+    const char* e = std::getenv("VOX_GRAPHS");
+    return !(e && e[0] == '0');
+  }();
+  cudaGraphExec_t cyc = nullptr;
+  if (use_graphs) VOX_TRY(get_cycle_graph<R>(op, pc, side, &cyc));
   double rel = 1.0;  // ||r0|| / bnorm with x0 = 0
   if (resvec) resvec->push_back(rel);
   int outit = 0, p = 0;
   while (rel > tol && outit < maxit) {
     outit++;
-    VOX_CUDA(cudaGraphLaunch(cyc, st));
-    op->launches += op->graph_nodes[cyc];
+    if (cyc) {
+      VOX_CUDA(cudaGraphLaunch(cyc, st));
+      op->launches += op->graph_nodes[cyc];
+    } else {
+      VOX_TRY(enqueue_cycle<R>(op, pc, side, st));
+    }
     VOX_CUDA(cudaMemcpyAsync(w.hst, w.st, offsetof(GmresDev, sn), cudaMemcpyDeviceToHost, st));
     VOX_CUDA(cudaStreamSynchronize(st));
     p = w.hst->k;
@@ -936,6 +978,34 @@ vox_status vox_op_set_stream(vox_op_t op, void* stream) {
   return VOX_OK;
 }
 
+vox_status vox_precond_share(vox_precond_t src, vox_op_t op, vox_precond_t* out) {
+  if (!src || !op || !out) {
+    set_error("vox_precond_share: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  const vox_op_s* so = src->op;
+  if (op->g.L != so->g.L || op->g.M != so->g.M || op->g.N != so->g.N || op->g.n != so->g.n ||
+      op->gram != so->gram || op->device != so->device || op->has_f != so->has_f) {
+    set_error("vox_precond_share: the operator differs in grid, support size, Gram or device");
+    return VOX_ERR_BAD_ARG;
+  }
+  DeviceGuard dg(op->device);
+  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
+  *p = *src;  // geometry, plans and factor pointers (shared owner copied)
+  p->op = op;
+  p->Td = p->Td2 = nullptr;
+  p->Tf = p->Tf2 = nullptr;
+  const long long LT = (long long)p->g.L * p->g.n3;
+  VOX_TRY(dalloc(&p->Td, LT));
+  VOX_TRY(dalloc(&p->Td2, LT));
+  VOX_TRY(dalloc(&p->Tf, LT));
+  VOX_TRY(dalloc(&p->Tf2, LT));
+  op->pcs.push_back(p.get());
+  *out = p.release();
+  return VOX_OK;
+}
+
 vox_status vox_precond_info(vox_precond_t p, int* n_factored, int* ld, int* is_lu) {
   if (!p) {
     set_error("vox_precond_info: NULL preconditioner");
@@ -953,6 +1023,63 @@ vox_status vox_op_flags(vox_op_t op, int* flags) {
     return VOX_ERR_BAD_ARG;
   }
   *flags = op->g.sym ? 1 : 0;
+  return VOX_OK;
+}
+
+}  // extern "C"
+
+namespace vox {
+
+template <typename R>
+__global__ void k_lincomb_acc(long long n, const Cx<R>* __restrict__ src, double w, int first,
+                              Cx<R>* dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const Cx<R> s = src[i];
+    Cx<R> d = first ? czero<Cx<R>>() : dst[i];
+    d.x += (R)w * s.x;
+    d.y += (R)w * s.y;
+    dst[i] = d;
+  }
+}
+
+template <typename R>
+static long long fN_count(const OpGeom& g) {
+  return g.sym ? 6LL * (g.Px / 2 + 1) * (g.Py / 2 + 1) * (g.Pz / 2 + 1)
+               : 6LL * g.Px * g.Py * g.Pz;
+}
+
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_op_interp(vox_op_t dst, const vox_op_t* srcs, const double* w, int n) {
+  if (!dst || !srcs || !w || n < 1) {
+    set_error("vox_op_interp: bad argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  for (int i = 0; i < n; i++) {
+    const vox_op_s* s = srcs[i];
+    if (!s || s->g.L != dst->g.L || s->g.M != dst->g.M || s->g.N != dst->g.N ||
+        s->g.Px != dst->g.Px || s->g.Py != dst->g.Py || s->g.Pz != dst->g.Pz ||
+        s->g.sym != dst->g.sym || s->has_d != dst->has_d || s->has_f != dst->has_f ||
+        s->gram != dst->gram || s->device != dst->device) {
+      set_error("vox_op_interp: operators differ in grid, padding, storage or precisions");
+      return VOX_ERR_BAD_ARG;
+    }
+  }
+  DeviceGuard dg(dst->device);
+  cudaStream_t st = dst->stream;
+  const long long cnt = fN_count<double>(dst->g);
+  for (int i = 0; i < n; i++) {
+    if (dst->has_d)
+      k_lincomb_acc<double><<<nblk(cnt), 256, 0, st>>>(cnt, srcs[i]->d.fN, w[i], i == 0,
+                                                        dst->d.fN);
+    if (dst->has_f)
+      k_lincomb_acc<float><<<nblk(cnt), 256, 0, st>>>(cnt, srcs[i]->f.fN, w[i], i == 0,
+                                                       dst->f.fN);
+  }
+  VOX_CUDA(cudaGetLastError());
   return VOX_OK;
 }
 

@@ -132,6 +132,12 @@ class Operator:
         return self.mv_AN(JIn0)
 
     # ----------------------------------------------- device-resident calls
+    def interp(self, srcs, weights):
+        """fN <- sum_i weights[i] * srcs[i].fN on the device (lagrange_int.m)."""
+        arr = (ctypes.c_void_p * len(srcs))(*[s.handle for s in srcs])
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+        check(lib().vox_op_interp(self._h, arr, dptr(w), len(srcs)))
+
     def set_stream(self, stream_ptr):
         """Run on the caller's cudaStream_t (an int handle; 0 restores the op's)."""
         check(lib().vox_op_set_stream(self._h, ctypes.c_void_p(stream_ptr or None)))
@@ -232,6 +238,13 @@ class Preconditioner:
     @property
     def handle(self):
         return self._h
+
+    def share(self, op: Operator):
+        """A handle on the same factors bound to `op` (same grid and idx), with its
+        own work buffers, for concurrent solves on another operator/stream."""
+        h = ctypes.c_void_p()
+        check(lib().vox_precond_share(self._h, op.handle, ctypes.byref(h)))
+        return Preconditioner(op, h)
 
     def info(self):
         nf, ld, lu = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
