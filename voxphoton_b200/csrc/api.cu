@@ -224,15 +224,24 @@ static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cu
   return VOX_OK;
 }
 
+// Every launch shape is checked against kSmemCap before use.  The attribute
+// below is a property of the kernel (per device), not of one operator, so it
+// is always raised to this one fixed cap: operators and preconditioners of
+// different sizes then coexist, and setting it from several host threads is
+// idempotent.
+static const int kSmemCap = 220 * 1024;
+
+template <typename K>
+static vox_status smem_cap(K* kernel) {
+  VOX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
+  return VOX_OK;
+}
+
 template <typename R>
-static vox_status set_smem_attrs(const OpGeom& g) {
-  const size_t cs = sizeof(Cx<R>);
-  VOX_CUDA(cudaFuncSetAttribute(k_xfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)xsmem(g, cs)));
-  VOX_CUDA(cudaFuncSetAttribute(k_xinv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)xsmem(g, cs)));
-  VOX_CUDA(cudaFuncSetAttribute(k_plane<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)psmem(g, cs)));
+static vox_status set_smem_attrs() {
+  VOX_TRY(smem_cap(k_xfwd<R>));
+  VOX_TRY(smem_cap(k_xinv<R>));
+  VOX_TRY(smem_cap(k_plane<R>));
   return VOX_OK;
 }
 
@@ -246,7 +255,7 @@ static bool pick_shapes(OpGeom& g, size_t csz) {
   g.sz = pad_stride(g.Pz);
   int yb = (int)(kSmemBudget / (2ull * g.sx * csz));
   if (yb < 1) {
-    if (2ull * g.sx * csz > 220 * 1024) return false;
+    if (2ull * g.sx * csz > (size_t)kSmemCap) return false;
     yb = 1;
   }
   g.ybx = std::max(1, std::min({yb, 8, g.M}));
@@ -263,7 +272,7 @@ static bool pick_shapes(OpGeom& g, size_t csz) {
     else
       g.kc = (g.kc + 1) / 2;
   }
-  return fits(220 * 1024);
+  return fits(kSmemCap);
 }
 
 // In-place batched FFT of a 3-D array along one axis (setup path).
@@ -299,7 +308,7 @@ static vox_status fft_axis_d(double2* data, int d0, int d1, int d2, long long s0
   lb = std::min(lb, a.d[a.axA]);
   a.lb = lb;
   const size_t smem = (size_t)lb * per;
-  if (smem > 220 * 1024) {
+  if (smem > (size_t)kSmemCap) {
     set_error("FFT length " + std::to_string(n) + " too long for the setup kernel");
     return VOX_ERR_UNSUPPORTED;
   }
@@ -307,8 +316,7 @@ static vox_status fft_axis_d(double2* data, int d0, int d1, int d2, long long s0
   double2* dtw;
   VOX_TRY(dalloc(&dtw, n));
   VOX_CUDA(cudaMemcpyAsync(dtw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
-  VOX_CUDA(cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+  VOX_TRY(smem_cap(k_fft_axis<double>));
   const int tilesA = (a.d[a.axA] + lb - 1) / lb;
   dim3 grid(tilesA * a.d[a.axB], ncomp);
   k_fft_axis<double><<<grid, 256, smem, st>>>(a, p, dtw, sign, data);
@@ -373,7 +381,7 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
   const long long tsz = (long long)g.Px * 3 * g.N * g.M;
   VOX_TRY(dalloc(&b.T1, tsz));
   VOX_TRY(dalloc(&b.T2, tsz));
-  VOX_TRY(set_smem_attrs<R>(b.geo));
+  VOX_TRY(set_smem_attrs<R>());
   return VOX_OK;
 }
 

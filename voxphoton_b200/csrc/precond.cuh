@@ -10,9 +10,11 @@
 //   4. batched LU with partial pivoting of all B_i (one CTA per block,
 //      right-looking, 8-column panels staged in shared memory)
 // Apply (chan_mvp_idx.m:4-16): scatter to the grid, FFT along x of every
-// (y,z,c) line, per mode P*L*U solve (blocked triangular solves, one CTA per
-// mode), inverse FFT along x (1/L), gather.  The apply reads each factor once:
-// L*(3MN)^2 complex values, the same bytes as the reference's inverse-block GEMV.
+// (y,z,c) line, per mode P*L*U solve (factor tiles streamed through shared
+// memory, one CTA per factored mode; modes i and L-i share one factorisation),
+// inverse FFT along x (1/L), gather.  The apply reads each factor once for two
+// modes: (L/2+1)*(3MN)^2 complex values, about half the bytes of the
+// reference's inverse-block GEMV.
 // Caller-supplied inverse blocks (chan_mvp_idx's inv_blocks) are applied by a
 // plain per-mode GEMV instead.
 #pragma once
@@ -120,112 +122,6 @@ __global__ void __launch_bounds__(256) k_pc_gemv(PcGeom g, const Cx<R>* __restri
   }
   if (c < n3) cfma(acc0, Bi[(long long)c * n3 + r], xs[c]);
   Tout[(long long)i * n3 + r] = cadd(acc0, acc1);
-}
-
-// ------------------------------------------------ apply: LU triangular solves
-// One CTA per mode: t = P t; t = L^{-1} t (unit lower); t = U^{-1} t.
-// Factors column-major in A (n3 x n3 per mode), pivots 0-based rows in piv.
-template <typename R>
-__global__ void __launch_bounds__(512) k_pc_lu_solve(PcGeom g, const Cx<R>* __restrict__ A,
-                                                     const int* __restrict__ piv, Cx<R>* T,
-                                                     const int* skip) {
-  using C = Cx<R>;
-  if (skip && *skip) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* t = reinterpret_cast<C*>(smem_raw);  // n3
-  const int n = g.n3;
-  const int i = blockIdx.x;
-  const C* Ai = A + (long long)i * n * n;
-  const int* pv = piv + (long long)i * n;
-  C* Ti = T + (long long)i * n;
-  for (int c = threadIdx.x; c < n; c += blockDim.x) t[c] = Ti[c];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < n; k++) {
-      const int p = pv[k];
-      if (p != k) {
-        C a = t[k];
-        t[k] = t[p];
-        t[p] = a;
-      }
-    }
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // forward substitution with unit lower L, blocks of kTrsvNb columns
-  for (int k0 = 0; k0 < n; k0 += kTrsvNb) {
-    const int kb = min(kTrsvNb, n - k0);
-    if (warp == 0) {
-      // solve the diagonal block: lane r holds t[k0+r]
-      C v = (lane < kb) ? t[k0 + lane] : czero<C>();
-      for (int j = 0; j < kb; j++) {
-        C tj;
-        tj.x = __shfl_sync(0xffffffffu, v.x, j);
-        tj.y = __shfl_sync(0xffffffffu, v.y, j);
-        if (lane > j && lane < kb) {
-          const C l = Ai[(long long)(k0 + j) * n + k0 + lane];
-          v.x -= l.x * tj.x - l.y * tj.y;
-          v.y -= l.x * tj.y + l.y * tj.x;
-        }
-      }
-      if (lane < kb) t[k0 + lane] = v;
-    }
-    __syncthreads();
-    // update the rows below with the panel columns
-    for (int r = k0 + kb + threadIdx.x; r < n; r += blockDim.x) {
-      C acc = t[r];
-      for (int j = 0; j < kb; j++) {
-        const C l = Ai[(long long)(k0 + j) * n + r];
-        const C tj = t[k0 + j];
-        acc.x -= l.x * tj.x - l.y * tj.y;
-        acc.y -= l.x * tj.y + l.y * tj.x;
-      }
-      t[r] = acc;
-    }
-    __syncthreads();
-  }
-  // back substitution with U, blocks from the bottom
-  const int nblk = (n + kTrsvNb - 1) / kTrsvNb;
-  for (int bk = nblk - 1; bk >= 0; bk--) {
-    const int k0 = bk * kTrsvNb;
-    const int kb = min(kTrsvNb, n - k0);
-    if (warp == 0) {
-      C v = (lane < kb) ? t[k0 + lane] : czero<C>();
-      for (int j = kb - 1; j >= 0; j--) {
-        // v_j /= U(j,j)
-        if (lane == j) {
-          const C d = Ai[(long long)(k0 + j) * n + k0 + j];
-          const R dd = d.x * d.x + d.y * d.y;
-          C q;
-          q.x = (v.x * d.x + v.y * d.y) / dd;
-          q.y = (v.y * d.x - v.x * d.y) / dd;
-          v = q;
-        }
-        C tj;
-        tj.x = __shfl_sync(0xffffffffu, v.x, j);
-        tj.y = __shfl_sync(0xffffffffu, v.y, j);
-        if (lane < j) {
-          const C u = Ai[(long long)(k0 + j) * n + k0 + lane];
-          v.x -= u.x * tj.x - u.y * tj.y;
-          v.y -= u.x * tj.y + u.y * tj.x;
-        }
-      }
-      if (lane < kb) t[k0 + lane] = v;
-    }
-    __syncthreads();
-    for (int r = threadIdx.x; r < k0; r += blockDim.x) {
-      C acc = t[r];
-      for (int j = 0; j < kb; j++) {
-        const C u = Ai[(long long)(k0 + j) * n + r];
-        const C tj = t[k0 + j];
-        acc.x -= u.x * tj.x - u.y * tj.y;
-        acc.y -= u.x * tj.y + u.y * tj.x;
-      }
-      t[r] = acc;
-    }
-    __syncthreads();
-  }
-  for (int c = threadIdx.x; c < n; c += blockDim.x) Ti[c] = t[c];
 }
 
 // ------------------------------------------------------------------- build
@@ -543,150 +439,14 @@ __global__ void k_tri_inv_blocks(int n, int ld, const double2* __restrict__ A,
   }
 }
 
-// One CTA per factored mode f.  With pairing, the CTA also solves mode L-f:
-// B_{L-f} = D B_f D (D negates the x-component rows), so
-// x_{L-f} = D (B_f^{-1} (D b_{L-f})) reuses the same factors - each factor
-// element is read once for two right-hand sides.  Blocked forward/back
-// substitution: x_blk = inv(diag block) * t_blk, then a rank-kTrsvNb update of
-// the remaining rows (column-major factor panels, coalesced).
-template <typename R>
-__global__ void __launch_bounds__(512) k_pc_lu_solve2(PcGeom g, int paired,
-                                                      const Cx<R>* __restrict__ A,
-                                                      const Cx<R>* __restrict__ Dl,
-                                                      const Cx<R>* __restrict__ Du,
-                                                      const int* __restrict__ perm, Cx<R>* T,
-                                                      const int* skip) {
-  using C = Cx<R>;
-  constexpr int B = kTrsvNb;
-  if (skip && *skip) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int n = g.n3;
-  const int MN = n / 3;
-  const int nb = (n + B - 1) / B;
-  const int npad = nb * B;  // right-hand sides padded with zeros to whole blocks
-  C* t1 = reinterpret_cast<C*>(smem_raw);
-  C* t2 = t1 + npad;
-  __shared__ C xb1[B], xb2[B];
-  const int f = blockIdx.x;
-  const int i2 = g.L - f;
-  const bool two = paired && f != 0 && i2 != f;
-  const C* Af = A + (long long)f * n * n;
-  const int* pm = perm + (long long)f * n;
-  C* T1 = T + (long long)f * n;
-  C* T2 = T + (long long)(two ? i2 : f) * n;
-  const int tid = threadIdx.x;
-  for (int k = tid; k < npad; k += blockDim.x) {
-    C v1 = czero<C>(), v2 = czero<C>();
-    if (k < n) {
-      const int p = pm[k];
-      v1 = T1[p];
-      if (two) {
-        v2 = T2[p];
-        if (p < MN) v2 = cscale(v2, (R)-1);
-      }
-    }
-    t1[k] = v1;
-    t2[k] = v2;
-  }
-  __syncthreads();
-  const C* DL = Dl + (long long)f * nb * B * B;
-  const C* DU = Du + (long long)f * nb * B * B;
-  // x_blk = inv(diag block) * t_blk (padded blocks are identity on zeros):
-  // 32 independent loads per thread, fully unrolled.
-  auto diag = [&](const C* Dblk, int k0) {
-    if (tid < 2 * B) {
-      const int q = tid & (B - 1), which = tid / B;
-      if (which == 0 || two) {
-        const C* tv = (which ? t2 : t1) + k0;
-        const C* D = Dblk + q;
-        C acc = czero<C>();
-#pragma unroll
-        for (int c = 0; c < B; c++) cfma(acc, __ldg(D + c * B), tv[c]);
-        (which ? xb2 : xb1)[q] = acc;
-      }
-    }
-    __syncthreads();
-    if (tid < B) {
-      t1[k0 + tid] = xb1[tid];
-      if (two) t2[k0 + tid] = xb2[tid];
-    }
-  };
-  // t[r] -= sum_j F[r, k0+j] x_j for rows r in [r0, r1): column-major panel,
-  // coalesced across threads, 16 loads in flight per thread
-  auto update = [&](int k0, int kb, int r0, int r1) {
-    const C* col = Af + (long long)k0 * n;
-    for (int r = r0 + tid; r < r1; r += blockDim.x) {
-      C a1 = t1[r], a2 = t2[r];
-      if (kb == B) {
-#pragma unroll 16
-        for (int j = 0; j < B; j++) {
-          const C l = __ldg(col + (long long)j * n + r);
-          const C x1 = xb1[j];
-          a1.x -= l.x * x1.x - l.y * x1.y;
-          a1.y -= l.x * x1.y + l.y * x1.x;
-          if (two) {
-            const C x2 = xb2[j];
-            a2.x -= l.x * x2.x - l.y * x2.y;
-            a2.y -= l.x * x2.y + l.y * x2.x;
-          }
-        }
-      } else {
-        for (int j = 0; j < kb; j++) {
-          const C l = __ldg(col + (long long)j * n + r);
-          const C x1 = xb1[j];
-          a1.x -= l.x * x1.x - l.y * x1.y;
-          a1.y -= l.x * x1.y + l.y * x1.x;
-          if (two) {
-            const C x2 = xb2[j];
-            a2.x -= l.x * x2.x - l.y * x2.y;
-            a2.y -= l.x * x2.y + l.y * x2.x;
-          }
-        }
-      }
-      t1[r] = a1;
-      if (two) t2[r] = a2;
-    }
-    __syncthreads();
-  };
-  // forward substitution with the unit-lower L, then back substitution with U
-  for (int bk = 0; bk < nb; bk++) {
-    const int k0 = bk * B;
-    diag(DL + (long long)bk * B * B, k0);
-    update(k0, min(B, n - k0), k0 + B, n);
-  }
-  for (int bk = nb - 1; bk >= 0; bk--) {
-    const int k0 = bk * B;
-    diag(DU + (long long)bk * B * B, k0);
-    update(k0, min(B, n - k0), 0, k0);
-  }
-  for (int k = tid; k < n; k += blockDim.x) {
-    T1[k] = t1[k];
-    if (two) T2[k] = (k < MN) ? cscale(t2[k], (R)-1) : t2[k];
-  }
-}
-
 // ------------------------------------------ streamed LU solves (the apply)
 // The factors are static, so their 32 x 32 tiles are streamed through a ring
-// of shared-memory slots with cp.async, kRing-1 tiles in flight, in exactly
+// of shared-memory slots with cp.async, half the ring in flight, in exactly
 // the order the substitution consumes them; only the arithmetic waits on the
 // dependency chain.  Tile order: forward [Dl(k), L(c,k) for c > k] for
 // k = 0..nb-1, then backward [Du(k), U(c,k) for c < k] for k = nb-1..0.
 // Factor storage is padded to ld = nb*32 (zero rows/columns), so every tile
 // column is 32 contiguous, 16-byte aligned values.
-constexpr int kTileLd = 36;  // smem column stride of a tile (bank-conflict free)
-
-template <typename R> struct RingDepth;
-// ring depth: 4 slots keep 3 tiles in flight and fit 4 CTAs (c64) per SM, so
-// up to 592 factored modes run in a single wave on 148 SMs
-template <> struct RingDepth<float> { static constexpr int value = 4; };
-template <> struct RingDepth<double> { static constexpr int value = 3; };
-
-template <typename R>
-constexpr size_t lu_stream_smem(int npad) {
-  return (size_t)RingDepth<R>::value * kTrsvNb * kTileLd * sizeof(Cx<R>) +
-         2 * (size_t)npad * sizeof(Cx<R>);
-}
-
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -784,16 +544,45 @@ __global__ void k_tile_pack(int nb, int ld, const double2* __restrict__ A,
   }
 }
 
+// Second form of the streamed solve, with less issue overhead per tile: a tile
+// is consumed by one warp (lane = tile row, 32 column steps, no cross-lane
+// reduction), and up to kRoundTiles independent panel tiles of one block column
+// are consumed per barrier round, one per warp.  The two right-hand sides are
+// interleaved, so each factor value is read once from shared memory for both.
+// Tiles keep their HBM layout in shared memory (32 x 32, column-major).
+constexpr int kRoundTiles = 4;  // warps per CTA = panel tiles per round
+template <typename R> struct Ring2;
+template <> struct Ring2<float> { static constexpr int value = 8; };
+template <> struct Ring2<double> { static constexpr int value = 4; };
+
 template <typename R>
-__global__ void __launch_bounds__(256) k_pc_lu_stream(PcGeom g, int paired,
-                                                      const Cx<R>* __restrict__ tiles,
-                                                      const int* __restrict__ perm, Cx<R>* T,
-                                                      const int* skip) {
+constexpr size_t lu_stream2_smem(int npad) {
+  return (size_t)Ring2<R>::value * kTrsvNb * kTrsvNb * sizeof(Cx<R>) +
+         (size_t)npad * 2 * sizeof(Cx<R>) + (size_t)kTrsvNb * 2 * sizeof(Cx<R>);
+}
+
+__device__ __forceinline__ void cp_async_wait_n(int n) {
+  switch (n) {
+    case 0: cp_async_wait<0>(); break;
+    case 1: cp_async_wait<1>(); break;
+    case 2: cp_async_wait<2>(); break;
+    case 3: cp_async_wait<3>(); break;
+    case 4: cp_async_wait<4>(); break;
+    case 5: cp_async_wait<5>(); break;
+    case 6: cp_async_wait<6>(); break;
+    default: cp_async_wait<7>(); break;
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32 * kRoundTiles) k_pc_lu_stream2(
+    PcGeom g, int paired, const Cx<R>* __restrict__ tiles, const int* __restrict__ perm,
+    Cx<R>* T, const int* skip) {
   using C = Cx<R>;
   constexpr int B = kTrsvNb;
-  constexpr int S = RingDepth<R>::value;
-  constexpr int SLOT = B * kTileLd;
-  constexpr int PPC = B * (int)sizeof(C) / 16;  // 16-byte pieces per tile column
+  constexpr int S = Ring2<R>::value;
+  constexpr int TILE = B * B;
+  constexpr int PER = 16 / (int)sizeof(C);  // values per 16-byte piece
   if (skip && *skip) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* ring = reinterpret_cast<C*>(smem_raw);
@@ -801,31 +590,27 @@ __global__ void __launch_bounds__(256) k_pc_lu_stream(PcGeom g, int paired,
   const int MN = n / 3;
   const int nb = (n + B - 1) / B;
   const int npad = nb * B;
-  C* t1 = ring + S * SLOT;
-  C* t2 = t1 + npad;
-  __shared__ C xb[2][B];
+  C* t = ring + S * TILE;  // t[2*i] first right-hand side, t[2*i+1] second
+  C* xb = t + 2 * npad;    // xb[2*j], xb[2*j+1]
   const int f = blockIdx.x;
   const int i2 = g.L - f;
   const bool two = paired && f != 0 && i2 != f;
   const int total = lu_tiles(nb);
-  const C* tf = tiles + (long long)f * total * B * B;  // this mode's tile stream
+  const C* tf = tiles + (long long)f * total * TILE;
   const int* pm = perm + (long long)f * n;
   C* T1 = T + (long long)f * n;
   C* T2 = T + (long long)(two ? i2 : f) * n;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nthr = blockDim.x;
 
-  // tile i is 32*32 contiguous values: coalesced 16-byte pieces
-  auto issue = [&](int i, C* slot) {
-    const C* src = tf + (long long)i * B * B;
-    constexpr int per = 16 / (int)sizeof(C);
-    for (int p = tid; p < B * PPC; p += blockDim.x) {
-      const int j = p / PPC, q = p - j * PPC;
-      cp_async16(slot + j * kTileLd + q * per, src + j * B + q * per);
-    }
+  auto issue = [&](int i) {
+    const C* src = tf + (long long)i * TILE;
+    C* dst = ring + (i % S) * TILE;
+    for (int p = tid; p < TILE / PER; p += nthr) cp_async16(dst + p * PER, src + p * PER);
+    cp_async_commit();
   };
 
-  // right-hand sides: t = P (D b) for the paired mode
-  for (int k = tid; k < npad; k += blockDim.x) {
+  for (int k = tid; k < npad; k += nthr) {
     C v1 = czero<C>(), v2 = czero<C>();
     if (k < n) {
       const int p = pm[k];
@@ -835,90 +620,72 @@ __global__ void __launch_bounds__(256) k_pc_lu_stream(PcGeom g, int paired,
         if (p < MN) v2 = cscale(v2, (R)-1);
       }
     }
-    t1[k] = v1;
-    t2[k] = v2;
+    t[2 * k] = v1;
+    t[2 * k + 1] = v2;
   }
-
-  TileIt cons{0, 0, -1};
-  for (int s = 0; s < S - 1; s++) {
-    if (s < total) issue(s, ring + s * SLOT);
-    cp_async_commit();
-  }
-  // thread mapping for a tile: warp w -> right-hand side w>>2 and rows
-  // (w&3)*8 + (lane&7); lane>>3 picks 8 of the 32 tile columns
-  const int lane = tid & 31, w = tid >> 5;
-  const int which = w >> 2;
-  const int q = (w & 3) * 8 + (lane & 7);
-  const int jp = lane >> 3;
-  const bool active = which == 0 || two;
-  C* tv = which ? t2 : t1;
+  int issued = 0;
+  while (issued < total && issued < S) issue(issued++);
   __syncthreads();
-  for (int ci = 0; ci < total; ci++) {
-    const int pi = ci + S - 1;
-    if (pi < total) issue(pi, ring + (pi % S) * SLOT);
-    cp_async_commit();
-    cp_async_wait<S - 1>();
-    __syncthreads();
-    const C* tile = ring + (ci % S) * SLOT;
-    const int k0 = cons.k * B;
-    if (cons.c < 0) {
-      // x_blk = inv(diag block) * t_blk
-      C acc = czero<C>();
-      if (active) {
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-          const int j = jj * 4 + jp;
-          cfma(acc, tile[j * kTileLd + q], tv[k0 + j]);
-        }
-      }
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 8);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 8);
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 16);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 16);
-      if (active && jp == 0) xb[which][q] = acc;
-      __syncthreads();
-      if (active && jp == 0) tv[k0 + q] = acc;
-    } else {
-      // t_rows(c) -= tile * x_blk
-      C acc = czero<C>();
-      if (active) {
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-          const int j = jj * 4 + jp;
-          cfma(acc, tile[j * kTileLd + q], xb[which][j]);
-        }
-      }
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 8);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 8);
-      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 16);
-      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 16);
-      if (active && jp == 0) {
-        const int r = cons.c * B + q;
-        tv[r] = csub(tv[r], acc);
-      }
+
+  // at most half the ring is consumed per round, so the other half streams in
+  constexpr int RMAX = (S / 2 < kRoundTiles) ? S / 2 : kRoundTiles;
+  int ci = 0;
+  TileIt it{0, 0, -1};
+  while (ci < total) {
+    int r = 1;
+    if (it.c >= 0) {
+      // panel tiles left in this block column: forward c = it.c..nb-1,
+      // backward c = it.c..it.k-1
+      const int left = (it.phase == 0) ? nb - it.c : it.k - it.c;
+      r = min(RMAX, left);
     }
-    tile_next(cons, nb);
+    cp_async_wait_n(issued - (ci + r));
     __syncthreads();
+    const int k0 = it.k * B;
+    if (it.c < 0) {
+      if (warp == 0) {
+        // x = inv(diag block) * t_blk, both right-hand sides
+        const C* D = ring + (ci % S) * TILE;
+        C a1 = czero<C>(), a2 = czero<C>();
+#pragma unroll 8
+        for (int c = 0; c < B; c++) {
+          const C d = D[c * B + lane];
+          cfma(a1, d, t[2 * (k0 + c)]);
+          cfma(a2, d, t[2 * (k0 + c) + 1]);
+        }
+        __syncwarp();
+        xb[2 * lane] = a1;
+        xb[2 * lane + 1] = a2;
+        t[2 * (k0 + lane)] = a1;
+        t[2 * (k0 + lane) + 1] = a2;
+      }
+    } else if (warp < r) {
+      // t_rows(c) -= tile * x_blk, one tile per warp
+      const int ti = ci + warp;
+      const C* P = ring + (ti % S) * TILE;
+      const int row = (it.c + warp) * B + lane;
+      C a1 = t[2 * row], a2 = t[2 * row + 1];
+#pragma unroll 8
+      for (int j = 0; j < B; j++) {
+        const C v = P[j * B + lane];
+        const C x1 = xb[2 * j], x2 = xb[2 * j + 1];
+        a1.x -= v.x * x1.x - v.y * x1.y;
+        a1.y -= v.x * x1.y + v.y * x1.x;
+        a2.x -= v.x * x2.x - v.y * x2.y;
+        a2.y -= v.x * x2.y + v.y * x2.x;
+      }
+      t[2 * row] = a1;
+      t[2 * row + 1] = a2;
+    }
+    __syncthreads();
+    ci += r;
+    for (int q = 0; q < r; q++) tile_next(it, nb);
+    while (issued < total && issued < ci + S) issue(issued++);
   }
   cp_async_wait<0>();
-  for (int k = tid; k < n; k += blockDim.x) {
-    T1[k] = t1[k];
-    if (two) T2[k] = (k < MN) ? cscale(t2[k], (R)-1) : t2[k];
-  }
-}
-
-// Cast LU factors to precision R, scaling the upper triangle (U, with the
-// diagonal) of every n x n column-major block by s.
-template <typename R>
-__global__ void k_cast_scale_upper(long long tot, int n, const double2* __restrict__ src, double s,
-                                   Cx<R>* dst) {
-  const long long per = (long long)n * n;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long e = i % per;
-    const int col = (int)(e / n), row = (int)(e - (long long)col * n);
-    const double f = row <= col ? s : 1.0;
-    dst[i] = from_d2<Cx<R>>(make_double2(src[i].x * f, src[i].y * f));
+  for (int k = tid; k < n; k += nthr) {
+    T1[k] = t[2 * k];
+    if (two) T2[k] = (k < MN) ? cscale(t[2 * k + 1], (R)-1) : t[2 * k + 1];
   }
 }
 

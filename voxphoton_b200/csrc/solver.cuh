@@ -2,6 +2,10 @@
 // complex64 + FP64-refinement solver.  Included at the end of api.cu.
 #pragma once
 
+namespace vox {
+struct PcFactors;
+}
+
 struct vox_precond_s {
   vox_op_s* op = nullptr;
   PcGeom g{};
@@ -29,7 +33,7 @@ struct vox_precond_s {
   // Owner of the factor arrays above (Ad/Af/piv/perm/D*/tiles/tw): set once
   // construction succeeds; views made by vox_precond_share hold a copy, and the
   // arrays are freed with the last holder.  Work buffers T* are per handle.
-  std::shared_ptr<void> factors;
+  std::shared_ptr<vox::PcFactors> factors;
 };
 
 namespace vox {
@@ -65,7 +69,7 @@ static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaSt
   Cx<R>* T = pc_T<R>(p, 0);
   k_pc_xfwd<R><<<nb, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip);
   if (p->lu) {
-    k_pc_lu_stream<R><<<p->Lf, 256, lu_stream_smem<R>(lu_npad(g.n3)), st>>>(
+    k_pc_lu_stream2<R><<<p->Lf, 32 * kRoundTiles, lu_stream2_smem<R>(lu_npad(g.n3)), st>>>(
         g, p->paired, pc_tiles<R>(p), p->perm, T, skip);
   } else {
     Cx<R>* T2 = pc_T<R>(p, 1);
@@ -80,27 +84,22 @@ static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaSt
 }
 
 template <typename R>
-static vox_status pc_attrs(const PcGeom& g) {
-  const size_t cs = sizeof(Cx<R>);
-  VOX_CUDA(cudaFuncSetAttribute(k_pc_xfwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pc_xsmem(g, cs)));
-  VOX_CUDA(cudaFuncSetAttribute(k_pc_xinv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pc_xsmem(g, cs)));
-  VOX_CUDA(cudaFuncSetAttribute(k_pc_lu_stream<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)lu_stream_smem<R>(lu_npad(g.n3))));
-  VOX_CUDA(cudaFuncSetAttribute(k_pc_gemv<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(g.n3 * cs)));
-  VOX_CUDA(cudaFuncSetAttribute(k_lu_batched<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)((size_t)g.n3 * kLuNb * cs)));
+static vox_status pc_attrs() {
+  VOX_TRY(smem_cap(k_pc_xfwd<R>));
+  VOX_TRY(smem_cap(k_pc_xinv<R>));
+  VOX_TRY(smem_cap(k_pc_lu_stream2<R>));
+  VOX_TRY(smem_cap(k_pc_gemv<R>));
+  VOX_TRY(smem_cap(k_lu_batched<R>));
   return VOX_OK;
 }
 
-// Hand the factor arrays to a shared owner (called once a handle is complete).
-static void pc_seal(vox_precond_s* p) {
-  double2 *Ad = p->Ad, *Dld = p->Dld, *Dud = p->Dud, *td = p->tiles_d, *twd = p->twd;
-  float2 *Af = p->Af, *Dlf = p->Dlf, *Duf = p->Duf, *tf = p->tiles_f, *twf = p->twf;
-  int *piv = p->piv, *perm = p->perm;
-  p->factors = std::shared_ptr<void>(nullptr, [=](void*) {
+// The factor arrays of a finished preconditioner; freed when the last handle
+// (the original or a view made by vox_precond_share) lets go of them.
+struct PcFactors {
+  double2 *Ad = nullptr, *Dld = nullptr, *Dud = nullptr, *tiles_d = nullptr, *twd = nullptr;
+  float2 *Af = nullptr, *Dlf = nullptr, *Duf = nullptr, *tiles_f = nullptr, *twf = nullptr;
+  int *piv = nullptr, *perm = nullptr;
+  ~PcFactors() {
     cudaFree(Ad);
     cudaFree(Af);
     cudaFree(piv);
@@ -109,30 +108,49 @@ static void pc_seal(vox_precond_s* p) {
     cudaFree(Dud);
     cudaFree(Dlf);
     cudaFree(Duf);
-    cudaFree(td);
-    cudaFree(tf);
+    cudaFree(tiles_d);
+    cudaFree(tiles_f);
     cudaFree(twd);
     cudaFree(twf);
-  });
+  }
+};
+
+// Hand the factor arrays to a shared owner (called once a handle is complete).
+static void pc_seal(vox_precond_s* p) {
+  auto f = std::make_shared<PcFactors>();
+  f->Ad = p->Ad;
+  f->Dld = p->Dld;
+  f->Dud = p->Dud;
+  f->tiles_d = p->tiles_d;
+  f->twd = p->twd;
+  f->Af = p->Af;
+  f->Dlf = p->Dlf;
+  f->Duf = p->Duf;
+  f->tiles_f = p->tiles_f;
+  f->twf = p->twf;
+  f->piv = p->piv;
+  f->perm = p->perm;
+  p->factors = std::move(f);
 }
 
 static void pc_free(vox_precond_s* p) {
   if (!p) return;
   if (p->factors) {
-    p->factors.reset();
+    p->factors.reset();  // frees the arrays only if no view still holds them
   } else {  // construction did not complete: the arrays are still this handle's
-    cudaFree(p->Ad);
-    cudaFree(p->Af);
-    cudaFree(p->piv);
-    cudaFree(p->perm);
-    cudaFree(p->Dld);
-    cudaFree(p->Dud);
-    cudaFree(p->Dlf);
-    cudaFree(p->Duf);
-    cudaFree(p->tiles_d);
-    cudaFree(p->tiles_f);
-    cudaFree(p->twd);
-    cudaFree(p->twf);
+    PcFactors own;
+    own.Ad = p->Ad;
+    own.Dld = p->Dld;
+    own.Dud = p->Dud;
+    own.tiles_d = p->tiles_d;
+    own.twd = p->twd;
+    own.Af = p->Af;
+    own.Dlf = p->Dlf;
+    own.Duf = p->Duf;
+    own.tiles_f = p->tiles_f;
+    own.twf = p->twf;
+    own.piv = p->piv;
+    own.perm = p->perm;
   }
   cudaFree(p->Td);
   cudaFree(p->Td2);
@@ -156,11 +174,14 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   g.sx = pad_stride(g.L);
   const size_t per = 2ull * g.sx * sizeof(double2);
   g.ybx = (int)std::max<size_t>(1, std::min<size_t>(8, kSmemBudget / per));
-  if (per > 220 * 1024) {
+  if (per > (size_t)kSmemCap) {
     set_error("preconditioner: L too long for the shared-memory FFT");
     return VOX_ERR_UNSUPPORTED;
   }
-  if ((size_t)g.n3 * kLuNb * sizeof(double2) > 220 * 1024) {
+  // the LU panel bound (n3 <= 1760) also keeps the streamed solve's
+  // ring + right-hand sides (64 KiB + 32 B * n3) under the cap
+  if ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
+      lu_stream2_smem<double>(lu_npad(g.n3)) > (size_t)kSmemCap) {
     set_error("preconditioner: 3*M*N too large for the batched LU panel");
     return VOX_ERR_UNSUPPORTED;
   }
@@ -176,8 +197,8 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   VOX_TRY(dalloc(&p->Td2, LT));
   VOX_TRY(dalloc(&p->Tf, LT));
   VOX_TRY(dalloc(&p->Tf2, LT));
-  VOX_TRY(pc_attrs<double>(g));
-  VOX_TRY(pc_attrs<float>(g));
+  VOX_TRY(pc_attrs<double>());
+  VOX_TRY(pc_attrs<float>());
   return VOX_OK;
 }
 
@@ -909,9 +930,8 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     });
     out[4] = timeit([&] {
       if (pc->lu)
-        k_pc_lu_stream<R><<<pc->Lf, 256, lu_stream_smem<R>(lu_npad(pg.n3)), st>>>(
-            pg, pc->paired, pc_tiles<R>(pc), pc->perm, T,
-            nullptr);
+        k_pc_lu_stream2<R><<<pc->Lf, 32 * kRoundTiles, lu_stream2_smem<R>(lu_npad(pg.n3)),
+                             st>>>(pg, pc->paired, pc_tiles<R>(pc), pc->perm, T, nullptr);
       else
         k_pc_gemv<R><<<pg.L * ((pg.n3 + 255) / 256), 256, (size_t)pg.n3 * cs, st>>>(
             pg, pc_A<R>(pc), T, pc_T<R>(pc, 1), nullptr);
