@@ -177,6 +177,8 @@ def bragg_config(name):
         return bragg(res=20e-9, M=30)
     if name == "bragg10":
         return bragg(res=10e-9, M=60)
+    if name.startswith("bragg20-p"):  # e.g. bragg20-p20: 20 periods -> 520 x 30 x 11
+        return bragg(periods=int(name[len("bragg20-p"):]), res=20e-9, M=30)
     raise KeyError(name)
 
 

@@ -215,6 +215,15 @@ class SweepServer:
                                       _lib.dptr(xre), _lib.dptr(xim), ctypes.byref(info)))
         return info, (xre + 1j * xim if c.keep_x else None)
 
+    def solve_one(self, fam: Family, req: Request, slot=0):
+        """One request on one slot of its family, on the calling thread."""
+        op, pc = fam.slots[slot]
+        t0 = time.perf_counter()
+        info, x = self._solve(fam, op, pc, req)
+        t1 = time.perf_counter()
+        return Result(req.rid, req.key, req.lam, 0.0, 0.0, t1 - t0, info.total_iters,
+                      info.relres, info.flag, x)
+
     def serve(self, requests, realtime=True):
         """Run the stream; returns (results, wall seconds)."""
         queues = {k: deque() for k in self.families}
