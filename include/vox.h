@@ -102,6 +102,17 @@ const char* vox_last_error(void);
 int vox_abi_version(void);
 
 vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out);
+/* An operator with `members` (1..8) independent copies of fN and of all solve
+ * state, sharing grid, support idx, Mr, Mc and Gram: the co-resident
+ * same-shape solves of a serving loop (e.g. one device at several
+ * wavelengths), which vox_solve_refined_batch advances in lockstep with one
+ * launch per kernel for all of them.  Every member starts with desc's fN; set
+ * a member's operator with vox_op_interp_member.  The single-right-hand-side
+ * entry points act on member 0.  No reference counterpart (MATLAB solves one
+ * system per call). */
+vox_status vox_op_create_batch(const vox_op_desc* desc, int members, vox_op_t* out);
+/* Number of members (1 for vox_op_create). */
+vox_status vox_op_members(vox_op_t op, int* members);
 void vox_op_destroy(vox_op_t op);
 /* Sizes chosen for the device matvec: padded grid and vector length. */
 vox_status vox_op_info(vox_op_t op, int* Px, int* Py, int* Pz, long long* n);
@@ -116,11 +127,15 @@ vox_status vox_op_stats(vox_op_t op, long long* launches);
  * wavelength interpolation of the operator between Legendre nodes.  Enqueued
  * on dst's stream; Mr, Mc, Gram and idx of dst are unchanged. */
 vox_status vox_op_interp(vox_op_t dst, const vox_op_t* srcs, const double* w, int n);
+/* The same for one member of a batched dst (the sources' member 0). */
+vox_status vox_op_interp_member(vox_op_t dst, int member, const vox_op_t* srcs, const double* w,
+                                int n);
 /* Storage flags: bit 0 set when fN is kept as one octant (the transformed
  * circulant has the per-axis parity of the Green tensor). */
 vox_status vox_op_flags(vox_op_t op, int* flags);
 /* Device time (ms, CUDA events on the operator's stream, mean of reps) of each
- * kernel of one GMRES iteration: [0..2] matvec x-forward / plane / x-inverse,
+ * kernel of one GMRES iteration, launched for all members of the operator:
+ * [0..2] matvec x-forward / plane / x-inverse,
  * [3..5] preconditioner x-forward / per-mode solve / x-inverse (0 if pc is
  * NULL), [6..9] Gram-Schmidt dots / update+dots / update+norm / scale at a
  * basis of kgs+1 vectors.  ms_out holds 10 doubles. */
@@ -198,6 +213,23 @@ vox_status vox_pgmres_device(vox_op_t op, vox_precond_t pc, int side, vox_prec p
 vox_status vox_solve_refined_device(vox_op_t op, vox_precond_t pc, int side, const void* b,
                                     double tol, int restart, int maxit_inner, double inner_tol,
                                     int max_refine, void* x, vox_gmres_info* info);
+
+/* vox_solve_refined for `count` (1..members) right-hand sides at once on the
+ * members 0..count-1 of a batched operator: b and x hold count vectors of
+ * n_idx, member-major; infos holds count records.  The solves advance in
+ * lockstep (one launch per kernel for all members; the preconditioner's
+ * factors are read once for all of them), and each member's result is
+ * identical to solving it alone.  No reference counterpart. */
+vox_status vox_solve_refined_batch(vox_op_t op, vox_precond_t pc, int side, int count,
+                                   const double* b_re, const double* b_im, double tol,
+                                   int restart, int maxit_inner, double inner_tol,
+                                   int max_refine, double* x_re, double* x_im,
+                                   vox_gmres_info* infos);
+/* Device variant: b and x are count interleaved double2 device vectors of n. */
+vox_status vox_solve_refined_batch_device(vox_op_t op, vox_precond_t pc, int side, int count,
+                                          const void* b, double tol, int restart,
+                                          int maxit_inner, double inner_tol, int max_refine,
+                                          void* x, vox_gmres_info* infos);
 
 /* Vrhs = Gram * (j omega eo Mc_raw) .* Einc(idx) ./ Mr(idx)  (JVIE-II), with
  * Mc_raw = e_r - 1, Mr = e_r; e_r and Einc column-major (L x M x N, x3 for Einc). */

@@ -123,6 +123,23 @@ SIGNATURES = [
                                         ctypes.POINTER(ctypes.c_int)]),
     ("vox_profile_stages", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]),
+    ("vox_op_create_batch", ctypes.c_int, [ctypes.POINTER(OpDesc), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    ("vox_op_members", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    ("vox_op_interp_member", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p), _dp, ctypes.c_int]),
+    ("vox_solve_refined_batch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_int, _dp, _dp, ctypes.c_double,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_int, _dp, _dp,
+                                               ctypes.POINTER(GmresInfo)]),
+    ("vox_solve_refined_batch_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                                      ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_void_p, ctypes.c_double,
+                                                      ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_double, ctypes.c_int,
+                                                      ctypes.c_void_p,
+                                                      ctypes.POINTER(GmresInfo)]),
 ]
 
 _LIB = None

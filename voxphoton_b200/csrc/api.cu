@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -14,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/vox.h"
@@ -126,35 +128,56 @@ struct DeviceGuard {
     if (s__ != VOX_OK) return s__;  \
   } while (0)
 
-// GMRES workspace for one precision and restart length.
+// Bytes of a GmresDev record read back per cycle (everything before sn).
+constexpr size_t kGmresHdr = (offsetof(GmresDev, sn) + 15) / 16 * 16;
+
+// GMRES workspace for one precision and restart length, for every member of
+// the operator.  Member b's vectors form one arena, vs elements after member
+// 0's: [V (m+1 columns) | w | t | r | x | b], each column ldv elements long.
 template <typename R>
 struct GmresWork {
   int m = 0;
-  Cx<R>* V = nullptr;  // (m+1) x n
+  int K = 0;
+  long long ldv = 0;        // column length (n rounded up to 32)
+  long long vs = 0;         // member stride = (m + 6) * ldv
+  Cx<R>* arena = nullptr;
+  Cx<R>* V = nullptr;       // member 0's pointers into the arena
   Cx<R>* w = nullptr;
-  Cx<R>* t = nullptr;  // preconditioner output / right-precond temp
+  Cx<R>* t = nullptr;       // preconditioner output / right-precond temp
   Cx<R>* r = nullptr;
   Cx<R>* x = nullptr;
   Cx<R>* b = nullptr;
-  GmresDev* st = nullptr;
-  GmresDev* hst = nullptr;  // pinned host mirror for readback
-  std::map<std::pair<void*, int>, cudaGraphExec_t> graphs;  // (precond, side) -> cycle
+  GmresDev* st = nullptr;   // K records
+  unsigned char* hst = nullptr;  // pinned: K headers of kGmresHdr bytes
+  int* hflag = nullptr;          // pinned: K frozen flags
+  double* hscal = nullptr;       // pinned: K scalars
+  // (precond, side, members launched) -> captured cycle
+  std::map<std::tuple<void*, int, int>, cudaGraphExec_t> graphs;
+  GmresDev* hdr(int mb) { return reinterpret_cast<GmresDev*>(hst + (size_t)mb * kGmresHdr); }
+  template <typename T> T* mem(T* p, int mb) const { return p + mb * vs; }
   void release() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     graphs.clear();
-    cudaFree(V);
-    cudaFree(w);
-    cudaFree(t);
-    cudaFree(r);
-    cudaFree(x);
-    cudaFree(b);
+    cudaFree(arena);
     cudaFree(st);
     if (hst) cudaFreeHost(hst);
-    V = w = t = r = x = b = nullptr;
+    if (hflag) cudaFreeHost(hflag);
+    if (hscal) cudaFreeHost(hscal);
+    arena = V = w = t = r = x = b = nullptr;
     st = nullptr;
     hst = nullptr;
+    hflag = nullptr;
+    hscal = nullptr;
+    m = 0;
   }
 };
+
+// members of one operator: the streamed LU solve takes up to 16 columns
+constexpr int kMaxMembers = 8;
+
+// int stride between the skip flags of consecutive members (GmresDev::done)
+constexpr int kFlagStride = (int)(sizeof(GmresDev) / sizeof(int));
+static_assert(sizeof(GmresDev) % sizeof(int) == 0, "GmresDev size");
 
 }  // namespace vox
 
@@ -162,6 +185,7 @@ using namespace vox;
 
 struct vox_op_s {
   int device = 0;
+  int K = 1;                          // members (independent solves of this shape)
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;  // created here; `stream` may be the caller's
   long long launches = 0;             // kernels launched by solver entry points
@@ -174,17 +198,13 @@ struct vox_op_s {
   OpBuffers<float> f;
   double gram = 0;
   // host staging (pinned) and device vectors for host-buffer entry points
+  // (K vectors of n for d_in/d_out and the host buffers)
   double2* h_in = nullptr;
   double2* h_out = nullptr;
   double2* d_in = nullptr;
   double2* d_out = nullptr;
   float2* f_in = nullptr;
   float2* f_out = nullptr;
-  // refinement workspace (c128 x, r, b) and casts
-  double2* x64 = nullptr;
-  double2* r64 = nullptr;
-  double2* b64 = nullptr;
-  GmresDev* st64 = nullptr;  // scratch for norms in the refinement loop
   GmresWork<double> wd;
   GmresWork<float> wf;
   std::vector<vox_precond_s*> pcs;
@@ -205,21 +225,35 @@ static size_t psmem(const OpGeom& g, size_t csz) {
   return ((size_t)3 * g.N * g.sy + 2 * wsize) * csz;
 }
 
+// Members taking part in one launch: km members starting at m0 (their fN
+// and plane scratch), vectors vs elements apart, skip flags fs ints apart.
+struct Members {
+  int km = 1;
+  int m0 = 0;
+  long long vs = 0;
+  int fs = 0;
+};
+
 // Launch the three matvec kernels.
 template <typename R>
 static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cudaStream_t st,
-                         const int* skip) {
+                         const int* skip, Members mm = Members()) {
   OpBuffers<R>& b = bufs<R>(op);
   const OpGeom& g = b.geo;
   const size_t cs = sizeof(Cx<R>);
-  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3);
+  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3 * mm.km);
+  dim3 gp(g.Px, mm.km);
   const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
-  k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, b.T1,
-                                            skip);
-  k_plane<R><<<g.Px, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, b.T1, b.fN, b.T2,
-                                               skip);
-  k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, in, b.Mr, b.Mc,
-                                            b.gram, scale, b.out_scale, mode, out, skip);
+  Cx<R>* T1 = b.T1 + mm.m0 * plane_elems(g);
+  Cx<R>* T2 = b.T2 + mm.m0 * plane_elems(g);
+  const Cx<R>* fN = b.fN + mm.m0 * fN_elems(g);
+  k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1, skip,
+                                            mm.vs, mm.fs);
+  k_plane<R><<<gp, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1, fN, T2, skip,
+                                             mm.fs);
+  k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
+                                            b.gram, scale, b.out_scale, mode, out, skip, mm.vs,
+                                            mm.fs);
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
 }
@@ -346,15 +380,18 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
   const OpGeom& g = b.geo;
   const long long P = (long long)g.Px * g.Py * g.Pz;
   cudaStream_t st = op->stream;
+  const long long fe = fN_elems(g);
+  VOX_TRY(dalloc(&b.fN, fe * op->K));
   if (g.sym) {
-    const long long H = (long long)(g.Px / 2 + 1) * (g.Py / 2 + 1) * (g.Pz / 2 + 1);
-    VOX_TRY(dalloc(&b.fN, 6 * H));
-    k_pack_fN_sym<R><<<nblk(6 * H), 256, 0, st>>>(g, fN_packed_src, scale, b.fN);
+    k_pack_fN_sym<R><<<nblk(fe), 256, 0, st>>>(g, fN_packed_src, scale, b.fN);
   } else {
-    VOX_TRY(dalloc(&b.fN, 6 * P));
-    k_pack_fN<R><<<nblk(6 * P), 256, 0, st>>>(P, fN_packed_src, scale, b.fN);
+    k_pack_fN<R><<<nblk(fe), 256, 0, st>>>(P, fN_packed_src, scale, b.fN);
   }
   VOX_CUDA(cudaGetLastError());
+  // every member starts as a copy of member 0
+  for (int mb = 1; mb < op->K; mb++)
+    VOX_CUDA(cudaMemcpyAsync(b.fN + mb * fe, b.fN, fe * sizeof(Cx<R>), cudaMemcpyDeviceToDevice,
+                             st));
   double2* tmp;
   VOX_TRY(dalloc(&tmp, g.V));
   if (has_Mr) {
@@ -378,9 +415,9 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
   VOX_TRY(up_tw(g.Px, &b.twX));
   VOX_TRY(up_tw(g.Py, &b.twY));
   VOX_TRY(up_tw(g.Pz, &b.twZ));
-  const long long tsz = (long long)g.Px * 3 * g.N * g.M;
-  VOX_TRY(dalloc(&b.T1, tsz));
-  VOX_TRY(dalloc(&b.T2, tsz));
+  const long long tsz = plane_elems(g);
+  VOX_TRY(dalloc(&b.T1, tsz * op->K));
+  VOX_TRY(dalloc(&b.T2, tsz * op->K));
   VOX_TRY(set_smem_attrs<R>());
   return VOX_OK;
 }
@@ -419,10 +456,6 @@ static void destroy_op(vox_op_s* op) {
   cudaFree(op->d_out);
   cudaFree(op->f_in);
   cudaFree(op->f_out);
-  cudaFree(op->x64);
-  cudaFree(op->r64);
-  cudaFree(op->b64);
-  cudaFree(op->st64);
   if (op->own_stream) cudaStreamDestroy(op->own_stream);
   delete op;
 }
@@ -435,13 +468,27 @@ extern "C" {
 const char* vox_last_error(void) { return vox::last_error(); }
 int vox_abi_version(void) { return VOX_ABI_VERSION; }
 
+static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out);
+
 vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out) {
+  return create_op(desc, 1, out);
+}
+
+vox_status vox_op_create_batch(const vox_op_desc* desc, int members, vox_op_t* out) {
+  return create_op(desc, members, out);
+}
+
+static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
   cudaGetLastError();  // drop a stale error left by an unrelated earlier call
   if (!desc || !out) {
     set_error("vox_op_create: NULL argument");
     return VOX_ERR_BAD_ARG;
   }
   *out = nullptr;
+  if (K < 1 || K > kMaxMembers) {
+    set_error("vox_op_create: members must be 1.." + std::to_string(kMaxMembers));
+    return VOX_ERR_BAD_ARG;
+  }
   const int L = desc->L, M = desc->M, N = desc->N;
   if (L < 1 || M < 1 || N < 1) {
     set_error("vox_op_create: grid dimensions must be positive");
@@ -473,6 +520,7 @@ vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out) {
   int precs = desc->precisions ? desc->precisions : 3;
   std::unique_ptr<vox_op_s, void (*)(vox_op_s*)> op(new vox_op_s(), destroy_op);
   op->device = desc->device;
+  op->K = K;
   DeviceGuard dg(op->device);
   VOX_CUDA(cudaSetDevice(op->device));
   VOX_CUDA(cudaStreamCreateWithFlags(&op->own_stream, cudaStreamNonBlocking));
@@ -601,10 +649,10 @@ vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out) {
   }
   // staging for host-buffer entry points
   const long long n = g.n;
-  VOX_CUDA(cudaMallocHost((void**)&op->h_in, n * sizeof(double2)));
-  VOX_CUDA(cudaMallocHost((void**)&op->h_out, n * sizeof(double2)));
-  VOX_TRY(dalloc(&op->d_in, n));
-  VOX_TRY(dalloc(&op->d_out, n));
+  VOX_CUDA(cudaMallocHost((void**)&op->h_in, K * n * sizeof(double2)));
+  VOX_CUDA(cudaMallocHost((void**)&op->h_out, K * n * sizeof(double2)));
+  VOX_TRY(dalloc(&op->d_in, K * n));
+  VOX_TRY(dalloc(&op->d_out, K * n));
   VOX_TRY(dalloc(&op->f_in, n));
   VOX_TRY(dalloc(&op->f_out, n));
   VOX_CUDA(cudaStreamSynchronize(st));
@@ -775,11 +823,11 @@ static vox_status matvec_noalloc(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>*
   dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3);
   const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
   k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1,
-                                            nullptr);
+                                            nullptr, 0, 0);
   k_plane<R><<<g.Px, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1, b.fN, T2,
-                                               nullptr);
+                                               nullptr, 0);
   k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
-                                            b.gram, scale, b.out_scale, mode, out, nullptr);
+                                            b.gram, scale, b.out_scale, mode, out, nullptr, 0, 0);
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
 }

@@ -10,6 +10,13 @@
 //
 // Reductions are deterministic: every CTA writes its partial sums, and the
 // last CTA to finish (atomic ticket) adds them in block order.
+//
+// Members: one launch serves every member of a batched operator (independent
+// solves of the same shape).  The member is blockIdx.y; member b's vectors sit
+// b * vs elements after member 0's (one workspace arena per member) and its
+// state is st[b].  A member whose solve has finished is `frozen`: every kernel
+// of the cycle leaves it untouched, so each member runs exactly the cycles it
+// would run alone and its arithmetic does not depend on the other members.
 #pragma once
 
 #include "vox_common.cuh"
@@ -27,6 +34,7 @@ struct GmresDev {
   int breakdown;     // H(k+1,k) == 0
   unsigned ticket;   // last-block counter
   int m;             // restart length
+  int frozen;        // member takes no part in this cycle (batched launches)
   double tol_abs;    // tol * bnorm
   double beta;       // ||r|| at cycle start
   double inv_norm;   // 1/H(k+1,k) for the pending basis vector
@@ -152,8 +160,11 @@ template <typename R>
 __global__ void __launch_bounds__(kRedThreads) k_gs_dots(GmresDev* st, int k,
                                                          const Cx<R>* __restrict__ V,
                                                          long long ldv, const Cx<R>* __restrict__ w,
-                                                         long long n) {
+                                                         long long n, long long vs) {
   __shared__ double2 sh[32];
+  st += blockIdx.y;
+  V += blockIdx.y * vs;
+  w += blockIdx.y * vs;
   if (st->done) return;
   cta_dots<R>(V, ldv, k + 1, w, n, st->partial, sh);
   if (last_block(&st->ticket)) {
@@ -167,9 +178,12 @@ template <typename R>
 __global__ void __launch_bounds__(kRedThreads) k_gs_update_dots(GmresDev* st, int k,
                                                                 const Cx<R>* __restrict__ V,
                                                                 long long ldv, Cx<R>* w,
-                                                                long long n) {
+                                                                long long n, long long vs) {
   __shared__ double2 sh[32];
   __shared__ Cx<R> hs[kMaxRestart + 1];
+  st += blockIdx.y;
+  V += blockIdx.y * vs;
+  w += blockIdx.y * vs;
   if (st->done) return;
   const int nj = k + 1;
   for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<Cx<R>>(st->h1[j]);
@@ -223,9 +237,12 @@ template <typename R>
 __global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, int k,
                                                                 const Cx<R>* __restrict__ V,
                                                                 long long ldv, Cx<R>* w,
-                                                                long long n) {
+                                                                long long n, long long vs) {
   __shared__ double2 sh[32];
   __shared__ Cx<R> hs[kMaxRestart + 1];
+  st += blockIdx.y;
+  V += blockIdx.y * vs;
+  w += blockIdx.y * vs;
   if (st->done) return;
   const int nj = k + 1;
   for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<Cx<R>>(st->h2[j]);
@@ -298,8 +315,11 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, in
 // that step ended the cycle: the restart residual V(:,1:k+1)*res needs it.
 template <typename R>
 __global__ void k_gs_scale(GmresDev* st, int k, Cx<R>* __restrict__ Vnext,
-                           const Cx<R>* __restrict__ w, long long n) {
-  if (st->k != k + 1) return;
+                           const Cx<R>* __restrict__ w, long long n, long long vs) {
+  st += blockIdx.y;
+  Vnext += blockIdx.y * vs;
+  w += blockIdx.y * vs;
+  if (st->frozen || st->k != k + 1) return;
   const R s = (R)st->inv_norm;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -307,11 +327,16 @@ __global__ void k_gs_scale(GmresDev* st, int k, Cx<R>* __restrict__ Vnext,
   }
 }
 
-// ||x||^2 -> st->scal[slot] (deterministic, grid = kRedBlocks)
+// ||x||^2 -> st->scal[slot] (deterministic, grid = (kRedBlocks, members));
+// with `in_cycle` a frozen member is skipped.
 template <typename R>
 __global__ void __launch_bounds__(kRedThreads) k_norm2(GmresDev* st, const Cx<R>* __restrict__ x,
-                                                       long long n, int slot) {
+                                                       long long n, int slot, long long vs,
+                                                       int in_cycle) {
   __shared__ double2 sh[32];
+  st += blockIdx.y;
+  x += blockIdx.y * vs;
+  if (in_cycle && st->frozen) return;
   double2 acc = make_double2(0.0, 0.0);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -331,7 +356,16 @@ __global__ void __launch_bounds__(kRedThreads) k_norm2(GmresDev* st, const Cx<R>
 }
 
 // Start a cycle: beta = sqrt(scal[0]); V(:,0) = r / beta; g = beta e1.
+// A frozen member ends its cycle before it starts (done, k = 0).
 __global__ void k_cycle_init(GmresDev* st) {
+  st += blockIdx.y;
+  if (st->frozen) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+      st->done = 1;
+      st->k = 0;
+    }
+    return;
+  }
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     st->beta = sqrt(st->scal[0]);
     st->inv_norm = st->beta > 0.0 ? 1.0 / st->beta : 0.0;
@@ -346,7 +380,11 @@ __global__ void k_cycle_init(GmresDev* st) {
 
 template <typename R>
 __global__ void k_cycle_v0(const GmresDev* st, Cx<R>* __restrict__ V0, const Cx<R>* __restrict__ r,
-                           long long n) {
+                           long long n, long long vs) {
+  st += blockIdx.y;
+  V0 += blockIdx.y * vs;
+  r += blockIdx.y * vs;
+  if (st->frozen) return;
   const R s = (R)st->inv_norm;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -357,7 +395,8 @@ __global__ void k_cycle_v0(const GmresDev* st, Cx<R>* __restrict__ V0, const Cx<
 // Least squares after the cycle: y = Rm(0:kk-1,0:kk-1) \ g(0:kk-1) (back
 // substitution), res = beta e1 - H(0:kk,0:kk-1) y  (pgmres_iter.m:117-119).
 __global__ void k_cycle_ls(GmresDev* st) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  st += blockIdx.y;
+  if (threadIdx.x != 0 || blockIdx.x != 0 || st->frozen) return;
   const int kk = st->k;
   const int ld = st->m + 1;
   for (int i = kk - 1; i >= 0; i--) {
@@ -388,9 +427,14 @@ __global__ void k_cycle_ls(GmresDev* st) {
 // x += V(:,0:kk-1) y ; r = V(:,0:kk) res   (pgmres_iter.m:133-150, no right preconditioner)
 template <typename R>
 __global__ void k_cycle_update(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
-                               Cx<R>* x, Cx<R>* r, long long n) {
+                               Cx<R>* x, Cx<R>* r, long long n, long long vs) {
   __shared__ Cx<R> ys[kMaxRestart];
   __shared__ Cx<R> rs[kMaxRestart + 1];
+  st += blockIdx.y;
+  V += blockIdx.y * vs;
+  if (x) x += blockIdx.y * vs;
+  r += blockIdx.y * vs;
+  if (st->frozen) return;
   const int kk = st->k;
   for (int j = threadIdx.x; j <= kk; j += blockDim.x) {
     if (j < kk) ys[j] = from_d2<Cx<R>>(st->y[j]);
@@ -414,8 +458,12 @@ __global__ void k_cycle_update(const GmresDev* st, const Cx<R>* __restrict__ V, 
 // y = V(:,0:kk-1) * ys (for the right-preconditioned update, into a temp)
 template <typename R>
 __global__ void k_cycle_vy(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
-                           Cx<R>* out, long long n) {
+                           Cx<R>* out, long long n, long long vs) {
   __shared__ Cx<R> ys[kMaxRestart];
+  st += blockIdx.y;
+  V += blockIdx.y * vs;
+  out += blockIdx.y * vs;
+  if (st->frozen) return;
   const int kk = st->k;
   for (int j = threadIdx.x; j < kk; j += blockDim.x) ys[j] = from_d2<Cx<R>>(st->y[j]);
   __syncthreads();
@@ -429,7 +477,12 @@ __global__ void k_cycle_vy(const GmresDev* st, const Cx<R>* __restrict__ V, long
 
 // elementwise helpers
 template <typename R>
-__global__ void k_axpy(Cx<R>* y, const Cx<R>* __restrict__ x, long long n) {
+__global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x, long long n,
+                       long long vs) {
+  st += blockIdx.y;
+  y += blockIdx.y * vs;
+  x += blockIdx.y * vs;
+  if (st->frozen) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     y[i] = cadd(y[i], x[i]);

@@ -57,21 +57,37 @@ struct OpBuffers {
 
 inline int pad_stride(int n) { return (n % 2 == 0) ? n + 1 : n; }
 
+// Members of a batched operator (independent solves of one shape, launched
+// together): member b's plane scratch and fN follow member 0's at the strides
+// below; its input/output vectors are vs elements apart and its skip flag fs
+// ints apart.  A single-member launch has b = 0 throughout.
+__host__ __device__ inline long long plane_elems(const OpGeom& g) {
+  return (long long)g.Px * 3 * g.N * g.M;
+}
+__host__ __device__ inline long long fN_elems(const OpGeom& g) {
+  if (g.sym) return 6LL * (g.Px / 2 + 1) * (g.Py / 2 + 1) * (g.Pz / 2 + 1);
+  return 6LL * g.Px * g.Py * g.Pz;
+}
+
 // ---------------------------------------------------------------- kernel 1
 template <typename R>
 __global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>* __restrict__ tw,
                                               const Cx<R>* __restrict__ in,
                                               const int* __restrict__ vmap,
                                               const Cx<R>* __restrict__ Mc, int mode,
-                                              Cx<R>* __restrict__ T1, const int* skip) {
+                                              Cx<R>* __restrict__ T1, const int* skip,
+                                              long long vs, int fs) {
   using C = Cx<R>;
-  if (skip && *skip) return;
+  const int mb = blockIdx.z / 3;
+  if (skip && skip[(long long)mb * fs]) return;
+  in += mb * vs;
+  T1 += mb * plane_elems(g);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int y0 = blockIdx.x * g.ybx;
   const int z = blockIdx.y;
-  const int c = blockIdx.z;
+  const int c = blockIdx.z - 3 * mb;
   const int YB = g.ybx;
   const long long cellbase = (long long)g.L * ((long long)g.M * z);
   // gather J along x for YB pencils; zero-pad
@@ -110,9 +126,13 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
                                                const Cx<R>* __restrict__ twZ,
                                                const Cx<R>* __restrict__ T1,
                                                const Cx<R>* __restrict__ fN,
-                                               Cx<R>* __restrict__ T2, const int* skip) {
+                                               Cx<R>* __restrict__ T2, const int* skip, int fs) {
   using C = Cx<R>;
-  if (skip && *skip) return;
+  const int mb = blockIdx.y;
+  if (skip && skip[(long long)mb * fs]) return;
+  T1 += mb * plane_elems(g);
+  T2 += mb * plane_elems(g);
+  fN += mb * fN_elems(g);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int rows = 3 * g.N;
   C* ybuf = reinterpret_cast<C*>(smem_raw);          // [3N][sy]
@@ -228,15 +248,19 @@ __global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>*
                                               const Cx<R>* in, const Cx<R>* __restrict__ Mr,
                                               const Cx<R>* __restrict__ Mc, R gram, R scale,
                                               R out_scale, int mode, Cx<R>* out,
-                                              const int* skip) {
+                                              const int* skip, long long vs, int fs) {
   using C = Cx<R>;
-  if (skip && *skip) return;
+  const int mb = blockIdx.z / 3;
+  if (skip && skip[(long long)mb * fs]) return;
+  T2 += mb * plane_elems(g);
+  in += mb * vs;
+  out += mb * vs;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int y0 = blockIdx.x * g.ybx;
   const int z = blockIdx.y;
-  const int c = blockIdx.z;
+  const int c = blockIdx.z - 3 * mb;
   const int YB = g.ybx;
   const int ny = min(YB, g.M - y0);
   for (int t = threadIdx.x; t < YB * g.Px; t += blockDim.x) {

@@ -37,14 +37,26 @@ struct PcGeom {
   int sx;          // smem stride of a line
 };
 
+// Members of a batched apply (blockIdx.y, or one CTA for all members in the
+// streamed solve): member b's x-transformed work follows member 0's at
+// L*n3 elements, its input/output vectors at vs elements, its skip flag at fs
+// ints.
+__host__ __device__ inline long long pc_work_elems(const PcGeom& g) {
+  return (long long)g.L * g.n3;
+}
+
 // --------------------------------------------------------------- apply: x-FFT
 template <typename R>
 __global__ void __launch_bounds__(256) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
                                                  const Cx<R>* __restrict__ in,
                                                  const int* __restrict__ vmap,
-                                                 Cx<R>* __restrict__ T, const int* skip) {
+                                                 Cx<R>* __restrict__ T, const int* skip,
+                                                 long long vs, int fs) {
   using C = Cx<R>;
-  if (skip && *skip) return;
+  const int mb = blockIdx.y;
+  if (skip && skip[(long long)mb * fs]) return;
+  in += mb * vs;
+  T += mb * pc_work_elems(g);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
@@ -73,9 +85,13 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_pc_xinv(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
                                                  const Cx<R>* __restrict__ T,
                                                  const int* __restrict__ vmap, R scale,
-                                                 Cx<R>* out, const int* skip) {
+                                                 Cx<R>* out, const int* skip, long long vs,
+                                                 int fs) {
   using C = Cx<R>;
-  if (skip && *skip) return;
+  const int mb = blockIdx.y;
+  if (skip && skip[(long long)mb * fs]) return;
+  T += mb * pc_work_elems(g);
+  out += mb * vs;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
@@ -101,9 +117,13 @@ __global__ void __launch_bounds__(256) k_pc_xinv(PcGeom g, FftPlan pl, const Cx<
 template <typename R>
 __global__ void __launch_bounds__(256) k_pc_gemv(PcGeom g, const Cx<R>* __restrict__ B,
                                                  const Cx<R>* __restrict__ Tin,
-                                                 Cx<R>* __restrict__ Tout, const int* skip) {
+                                                 Cx<R>* __restrict__ Tout, const int* skip,
+                                                 int fs) {
   using C = Cx<R>;
-  if (skip && *skip) return;
+  const int mb = blockIdx.y;
+  if (skip && skip[(long long)mb * fs]) return;
+  Tin += mb * pc_work_elems(g);
+  Tout += mb * pc_work_elems(g);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* xs = reinterpret_cast<C*>(smem_raw);
   const int n3 = g.n3;
@@ -547,18 +567,22 @@ __global__ void k_tile_pack(int nb, int ld, const double2* __restrict__ A,
 // Second form of the streamed solve, with less issue overhead per tile: a tile
 // is consumed by one warp (lane = tile row, 32 column steps, no cross-lane
 // reduction), and up to kRoundTiles independent panel tiles of one block column
-// are consumed per barrier round, one per warp.  The two right-hand sides are
-// interleaved, so each factor value is read once from shared memory for both.
-// Tiles keep their HBM layout in shared memory (32 x 32, column-major).
+// are consumed per barrier round, one per warp.  The right-hand sides are
+// interleaved in shared memory (P columns: modes f and L-f of each member), so
+// each factor value is read once from shared memory for all of them, and from
+// HBM once for every member of a batch.  Each column's arithmetic is a fixed
+// sequence of fused multiply-adds, so its result does not depend on P or on
+// the other columns.  Tiles keep their HBM layout in shared memory (32 x 32,
+// column-major).
 constexpr int kRoundTiles = 4;  // warps per CTA = panel tiles per round
 template <typename R> struct Ring2;
 template <> struct Ring2<float> { static constexpr int value = 8; };
 template <> struct Ring2<double> { static constexpr int value = 4; };
 
 template <typename R>
-constexpr size_t lu_stream2_smem(int npad) {
+constexpr size_t lu_stream2_smem(int npad, int P) {
   return (size_t)Ring2<R>::value * kTrsvNb * kTrsvNb * sizeof(Cx<R>) +
-         (size_t)npad * 2 * sizeof(Cx<R>) + (size_t)kTrsvNb * 2 * sizeof(Cx<R>);
+         (size_t)npad * P * sizeof(Cx<R>) + (size_t)kTrsvNb * P * sizeof(Cx<R>);
 }
 
 __device__ __forceinline__ void cp_async_wait_n(int n) {
@@ -574,32 +598,71 @@ __device__ __forceinline__ void cp_async_wait_n(int n) {
   }
 }
 
-template <typename R>
+__device__ __forceinline__ float fmaR(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaR(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// acc += a * b and acc -= a * b, complex, as four fused multiply-adds each
+template <typename C>
+__device__ __forceinline__ void cmac(C& acc, C a, C b) {
+  acc.x = fmaR(a.x, b.x, acc.x);
+  acc.x = fmaR(-a.y, b.y, acc.x);
+  acc.y = fmaR(a.x, b.y, acc.y);
+  acc.y = fmaR(a.y, b.x, acc.y);
+}
+template <typename C>
+__device__ __forceinline__ void cmsub(C& acc, C a, C b) {
+  acc.x = fmaR(-a.x, b.x, acc.x);
+  acc.x = fmaR(a.y, b.y, acc.x);
+  acc.y = fmaR(-a.x, b.y, acc.y);
+  acc.y = fmaR(-a.y, b.x, acc.y);
+}
+
+// two adjacent complex values from shared memory in one access where possible
+__device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  a = make_float2(q.x, q.y);
+  b = make_float2(q.z, q.w);
+}
+__device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b) {
+  a = p[0];
+  b = p[1];
+}
+
+// One CTA per factored mode f, for km members (P/2 >= km column pairs; the
+// unused pairs are zero and not written back).  Member b's work is
+// T + b * L * n3; its skip flag is skip[b * fs]; the launch is skipped when
+// every member's flag is set.
+template <typename R, int P>
 __global__ void __launch_bounds__(32 * kRoundTiles) k_pc_lu_stream2(
     PcGeom g, int paired, const Cx<R>* __restrict__ tiles, const int* __restrict__ perm,
-    Cx<R>* T, const int* skip) {
+    Cx<R>* T, const int* skip, int fs, int km) {
   using C = Cx<R>;
   constexpr int B = kTrsvNb;
   constexpr int S = Ring2<R>::value;
   constexpr int TILE = B * B;
   constexpr int PER = 16 / (int)sizeof(C);  // values per 16-byte piece
-  if (skip && *skip) return;
+  constexpr int KS = P / 2;                 // member slots
+  static_assert(P % 2 == 0, "columns come in mode pairs");
+  if (skip) {
+    bool all = true;
+    for (int b = 0; b < km; b++) all = all && skip[(long long)b * fs] != 0;
+    if (all) return;
+  }
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* ring = reinterpret_cast<C*>(smem_raw);
   const int n = g.n3;
   const int MN = n / 3;
   const int nb = (n + B - 1) / B;
   const int npad = nb * B;
-  C* t = ring + S * TILE;  // t[2*i] first right-hand side, t[2*i+1] second
-  C* xb = t + 2 * npad;    // xb[2*j], xb[2*j+1]
+  C* t = ring + S * TILE;  // t[P*i + 2b] mode f, t[P*i + 2b + 1] mode L-f of member b
+  C* xb = t + P * npad;    // xb[P*j + col]
   const int f = blockIdx.x;
   const int i2 = g.L - f;
   const bool two = paired && f != 0 && i2 != f;
   const int total = lu_tiles(nb);
   const C* tf = tiles + (long long)f * total * TILE;
   const int* pm = perm + (long long)f * n;
-  C* T1 = T + (long long)f * n;
-  C* T2 = T + (long long)(two ? i2 : f) * n;
+  const long long wstride = pc_work_elems(g);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nthr = blockDim.x;
 
@@ -610,18 +673,22 @@ __global__ void __launch_bounds__(32 * kRoundTiles) k_pc_lu_stream2(
     cp_async_commit();
   };
 
-  for (int k = tid; k < npad; k += nthr) {
-    C v1 = czero<C>(), v2 = czero<C>();
-    if (k < n) {
-      const int p = pm[k];
-      v1 = T1[p];
-      if (two) {
-        v2 = T2[p];
-        if (p < MN) v2 = cscale(v2, (R)-1);
+  for (int b = 0; b < KS; b++) {
+    for (int k = tid; k < npad; k += nthr) {
+      C v1 = czero<C>(), v2 = czero<C>();
+      if (b < km && k < n) {
+        const C* T1 = T + b * wstride + (long long)f * n;
+        const C* T2 = T + b * wstride + (long long)(two ? i2 : f) * n;
+        const int p = pm[k];
+        v1 = T1[p];
+        if (two) {
+          v2 = T2[p];
+          if (p < MN) v2 = cscale(v2, (R)-1);
+        }
       }
+      t[P * k + 2 * b] = v1;
+      t[P * k + 2 * b + 1] = v2;
     }
-    t[2 * k] = v1;
-    t[2 * k + 1] = v2;
   }
   int issued = 0;
   while (issued < total && issued < S) issue(issued++);
@@ -644,38 +711,52 @@ __global__ void __launch_bounds__(32 * kRoundTiles) k_pc_lu_stream2(
     const int k0 = it.k * B;
     if (it.c < 0) {
       if (warp == 0) {
-        // x = inv(diag block) * t_blk, both right-hand sides
+        // x = inv(diag block) * t_blk, every column
         const C* D = ring + (ci % S) * TILE;
-        C a1 = czero<C>(), a2 = czero<C>();
-#pragma unroll 8
+        C a[P];
+#pragma unroll
+        for (int q = 0; q < P; q++) a[q] = czero<C>();
+#pragma unroll 4
         for (int c = 0; c < B; c++) {
           const C d = D[c * B + lane];
-          cfma(a1, d, t[2 * (k0 + c)]);
-          cfma(a2, d, t[2 * (k0 + c) + 1]);
+          const C* tc = t + P * (k0 + c);
+#pragma unroll
+          for (int q = 0; q < P; q += 2) {
+            C u0, u1;
+            ld_pair(tc + q, u0, u1);
+            cmac(a[q], d, u0);
+            cmac(a[q + 1], d, u1);
+          }
         }
         __syncwarp();
-        xb[2 * lane] = a1;
-        xb[2 * lane + 1] = a2;
-        t[2 * (k0 + lane)] = a1;
-        t[2 * (k0 + lane) + 1] = a2;
+#pragma unroll
+        for (int q = 0; q < P; q++) {
+          xb[P * lane + q] = a[q];
+          t[P * (k0 + lane) + q] = a[q];
+        }
       }
     } else if (warp < r) {
       // t_rows(c) -= tile * x_blk, one tile per warp
       const int ti = ci + warp;
-      const C* P = ring + (ti % S) * TILE;
+      const C* Pt = ring + (ti % S) * TILE;
       const int row = (it.c + warp) * B + lane;
-      C a1 = t[2 * row], a2 = t[2 * row + 1];
-#pragma unroll 8
+      C a[P];
+#pragma unroll
+      for (int q = 0; q < P; q += 2) ld_pair(t + P * row + q, a[q], a[q + 1]);
+#pragma unroll 4
       for (int j = 0; j < B; j++) {
-        const C v = P[j * B + lane];
-        const C x1 = xb[2 * j], x2 = xb[2 * j + 1];
-        a1.x -= v.x * x1.x - v.y * x1.y;
-        a1.y -= v.x * x1.y + v.y * x1.x;
-        a2.x -= v.x * x2.x - v.y * x2.y;
-        a2.y -= v.x * x2.y + v.y * x2.x;
+        const C v = Pt[j * B + lane];
+        const C* xj = xb + P * j;
+#pragma unroll
+        for (int q = 0; q < P; q += 2) {
+          C x0, x1;
+          ld_pair(xj + q, x0, x1);
+          cmsub(a[q], v, x0);
+          cmsub(a[q + 1], v, x1);
+        }
       }
-      t[2 * row] = a1;
-      t[2 * row + 1] = a2;
+#pragma unroll
+      for (int q = 0; q < P; q++) t[P * row + q] = a[q];
     }
     __syncthreads();
     ci += r;
@@ -683,9 +764,13 @@ __global__ void __launch_bounds__(32 * kRoundTiles) k_pc_lu_stream2(
     while (issued < total && issued < ci + S) issue(issued++);
   }
   cp_async_wait<0>();
-  for (int k = tid; k < n; k += nthr) {
-    T1[k] = t[2 * k];
-    if (two) T2[k] = (k < MN) ? cscale(t[2 * k + 1], (R)-1) : t[2 * k + 1];
+  for (int b = 0; b < km; b++) {
+    C* T1 = T + b * wstride + (long long)f * n;
+    C* T2 = T + b * wstride + (long long)(two ? i2 : f) * n;
+    for (int k = tid; k < n; k += nthr) {
+      T1[k] = t[P * k + 2 * b];
+      if (two) T2[k] = (k < MN) ? cscale(t[P * k + 2 * b + 1], (R)-1) : t[P * k + 2 * b + 1];
+    }
   }
 }
 

@@ -59,26 +59,65 @@ template <typename R> Cx<R>* pc_tw(vox_precond_s* p);
 template <> double2* pc_tw<double>(vox_precond_s* p) { return p->twd; }
 template <> float2* pc_tw<float>(vox_precond_s* p) { return p->twf; }
 
-// out = M^{-1} in (c128) or f_scale * M^{-1} in (c64 copy).  in/out length n.
+// Right-hand-side columns of the streamed solve for km members: two per
+// member slot, slots rounded up to a power of two (one instantiation each).
+static int lu_cols(int km) {
+  int ks = 1;
+  while (ks < km) ks *= 2;
+  return 2 * ks;
+}
+constexpr int kMaxLuCols = 16;  // up to 8 members in one streamed solve
+
+template <typename R, int P>
+static void launch_lu_stream(vox_precond_s* p, Cx<R>* T, cudaStream_t st, const int* skip,
+                             int fs, int km) {
+  const PcGeom& g = p->g;
+  k_pc_lu_stream2<R, P><<<p->Lf, 32 * kRoundTiles, lu_stream2_smem<R>(lu_npad(g.n3), P), st>>>(
+      g, p->paired, pc_tiles<R>(p), p->perm, T, skip, fs, km);
+}
+
+// Streamed LU solve of the x-transformed work T for km members.
+template <typename R>
+static vox_status lu_stream(vox_precond_s* p, Cx<R>* T, cudaStream_t st, const int* skip, int fs,
+                            int km) {
+  const int P = lu_cols(km);
+  if (P > kMaxLuCols || lu_stream2_smem<R>(lu_npad(p->g.n3), P) > (size_t)kSmemCap) {
+    set_error("preconditioner: too many members for one streamed solve in this precision");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  switch (P) {
+    case 2: launch_lu_stream<R, 2>(p, T, st, skip, fs, km); break;
+    case 4: launch_lu_stream<R, 4>(p, T, st, skip, fs, km); break;
+    case 8: launch_lu_stream<R, 8>(p, T, st, skip, fs, km); break;
+    default: launch_lu_stream<R, 16>(p, T, st, skip, fs, km); break;
+  }
+  return VOX_OK;
+}
+
+// out = M^{-1} in (c128) or f_scale * M^{-1} in (c64 copy), for the members
+// of mm (vectors mm.vs apart, skip flags mm.fs apart); mm.m0 selects the
+// first member's work in this handle.
 template <typename R>
 static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaStream_t st,
-                           const int* skip) {
+                           const int* skip, Members mm = Members()) {
   const PcGeom& g = p->g;
   const size_t cs = sizeof(Cx<R>);
   const int nb = (g.n3 + g.ybx - 1) / g.ybx;
-  Cx<R>* T = pc_T<R>(p, 0);
-  k_pc_xfwd<R><<<nb, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip);
+  const dim3 gx(nb, mm.km);
+  Cx<R>* T = pc_T<R>(p, 0) + mm.m0 * pc_work_elems(g);
+  k_pc_xfwd<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip,
+                                                  mm.vs, mm.fs);
   if (p->lu) {
-    k_pc_lu_stream2<R><<<p->Lf, 32 * kRoundTiles, lu_stream2_smem<R>(lu_npad(g.n3)), st>>>(
-        g, p->paired, pc_tiles<R>(p), p->perm, T, skip);
+    VOX_TRY(lu_stream<R>(p, T, st, skip, mm.fs, mm.km));
   } else {
-    Cx<R>* T2 = pc_T<R>(p, 1);
+    Cx<R>* T2 = pc_T<R>(p, 1) + mm.m0 * pc_work_elems(g);
     const int tiles = (g.n3 + 255) / 256;
-    k_pc_gemv<R><<<g.L * tiles, 256, (size_t)g.n3 * cs, st>>>(g, pc_A<R>(p), T, T2, skip);
+    k_pc_gemv<R><<<dim3(g.L * tiles, mm.km), 256, (size_t)g.n3 * cs, st>>>(g, pc_A<R>(p), T, T2,
+                                                                          skip, mm.fs);
     T = T2;
   }
-  k_pc_xinv<R><<<nb, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T, p->op->vmap,
-                                                  (R)(1.0 / g.L), out, skip);
+  k_pc_xinv<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T, p->op->vmap,
+                                                  (R)(1.0 / g.L), out, skip, mm.vs, mm.fs);
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
 }
@@ -87,9 +126,22 @@ template <typename R>
 static vox_status pc_attrs() {
   VOX_TRY(smem_cap(k_pc_xfwd<R>));
   VOX_TRY(smem_cap(k_pc_xinv<R>));
-  VOX_TRY(smem_cap(k_pc_lu_stream2<R>));
+  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 2>));
+  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 4>));
+  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 8>));
+  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 16>));
   VOX_TRY(smem_cap(k_pc_gemv<R>));
   VOX_TRY(smem_cap(k_lu_batched<R>));
+  return VOX_OK;
+}
+
+// Per-handle work: the x-transformed vectors of every member of the operator.
+static vox_status pc_alloc_work(vox_precond_s* p, int K) {
+  const long long LT = pc_work_elems(p->g) * K;
+  VOX_TRY(dalloc(&p->Td, LT));
+  VOX_TRY(dalloc(&p->Td2, LT));
+  VOX_TRY(dalloc(&p->Tf, LT));
+  VOX_TRY(dalloc(&p->Tf2, LT));
   return VOX_OK;
 }
 
@@ -181,7 +233,7 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   // the LU panel bound (n3 <= 1760) also keeps the streamed solve's
   // ring + right-hand sides (64 KiB + 32 B * n3) under the cap
   if ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
-      lu_stream2_smem<double>(lu_npad(g.n3)) > (size_t)kSmemCap) {
+      lu_stream2_smem<double>(lu_npad(g.n3), 2) > (size_t)kSmemCap) {
     set_error("preconditioner: 3*M*N too large for the batched LU panel");
     return VOX_ERR_UNSUPPORTED;
   }
@@ -192,11 +244,7 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   VOX_TRY(dalloc(&p->twf, g.L));
   VOX_CUDA(cudaMemcpy(p->twd, tw.data(), g.L * sizeof(double2), cudaMemcpyHostToDevice));
   VOX_CUDA(cudaMemcpy(p->twf, twf.data(), g.L * sizeof(float2), cudaMemcpyHostToDevice));
-  const long long LT = (long long)g.L * g.n3;
-  VOX_TRY(dalloc(&p->Td, LT));
-  VOX_TRY(dalloc(&p->Td2, LT));
-  VOX_TRY(dalloc(&p->Tf, LT));
-  VOX_TRY(dalloc(&p->Tf2, LT));
+  VOX_TRY(pc_alloc_work(p, op->K));
   VOX_TRY(pc_attrs<double>());
   VOX_TRY(pc_attrs<float>());
   return VOX_OK;
@@ -361,7 +409,7 @@ static void pc_release(vox_precond_s* p) {
   op->pcs.erase(std::remove(op->pcs.begin(), op->pcs.end(), p), op->pcs.end());
   // drop cached GMRES graphs that captured this preconditioner
   for (auto it = op->wd.graphs.begin(); it != op->wd.graphs.end();) {
-    if (it->first.first == (void*)p) {
+    if (std::get<0>(it->first) == (void*)p) {
       cudaGraphExecDestroy(it->second);
       it = op->wd.graphs.erase(it);
     } else {
@@ -369,7 +417,7 @@ static void pc_release(vox_precond_s* p) {
     }
   }
   for (auto it = op->wf.graphs.begin(); it != op->wf.graphs.end();) {
-    if (it->first.first == (void*)p) {
+    if (std::get<0>(it->first) == (void*)p) {
       cudaGraphExecDestroy(it->second);
       it = op->wf.graphs.erase(it);
     } else {
@@ -417,70 +465,97 @@ namespace vox {
 template <typename R>
 static vox_status ensure_work(vox_op_s* op, int m) {
   GmresWork<R>& w = work<R>(op);
-  if (w.m == m && w.V) return VOX_OK;
+  if (w.m == m && w.arena) return VOX_OK;
+  VOX_CUDA(cudaStreamSynchronize(op->stream));
   w.release();
   const long long n = op->g.n;
-  VOX_TRY(dalloc(&w.V, (long long)(m + 1) * n));
-  VOX_TRY(dalloc(&w.w, n));
-  VOX_TRY(dalloc(&w.t, n));
-  VOX_TRY(dalloc(&w.r, n));
-  VOX_TRY(dalloc(&w.x, n));
-  VOX_TRY(dalloc(&w.b, n));
-  VOX_TRY(dalloc(&w.st, 1));
-  VOX_CUDA(cudaMallocHost((void**)&w.hst, sizeof(GmresDev)));
-  VOX_CUDA(cudaMemset(w.st, 0, sizeof(GmresDev)));
+  const int K = op->K;
+  w.K = K;
+  w.ldv = (n + 31) / 32 * 32;
+  w.vs = (long long)(m + 6) * w.ldv;
+  VOX_TRY(dalloc(&w.arena, w.vs * K));
+  w.V = w.arena;
+  w.w = w.V + (long long)(m + 1) * w.ldv;
+  w.t = w.w + w.ldv;
+  w.r = w.t + w.ldv;
+  w.x = w.r + w.ldv;
+  w.b = w.x + w.ldv;
+  VOX_TRY(dalloc(&w.st, K));
+  VOX_CUDA(cudaMemset(w.st, 0, K * sizeof(GmresDev)));
+  VOX_CUDA(cudaMallocHost((void**)&w.hst, K * kGmresHdr));
+  VOX_CUDA(cudaMallocHost((void**)&w.hflag, K * sizeof(int)));
+  VOX_CUDA(cudaMallocHost((void**)&w.hscal, K * sizeof(double)));
   w.m = m;
   return VOX_OK;
 }
 
-// Enqueue one restart cycle (pgmres_iter.m) on stream st.
 template <typename R>
-static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, cudaStream_t st) {
+static Members wmembers(const GmresWork<R>& w, int km) {
+  Members mm;
+  mm.km = km;
+  mm.vs = w.vs;
+  mm.fs = kFlagStride;
+  return mm;
+}
+
+// Enqueue one restart cycle (pgmres_iter.m) for members 0..km-1 on stream st;
+// *nk counts the kernels.
+template <typename R>
+static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int km,
+                                cudaStream_t st, int* nk) {
   GmresWork<R>& w = work<R>(op);
   const long long n = op->g.n;
+  const long long ld = w.ldv;
   const int m = w.m;
   GmresDev* d = w.st;
   const int* skip = &d->done;
-  const int nb = nblk(n);
-  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, w.r, n, 0);
-  k_cycle_init<<<1, 32, 0, st>>>(d);
-  k_cycle_v0<R><<<nb, 256, 0, st>>>(d, w.V, w.r, n);
+  const int* frozen = &d->frozen;
+  const Members mm = wmembers(w, km);
+  const dim3 gr(kRedBlocks, km), ge(nblk(n), km), g1(1, km);
+  const bool right = side == VOX_PREC_RIGHT && pc, left = side == VOX_PREC_LEFT && pc;
+  k_norm2<R><<<gr, kRedThreads, 0, st>>>(d, w.r, n, 0, w.vs, 1);
+  k_cycle_init<<<g1, 32, 0, st>>>(d);
+  k_cycle_v0<R><<<ge, 256, 0, st>>>(d, w.V, w.r, n, w.vs);
+  *nk += 3;
   for (int k = 0; k < m; k++) {
-    Cx<R>* vk = w.V + (long long)k * n;
+    Cx<R>* vk = w.V + (long long)k * ld;
     const Cx<R>* src = vk;
-    if (side == VOX_PREC_RIGHT && pc) {
-      VOX_TRY(pc_apply<R>(pc, vk, w.t, st, skip));
+    if (right) {
+      VOX_TRY(pc_apply<R>(pc, vk, w.t, st, skip, mm));
       src = w.t;
     }
-    VOX_TRY(matvec<R>(op, MV_AN, src, w.w, st, skip));
+    VOX_TRY(matvec<R>(op, MV_AN, src, w.w, st, skip, mm));
     Cx<R>* wv = w.w;
-    if (side == VOX_PREC_LEFT && pc) {
-      VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, skip));
+    if (left) {
+      VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, skip, mm));
       wv = w.t;
     }
-    k_gs_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
-    k_gs_update_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
-    k_gs_update_norm<R><<<kRedBlocks, kRedThreads, 0, st>>>(d, k, w.V, n, wv, n);
-    k_gs_scale<R><<<nb, 256, 0, st>>>(d, k, w.V + (long long)(k + 1) * n, wv, n);
+    k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
+    k_gs_update_dots<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
+    k_gs_update_norm<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
+    k_gs_scale<R><<<ge, 256, 0, st>>>(d, k, w.V + (long long)(k + 1) * ld, wv, n, w.vs);
+    *nk += 3 + ((right || left) ? 3 : 0) + 4;
   }
-  k_cycle_ls<<<1, 32, 0, st>>>(d);
-  if (side == VOX_PREC_RIGHT && pc) {
-    k_cycle_vy<R><<<nb, 256, 0, st>>>(d, w.V, n, w.w, n);
-    VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, nullptr));
-    k_axpy<R><<<nb, 256, 0, st>>>(w.x, w.t, n);
-    k_cycle_update<R><<<nb, 256, 0, st>>>(d, w.V, n, (Cx<R>*)nullptr, w.r, n);
+  k_cycle_ls<<<g1, 32, 0, st>>>(d);
+  if (right) {
+    k_cycle_vy<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.w, n, w.vs);
+    VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, frozen, mm));
+    k_axpy<R><<<ge, 256, 0, st>>>(d, w.x, w.t, n, w.vs);
+    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, (Cx<R>*)nullptr, w.r, n, w.vs);
+    *nk += 7;
   } else {
-    k_cycle_update<R><<<nb, 256, 0, st>>>(d, w.V, n, w.x, w.r, n);
+    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs);
+    *nk += 2;
   }
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
 }
 
 template <typename R>
-static vox_status get_cycle_graph(vox_op_s* op, vox_precond_s* pc, int side,
+static vox_status get_cycle_graph(vox_op_s* op, vox_precond_s* pc, int side, int km,
                                   cudaGraphExec_t* out) {
   GmresWork<R>& w = work<R>(op);
-  auto key = std::make_pair((void*)pc, side);
+  auto key = std::make_tuple((void*)pc, side, km);
   auto it = w.graphs.find(key);
   if (it != w.graphs.end()) {
     *out = it->second;
@@ -488,8 +563,9 @@ static vox_status get_cycle_graph(vox_op_s* op, vox_precond_s* pc, int side,
   }
   cudaStream_t st = op->stream;
   cudaGraph_t graph;
+  int nk = 0;
   VOX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  vox_status s = enqueue_cycle<R>(op, pc, side, st);
+  vox_status s = enqueue_cycle<R>(op, pc, side, km, st, &nk);
   cudaError_t e = cudaStreamEndCapture(st, &graph);
   if (s != VOX_OK) return s;
   if (e != cudaSuccess) {
@@ -501,11 +577,11 @@ static vox_status get_cycle_graph(vox_op_s* op, vox_precond_s* pc, int side,
   cudaGraphExec_t exec;
   e = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
-  op->graph_nodes[exec] = (int)nnodes;
   if (e != cudaSuccess) {
     set_error(std::string("graph instantiate: ") + cudaGetErrorString(e));
     return VOX_ERR_CUDA;
   }
+  op->graph_nodes[exec] = (int)nnodes;
   w.graphs[key] = exec;
   *out = exec;
   return VOX_OK;
@@ -519,51 +595,80 @@ __global__ void k_sub(long long n, const Cx<R>* __restrict__ b, const Cx<R>* __r
     r[i] = csub(b[i], ax[i]);
 }
 
+// st[b].scal[slot] of the members with use[b] (all when use is null), one sync
 template <typename R>
-static vox_status read_scal(vox_op_s* op, int slot, double* v) {
+static vox_status read_scals(vox_op_s* op, int slot, int km, const char* use, double* v) {
   GmresWork<R>& w = work<R>(op);
-  VOX_CUDA(cudaMemcpyAsync(v, &w.st->scal[slot], sizeof(double), cudaMemcpyDeviceToHost,
-                           op->stream));
+  for (int b = 0; b < km; b++)
+    if (!use || use[b])
+      VOX_CUDA(cudaMemcpyAsync(&w.hscal[b], &w.st[b].scal[slot], sizeof(double),
+                               cudaMemcpyDeviceToHost, op->stream));
   VOX_CUDA(cudaStreamSynchronize(op->stream));
+  for (int b = 0; b < km; b++)
+    if (!use || use[b]) v[b] = w.hscal[b];
   return VOX_OK;
 }
 
-// pgmres.m:70-181 on device vectors already in w.b; solution in w.x.
-// The preconditioned-residual history (relative) is appended to resvec.
 template <typename R>
-static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, double tol, int maxit,
-                             vox_gmres_info* info, std::vector<double>* resvec) {
+static vox_status read_scal(vox_op_s* op, int slot, double* v) {
+  return read_scals<R>(op, slot, 1, nullptr, v);
+}
+
+// pgmres.m:70-181 for members 0..km-1 in lockstep, on the right-hand sides
+// already in each member's w.b; solutions in each member's w.x.  Members with
+// take[b] == 0 are left untouched.  Every member runs exactly the cycles it
+// would run alone (its own tolerance, restart count and stopping test); the
+// preconditioned-residual history (relative) is appended to resvec[b].
+template <typename R>
+static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, int km, const double* tol,
+                             int maxit, vox_gmres_info* const* info,
+                             std::vector<double>* resvec, const char* take) {
   GmresWork<R>& w = work<R>(op);
   const long long n = op->g.n;
   cudaStream_t st = op->stream;
-  const int nb = nblk(n);
   if (side != VOX_PREC_NONE && !pc) side = VOX_PREC_NONE;
+  const Members mm = wmembers(w, km);
   // x0 = 0 -> r = b ; left preconditioning: r = M^{-1} b, bnorm = ||M^{-1} b||
-  VOX_CUDA(cudaMemsetAsync(w.x, 0, n * sizeof(Cx<R>), st));
+  for (int b = 0; b < km; b++)
+    if (take[b]) VOX_CUDA(cudaMemsetAsync(w.mem(w.x, b), 0, n * sizeof(Cx<R>), st));
   if (side == VOX_PREC_LEFT) {
-    VOX_TRY(pc_apply<R>(pc, w.b, w.r, st, nullptr));
+    VOX_TRY(pc_apply<R>(pc, w.b, w.r, st, nullptr, mm));
+    op->launches += 3;
   } else {
-    VOX_CUDA(cudaMemcpyAsync(w.r, w.b, n * sizeof(Cx<R>), cudaMemcpyDeviceToDevice, st));
+    for (int b = 0; b < km; b++)
+      if (take[b])
+        VOX_CUDA(cudaMemcpyAsync(w.mem(w.r, b), w.mem(w.b, b), n * sizeof(Cx<R>),
+                                 cudaMemcpyDeviceToDevice, st));
   }
-  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.r, n, 1);
-  op->launches += (side == VOX_PREC_LEFT) ? 4 : 1;
-  double bn2;
-  VOX_TRY(read_scal<R>(op, 1, &bn2));
-  const double bnorm = std::sqrt(bn2);
-  if (bnorm == 0.0) {
-    info->flag = 0;
-    info->relres = 0.0;
-    info->iter_inner = info->iter_outer = 0;
-    if (resvec) resvec->push_back(0.0);
-    return VOX_OK;
-  }
-  // reset the header fields (everything before resvec) of the device state
+  k_norm2<R><<<dim3(kRedBlocks, km), kRedThreads, 0, st>>>(w.st, w.r, n, 1, w.vs, 0);
+  op->launches += 1;
+  std::vector<double> bn2(km, 0.0), bnorm(km, 0.0), rel(km, 1.0);
+  VOX_TRY(read_scals<R>(op, 1, km, take, bn2.data()));
+  std::vector<int> outit(km, 0), p(km, 0);
+  std::vector<char> active(km, 0);
   std::vector<unsigned char> hdr(offsetof(GmresDev, resvec), 0);
-  GmresDev* init = reinterpret_cast<GmresDev*>(hdr.data());
-  init->m = w.m;
-  init->tol_abs = tol * bnorm;
-  VOX_CUDA(cudaMemcpyAsync(w.st, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  GmresDev* h = reinterpret_cast<GmresDev*>(hdr.data());
+  for (int b = 0; b < km; b++) {
+    std::fill(hdr.begin(), hdr.end(), 0);
+    h->m = w.m;
+    if (take[b]) {
+      bnorm[b] = std::sqrt(bn2[b]);
+      if (bnorm[b] == 0.0) {
+        info[b]->flag = 0;
+        info[b]->relres = 0.0;
+        info[b]->iter_inner = info[b]->iter_outer = 0;
+        if (resvec) resvec[b].push_back(0.0);
+      } else {
+        if (resvec) resvec[b].push_back(rel[b]);
+        active[b] = rel[b] > tol[b] && maxit > 0;
+      }
+      h->tol_abs = tol[b] * bnorm[b];
+    }
+    h->frozen = active[b] ? 0 : 1;
+    // reset the header fields (everything before resvec) of the member's state
+    VOX_CUDA(cudaMemcpyAsync(&w.st[b], hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
+    VOX_CUDA(cudaStreamSynchronize(st));
+  }
   // VOX_GRAPHS=0 enqueues each cycle's kernels directly instead of replaying
   // the captured graph (same kernels and order; for profilers that cannot
   // follow stream capture)
@@ -572,36 +677,54 @@ static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, double t
     return !(e && e[0] == '0');
   }();
   cudaGraphExec_t cyc = nullptr;
-  if (use_graphs) VOX_TRY(get_cycle_graph<R>(op, pc, side, &cyc));
-  double rel = 1.0;  // ||r0|| / bnorm with x0 = 0
-  if (resvec) resvec->push_back(rel);
-  int outit = 0, p = 0;
-  while (rel > tol && outit < maxit) {
-    outit++;
+  if (use_graphs) VOX_TRY(get_cycle_graph<R>(op, pc, side, km, &cyc));
+  auto any = [&] {
+    for (int b = 0; b < km; b++)
+      if (active[b]) return true;
+    return false;
+  };
+  while (any()) {
     if (cyc) {
       VOX_CUDA(cudaGraphLaunch(cyc, st));
       op->launches += op->graph_nodes[cyc];
     } else {
-      VOX_TRY(enqueue_cycle<R>(op, pc, side, st));
+      int nk = 0;
+      VOX_TRY(enqueue_cycle<R>(op, pc, side, km, st, &nk));
+      op->launches += nk;
     }
-    VOX_CUDA(cudaMemcpyAsync(w.hst, w.st, offsetof(GmresDev, sn), cudaMemcpyDeviceToHost, st));
+    for (int b = 0; b < km; b++)
+      if (active[b])
+        VOX_CUDA(cudaMemcpyAsync(w.hdr(b), &w.st[b], offsetof(GmresDev, sn),
+                                 cudaMemcpyDeviceToHost, st));
     VOX_CUDA(cudaStreamSynchronize(st));
-    p = w.hst->k;
-    for (int i = 0; i < p; i++)
-      if (resvec) resvec->push_back(w.hst->resvec[i] / bnorm);
-    info->total_iters += p;
-    rel = (p > 0) ? w.hst->resvec[p - 1] / bnorm : rel;
-    if (w.hst->breakdown && !w.hst->converged) {
+    for (int b = 0; b < km; b++) {
+      if (!active[b]) continue;
+      const GmresDev* hb = w.hdr(b);
+      outit[b]++;
+      p[b] = hb->k;
+      for (int i = 0; i < p[b]; i++)
+        if (resvec) resvec[b].push_back(hb->resvec[i] / bnorm[b]);
+      info[b]->total_iters += p[b];
+      if (p[b] > 0) rel[b] = hb->resvec[p[b] - 1] / bnorm[b];
       // exact breakdown: the Krylov space is invariant, the LS solution is exact
-      break;
+      const bool stop = !(rel[b] > tol[b] && outit[b] < maxit) || (hb->breakdown && !hb->converged);
+      if (stop) {
+        active[b] = 0;
+        w.hflag[b] = 1;
+        VOX_CUDA(cudaMemcpyAsync(&w.st[b].frozen, &w.hflag[b], sizeof(int),
+                                 cudaMemcpyHostToDevice, st));
+      }
     }
   }
-  info->iter_inner = p;
-  info->iter_outer = outit;
+  for (int b = 0; b < km; b++) {
+    if (!take[b] || bnorm[b] == 0.0) continue;
+    info[b]->iter_inner = p[b];
+    info[b]->iter_outer = outit[b];
+  }
   return VOX_OK;
 }
 
-// relres = ||b - A x|| / ||b|| in the given precision's vectors (x, b in work)
+// relres = ||b - A x|| / ||b|| in the given precision's vectors (member 0)
 template <typename R>
 static vox_status true_relres(vox_op_s* op, double* relres) {
   GmresWork<R>& w = work<R>(op);
@@ -609,8 +732,8 @@ static vox_status true_relres(vox_op_s* op, double* relres) {
   cudaStream_t st = op->stream;
   VOX_TRY(matvec<R>(op, MV_AN, w.x, w.w, st, nullptr));
   k_sub<R><<<nblk(n), 256, 0, st>>>(n, w.b, w.w, w.t);
-  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.t, n, 2);
-  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.b, n, 3);
+  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.t, n, 2, 0, 0);
+  k_norm2<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, w.b, n, 3, 0, 0);
   op->launches += 6;
   double a, b;
   VOX_TRY(read_scal<R>(op, 2, &a));
@@ -645,7 +768,8 @@ static vox_status pgmres_entry(vox_op_s* op, vox_precond_s* pc, int side, const 
   k_cast_scale<R><<<nblk(n), 256, 0, st>>>(n, b_dev, bscale, w.b);
   std::vector<double> rv;
   info->total_iters = 0;
-  VOX_TRY(pgmres_dev<R>(op, pc, side, tol, maxit, info, &rv));
+  const char take = 1;
+  VOX_TRY(pgmres_dev<R>(op, pc, side, 1, &tol, maxit, &info, &rv, &take));
   double relres;
   VOX_TRY(true_relres<R>(op, &relres));
   info->relres = relres;
@@ -665,10 +789,13 @@ __global__ void k_axpy_d2_from(long long n, const float2* __restrict__ d, double
   }
 }
 
-// complex64 GMRES inside FP64 iterative refinement.
-static vox_status refined_entry(vox_op_s* op, vox_precond_s* pc, int side, const double2* b_dev,
-                                double tol, int restart, int maxit_inner, double inner_tol,
-                                int max_refine, double2* x_dev, vox_gmres_info* info) {
+// complex64 GMRES inside FP64 iterative refinement, for `count` right-hand
+// sides at once (members 0..count-1; b_dev and x_dev hold count vectors of n).
+// Each member's result equals what the single-member solve gives for it.
+static vox_status refined_run(vox_op_s* op, vox_precond_s* pc, int side, int count,
+                              const double2* b_dev, double tol, int restart, int maxit_inner,
+                              double inner_tol, int max_refine, double2* x_dev,
+                              vox_gmres_info* const* info) {
   if (!op->has_d || !op->has_f) {
     set_error("refined solve needs both complex128 and complex64 operator copies");
     return VOX_ERR_BAD_ARG;
@@ -677,68 +804,107 @@ static vox_status refined_entry(vox_op_s* op, vox_precond_s* pc, int side, const
     set_error("restart must be in 1.." + std::to_string(kMaxRestart));
     return VOX_ERR_BAD_ARG;
   }
+  if (count < 1 || count > op->K) {
+    set_error("right-hand sides must number 1.." + std::to_string(op->K) +
+              " (the operator's members)");
+    return VOX_ERR_BAD_ARG;
+  }
   // inner_tol <= 0: aim each inner solve at the remaining target directly
   // (0.3 * tol * ||b|| / ||r||, the factor leaving room for the gap between the
   // preconditioned residual GMRES minimises and the true residual)
   const bool auto_tol = inner_tol <= 0;
   if (max_refine < 1) max_refine = 10;
   VOX_TRY(ensure_work<float>(op, restart));
-  if (!op->wd.V) VOX_TRY(ensure_work<double>(op, 1));
+  if (!op->wd.arena) VOX_TRY(ensure_work<double>(op, 1));
   GmresWork<float>& wf = op->wf;
   GmresWork<double>& wd = op->wd;
   const long long n = op->g.n;
   cudaStream_t st = op->stream;
   const int nb = nblk(n);
   // FP64 state: x = 0, r = b
-  VOX_CUDA(cudaMemsetAsync(x_dev, 0, n * sizeof(double2), st));
-  VOX_CUDA(cudaMemcpyAsync(wd.b, b_dev, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-  VOX_CUDA(cudaMemcpyAsync(wd.r, b_dev, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-  k_norm2<double><<<kRedBlocks, kRedThreads, 0, st>>>(wd.st, wd.b, n, 3);
+  for (int b = 0; b < count; b++) {
+    VOX_CUDA(cudaMemsetAsync(x_dev + b * n, 0, n * sizeof(double2), st));
+    VOX_CUDA(cudaMemcpyAsync(wd.mem(wd.b, b), b_dev + b * n, n * sizeof(double2),
+                             cudaMemcpyDeviceToDevice, st));
+    VOX_CUDA(cudaMemcpyAsync(wd.mem(wd.r, b), b_dev + b * n, n * sizeof(double2),
+                             cudaMemcpyDeviceToDevice, st));
+  }
+  k_norm2<double><<<dim3(kRedBlocks, count), kRedThreads, 0, st>>>(wd.st, wd.b, n, 3, wd.vs, 0);
   op->launches += 1;
-  double bn2;
-  VOX_TRY(read_scal<double>(op, 3, &bn2));
-  const double bn = std::sqrt(bn2);
-  info->total_iters = 0;
-  info->refinements = 0;
-  std::vector<double> rv;
-  if (bn == 0.0) {
-    info->flag = 0;
-    info->relres = 0;
-    fill_resvec(info, rv);
-    return VOX_OK;
+  std::vector<double> bn(count), rel(count, 1.0), rn(count), itol(count), r2(count);
+  VOX_TRY(read_scals<double>(op, 3, count, nullptr, bn.data()));
+  std::vector<char> active(count, 0);
+  std::vector<std::vector<double>> rv(count);
+  std::vector<int> outer_total(count, 0), last_inner(count, 0);
+  for (int b = 0; b < count; b++) {
+    bn[b] = std::sqrt(bn[b]);
+    info[b]->total_iters = 0;
+    info[b]->refinements = 0;
+    if (bn[b] == 0.0) {
+      rel[b] = 0.0;
+    } else {
+      active[b] = rel[b] > tol;
+    }
   }
-  double rel = 1.0;
-  int outer_total = 0, last_inner = 0;
-  for (int it = 0; it < max_refine && rel > tol; it++) {
-    const double rn = rel * bn;
-    // inner right-hand side: r / ||r|| in complex64 (operator copy is A/Gram)
-    k_cast_scale<float><<<nb, 256, 0, st>>>(n, wd.r, 1.0 / rn, wf.b);
-    vox_gmres_info ii{};
-    // tolerance relative to ||r||; never ask for less than what reaches tol
-    const double itol = auto_tol ? std::min(0.5, 0.3 * tol * bn / rn)
-                                 : std::min(0.5, std::max(inner_tol, 0.5 * tol * bn / rn));
-    VOX_TRY(pgmres_dev<float>(op, pc, side, itol, maxit_inner, &ii, &rv));
-    info->total_iters += ii.total_iters;
-    outer_total += ii.iter_outer;
-    last_inner = ii.iter_inner;
-    // x += (||r|| / Gram) * d   (d solves (A/Gram) d = r/||r||)
-    k_axpy_d2_from<<<nb, 256, 0, st>>>(n, wf.x, rn / op->gram, x_dev);
-    // r = b - A x in FP64
-    VOX_TRY(matvec<double>(op, MV_AN, x_dev, wd.w, st, nullptr));
-    k_sub<double><<<nb, 256, 0, st>>>(n, wd.b, wd.w, wd.r);
-    k_norm2<double><<<kRedBlocks, kRedThreads, 0, st>>>(wd.st, wd.r, n, 2);
-    op->launches += 7;
-    double r2;
-    VOX_TRY(read_scal<double>(op, 2, &r2));
-    rel = std::sqrt(r2) / bn;
-    info->refinements = it + 1;
+  std::vector<vox_gmres_info> ii(count);
+  std::vector<vox_gmres_info*> iip(count);
+  for (int b = 0; b < count; b++) iip[b] = &ii[b];
+  for (int it = 0; it < max_refine; it++) {
+    bool anyact = false;
+    for (int b = 0; b < count; b++) anyact = anyact || active[b];
+    if (!anyact) break;
+    for (int b = 0; b < count; b++) {
+      ii[b] = vox_gmres_info{};
+      if (!active[b]) continue;
+      rn[b] = rel[b] * bn[b];
+      // inner right-hand side: r / ||r|| in complex64 (operator copy is A/Gram)
+      k_cast_scale<float><<<nb, 256, 0, st>>>(n, wd.mem(wd.r, b), 1.0 / rn[b], wf.mem(wf.b, b));
+      // tolerance relative to ||r||; never ask for less than what reaches tol
+      itol[b] = auto_tol ? std::min(0.5, 0.3 * tol * bn[b] / rn[b])
+                         : std::min(0.5, std::max(inner_tol, 0.5 * tol * bn[b] / rn[b]));
+      op->launches += 1;
+    }
+    VOX_TRY(pgmres_dev<float>(op, pc, side, count, itol.data(), maxit_inner, iip.data(),
+                              rv.data(), active.data()));
+    for (int b = 0; b < count; b++) {
+      if (!active[b]) continue;
+      info[b]->total_iters += ii[b].total_iters;
+      outer_total[b] += ii[b].iter_outer;
+      last_inner[b] = ii[b].iter_inner;
+      double2* xb = x_dev + b * n;
+      // x += (||r|| / Gram) * d   (d solves (A/Gram) d = r/||r||)
+      k_axpy_d2_from<<<nb, 256, 0, st>>>(n, wf.mem(wf.x, b), rn[b] / op->gram, xb);
+      // r = b - A x in FP64 (member b's operator)
+      Members one;
+      one.m0 = b;
+      VOX_TRY(matvec<double>(op, MV_AN, xb, wd.mem(wd.w, b), st, nullptr, one));
+      k_sub<double><<<nb, 256, 0, st>>>(n, wd.mem(wd.b, b), wd.mem(wd.w, b), wd.mem(wd.r, b));
+      k_norm2<double><<<kRedBlocks, kRedThreads, 0, st>>>(wd.st + b, wd.mem(wd.r, b), n, 2, 0, 0);
+      op->launches += 7;
+    }
+    VOX_TRY(read_scals<double>(op, 2, count, active.data(), r2.data()));
+    for (int b = 0; b < count; b++) {
+      if (!active[b]) continue;
+      rel[b] = std::sqrt(r2[b]) / bn[b];
+      info[b]->refinements = it + 1;
+      active[b] = rel[b] > tol;
+    }
   }
-  info->relres = rel;
-  info->flag = rel <= tol ? 0 : 1;
-  info->iter_inner = last_inner;
-  info->iter_outer = outer_total;
-  fill_resvec(info, rv);
+  for (int b = 0; b < count; b++) {
+    info[b]->relres = rel[b];
+    info[b]->flag = rel[b] <= tol ? 0 : 1;
+    info[b]->iter_inner = last_inner[b];
+    info[b]->iter_outer = outer_total[b];
+    fill_resvec(info[b], rv[b]);
+  }
   return VOX_OK;
+}
+
+static vox_status refined_entry(vox_op_s* op, vox_precond_s* pc, int side, const double2* b_dev,
+                                double tol, int restart, int maxit_inner, double inner_tol,
+                                int max_refine, double2* x_dev, vox_gmres_info* info) {
+  return refined_run(op, pc, side, 1, b_dev, tol, restart, maxit_inner, inner_tol, max_refine,
+                     x_dev, &info);
 }
 
 }  // namespace vox
@@ -888,10 +1054,10 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
   const long long n = op->g.n;
   cudaStream_t st = op->stream;
   const size_t cs = sizeof(Cx<R>);
-  k_fill<R><<<nblk((long long)(restart + 1) * n), 256, 0, st>>>((long long)(restart + 1) * n,
-                                                               (R)1e-3, w.V);
-  k_fill<R><<<nblk(n), 256, 0, st>>>(n, (R)1e-3, w.w);
-  k_fill<R><<<nblk(n), 256, 0, st>>>(n, (R)1e-3, w.t);
+  // every member's whole arena (basis and vectors)
+  k_fill<R><<<nblk(w.vs * op->K), 256, 0, st>>>(w.vs * op->K, (R)1e-3, w.arena);
+  const int km = op->K;
+  const long long ld = w.ldv;
   cudaEvent_t e0, e1;
   VOX_CUDA(cudaEventCreate(&e0));
   VOX_CUDA(cudaEventCreate(&e1));
@@ -906,47 +1072,53 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     return ms / reps;
   };
   for (int i = 0; i < 10; i++) out[i] = 0;
-  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3);
+  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3 * km);
   const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
   out[0] = timeit([&] {
     k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, w.V, op->vmap, b.Mc, MV_AN, b.T1,
-                                              nullptr);
+                                              nullptr, w.vs, 0);
   });
   out[1] = timeit([&] {
-    k_plane<R><<<g.Px, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, b.T1, b.fN,
-                                                 b.T2, nullptr);
+    k_plane<R><<<dim3(g.Px, km), 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, b.T1,
+                                                           b.fN, b.T2, nullptr, 0);
   });
   out[2] = timeit([&] {
     k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, w.V, b.Mr, b.Mc,
-                                              b.gram, scale, b.out_scale, MV_AN, w.w, nullptr);
+                                              b.gram, scale, b.out_scale, MV_AN, w.w, nullptr,
+                                              w.vs, 0);
   });
   if (pc) {
     const PcGeom& pg = pc->g;
     const int nb = (pg.n3 + pg.ybx - 1) / pg.ybx;
     Cx<R>* T = pc_T<R>(pc, 0);
     out[3] = timeit([&] {
-      k_pc_xfwd<R><<<nb, 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), w.V, op->vmap,
-                                                       T, nullptr);
+      k_pc_xfwd<R><<<dim3(nb, km), 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), w.V,
+                                                                 op->vmap, T, nullptr, w.vs, 0);
     });
+    vox_status ps = VOX_OK;
     out[4] = timeit([&] {
-      if (pc->lu)
-        k_pc_lu_stream2<R><<<pc->Lf, 32 * kRoundTiles, lu_stream2_smem<R>(lu_npad(pg.n3)),
-                             st>>>(pg, pc->paired, pc_tiles<R>(pc), pc->perm, T, nullptr);
-      else
-        k_pc_gemv<R><<<pg.L * ((pg.n3 + 255) / 256), 256, (size_t)pg.n3 * cs, st>>>(
-            pg, pc_A<R>(pc), T, pc_T<R>(pc, 1), nullptr);
+      if (pc->lu) {
+        ps = lu_stream<R>(pc, T, st, nullptr, 0, km);
+      } else {
+        k_pc_gemv<R><<<dim3(pg.L * ((pg.n3 + 255) / 256), km), 256, (size_t)pg.n3 * cs, st>>>(
+            pg, pc_A<R>(pc), T, pc_T<R>(pc, 1), nullptr, 0);
+      }
     });
+    if (ps != VOX_OK) return ps;
     out[5] = timeit([&] {
-      k_pc_xinv<R><<<nb, 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), T, op->vmap,
-                                                       (R)(1.0 / pg.L), w.t, nullptr);
+      k_pc_xinv<R><<<dim3(nb, km), 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), T,
+                                                                 op->vmap, (R)(1.0 / pg.L), w.t,
+                                                                 nullptr, w.vs, 0);
     });
   }
   // Gram-Schmidt at basis size kgs+1 (done flag cleared before every launch)
   const int k = std::min(kgs, restart - 1);
   const int nb = nblk(n);
+  const dim3 gr(kRedBlocks, km);
   int zero = 0;
   auto clear = [&] {
-    cudaMemcpyAsync(&w.st->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+    for (int mb = 0; mb < km; mb++)
+      cudaMemcpyAsync(&w.st[mb].done, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
   };
   {
     // state header with m and a huge tolerance so no iteration "converges"
@@ -954,19 +1126,22 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     GmresDev* init = reinterpret_cast<GmresDev*>(hdr.data());
     init->m = restart;
     init->tol_abs = -1.0;
-    VOX_CUDA(cudaMemcpyAsync(w.st, hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
+    for (int mb = 0; mb < km; mb++)
+      VOX_CUDA(cudaMemcpyAsync(&w.st[mb], hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
     VOX_CUDA(cudaStreamSynchronize(st));
   }
-  out[6] = timeit([&] { k_gs_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, k, w.V, n, w.w, n); });
+  out[6] = timeit([&] {
+    k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+  });
   out[7] = timeit([&] {
-    k_gs_update_dots<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, k, w.V, n, w.w, n);
+    k_gs_update_dots<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
   });
   // update_norm sets done at the last column; time it at k < m-1 and clear after
   double tn = 0;
   for (int r = 0; r < reps + 1; r++) {
     clear();
     VOX_CUDA(cudaEventRecord(e0, st));
-    k_gs_update_norm<R><<<kRedBlocks, kRedThreads, 0, st>>>(w.st, k, w.V, n, w.w, n);
+    k_gs_update_norm<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
     VOX_CUDA(cudaEventRecord(e1, st));
     VOX_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -976,7 +1151,8 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
   out[8] = tn / reps;
   clear();
   out[9] = timeit([&] {
-    k_gs_scale<R><<<nb, 256, 0, st>>>(w.st, k, w.V + (long long)(k + 1) * n, w.w, n);
+    k_gs_scale<R><<<dim3(nb, km), 256, 0, st>>>(w.st, k, w.V + (long long)(k + 1) * ld, w.w, n,
+                                                 w.vs);
   });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1016,11 +1192,7 @@ vox_status vox_precond_share(vox_precond_t src, vox_op_t op, vox_precond_t* out)
   p->op = op;
   p->Td = p->Td2 = nullptr;
   p->Tf = p->Tf2 = nullptr;
-  const long long LT = (long long)p->g.L * p->g.n3;
-  VOX_TRY(dalloc(&p->Td, LT));
-  VOX_TRY(dalloc(&p->Td2, LT));
-  VOX_TRY(dalloc(&p->Tf, LT));
-  VOX_TRY(dalloc(&p->Tf2, LT));
+  VOX_TRY(pc_alloc_work(p.get(), op->K));
   op->pcs.push_back(p.get());
   *out = p.release();
   return VOX_OK;
@@ -1073,8 +1245,9 @@ static long long fN_count(const OpGeom& g) {
 
 extern "C" {
 
-vox_status vox_op_interp(vox_op_t dst, const vox_op_t* srcs, const double* w, int n) {
-  if (!dst || !srcs || !w || n < 1) {
+vox_status vox_op_interp_member(vox_op_t dst, int member, const vox_op_t* srcs, const double* w,
+                                int n) {
+  if (!dst || !srcs || !w || n < 1 || member < 0 || member >= dst->K) {
     set_error("vox_op_interp: bad argument");
     return VOX_ERR_BAD_ARG;
   }
@@ -1092,14 +1265,85 @@ vox_status vox_op_interp(vox_op_t dst, const vox_op_t* srcs, const double* w, in
   cudaStream_t st = dst->stream;
   const long long cnt = fN_count<double>(dst->g);
   for (int i = 0; i < n; i++) {
+    // each source's member 0
     if (dst->has_d)
       k_lincomb_acc<double><<<nblk(cnt), 256, 0, st>>>(cnt, srcs[i]->d.fN, w[i], i == 0,
-                                                        dst->d.fN);
+                                                        dst->d.fN + member * cnt);
     if (dst->has_f)
       k_lincomb_acc<float><<<nblk(cnt), 256, 0, st>>>(cnt, srcs[i]->f.fN, w[i], i == 0,
-                                                       dst->f.fN);
+                                                       dst->f.fN + member * cnt);
   }
   VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
+vox_status vox_op_interp(vox_op_t dst, const vox_op_t* srcs, const double* w, int n) {
+  return vox_op_interp_member(dst, 0, srcs, w, n);
+}
+
+vox_status vox_op_members(vox_op_t op, int* members) {
+  if (!op || !members) {
+    set_error("vox_op_members: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *members = op->K;
+  return VOX_OK;
+}
+
+vox_status vox_solve_refined_batch_device(vox_op_t op, vox_precond_t pc, int side, int count,
+                                          const void* b, double tol, int restart,
+                                          int maxit_inner, double inner_tol, int max_refine,
+                                          void* x, vox_gmres_info* infos) {
+  if (!op || !b || !x || !infos) {
+    set_error("vox_solve_refined_batch_device: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (count < 1 || count > op->K) {
+    set_error("vox_solve_refined_batch_device: count must be 1.." + std::to_string(op->K));
+    return VOX_ERR_BAD_ARG;
+  }
+  DeviceGuard dg(op->device);
+  std::vector<vox_gmres_info*> ip(count);
+  for (int i = 0; i < count; i++) ip[i] = &infos[i];
+  auto t0 = std::chrono::steady_clock::now();
+  VOX_TRY(refined_run(op, pc, side, count, (const double2*)b, tol, restart, maxit_inner,
+                      inner_tol, max_refine, (double2*)x, ip.data()));
+  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  for (int i = 0; i < count; i++) infos[i].seconds = sec;
+  return VOX_OK;
+}
+
+vox_status vox_solve_refined_batch(vox_op_t op, vox_precond_t pc, int side, int count,
+                                   const double* b_re, const double* b_im, double tol,
+                                   int restart, int maxit_inner, double inner_tol,
+                                   int max_refine, double* x_re, double* x_im,
+                                   vox_gmres_info* infos) {
+  if (!op || !b_re || !x_re || !infos) {
+    set_error("vox_solve_refined_batch: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (count < 1 || count > op->K) {
+    set_error("vox_solve_refined_batch: count must be 1.." + std::to_string(op->K));
+    return VOX_ERR_BAD_ARG;
+  }
+  DeviceGuard dg(op->device);
+  const long long n = op->g.n;
+  cudaStream_t st = op->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  split_to_d2(b_re, b_im, count * n, op->h_in);
+  VOX_CUDA(cudaMemcpyAsync(op->d_in, op->h_in, count * n * sizeof(double2),
+                           cudaMemcpyHostToDevice, st));
+  std::vector<vox_gmres_info*> ip(count);
+  for (int i = 0; i < count; i++) ip[i] = &infos[i];
+  VOX_TRY(refined_run(op, pc, side, count, op->d_in, tol, restart, maxit_inner, inner_tol,
+                      max_refine, op->d_out, ip.data()));
+  VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, count * n * sizeof(double2),
+                           cudaMemcpyDeviceToHost, st));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  d2_to_split(op->h_out, count * n, x_re, x_im);
+  const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  for (int i = 0; i < count; i++) infos[i].seconds = sec;
   return VOX_OK;
 }
 
