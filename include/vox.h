@@ -183,10 +183,10 @@ void vox_precond_destroy(vox_precond_t p);
  * apply one preconditioner concurrently.  The factors live until the last
  * handle sharing them is destroyed.  No reference counterpart. */
 vox_status vox_precond_share(vox_precond_t src, vox_op_t op, vox_precond_t* out);
-/* Factored modes (L, or L/2+1 when modes L-i reuse the factors of mode i),
- * the factor leading dimension, and whether the blocks are LU factors (1) or
- * caller-supplied explicit inverses (0). */
-vox_status vox_precond_info(vox_precond_t p, int* n_factored, int* ld, int* is_lu);
+/* Stored inverse blocks (L, or L/2+1 when mode L-i is applied with the block
+ * of mode i), their leading dimension (3MN rounded up to 32), and whether
+ * modes are paired that way (1) or every mode has its own block (0). */
+vox_status vox_precond_info(vox_precond_t p, int* n_blocks, int* ld, int* paired);
 /* mvp = chan_mvp_idx(inv_blocks, JIn, L, M, N, idx), host buffers of length n_idx. */
 vox_status vox_precond_apply(vox_precond_t p, vox_prec prec, const double* in_re,
                              const double* in_im, double* out_re, double* out_im);

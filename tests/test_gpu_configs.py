@@ -1,0 +1,103 @@
+"""Full-size GPU checks on the benchmark gratings.
+
+* Bragg grating, 60 periods at 20 nm (1160 x 30 x 11): matvec against the
+  oracle in both precisions; GMRES(50) with the level-1 preconditioner against
+  none (iteration counts, and the two solutions agree to the tolerance).
+* Bragg grating at 10 nm (2320 x 60 x 22, padded FFT grid 4640-class):
+  complex64 matvec against the oracle on seeded inputs (and 100 seeded inputs
+  against the complex128 matvec, itself pinned to the oracle), and the
+  complex64 + FP64-refinement solve against the plain complex128 solve at 1e-5
+  and 1e-8 (no preconditioner: its 3MN = 3960 blocks exceed the level-1 build).
+Sizes are the benchmark's own; the oracle is timed in seconds per product.
+"""
+import numpy as np
+import pytest
+
+import voxphoton_b200 as vb
+from oracle import vie as ov
+from voxphoton_b200 import geometry as geo
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand(n, rng):
+    return rng.standard_normal(n) + 1j * rng.standard_normal(n)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def bragg20():
+    p = geo.bragg_config("bragg20")
+    G = vb.assemble_toeplitz(p.shape, p.ko, p.res)
+    idx = p.idxS3()
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=G)
+    yield p, G, idx, op
+    op.close()
+
+
+def test_bragg20_matvec_matches_oracle(bragg20):
+    p, G, idx, op = bragg20
+    fN = ov.fN_from_toeplitz(G)
+    rng = np.random.default_rng(0)
+    for _ in range(2):
+        x = _rand(idx.size, rng)
+        ref = ov.mv_AN_const(x, fN, np.ones(p.shape), p.Mop(), p.Gram, "notransp", idx)
+        assert _rel(op.mv_AN(x, prec="c128"), ref) < 1e-12
+        assert _rel(op.mv_AN(x, prec="c64"), ref) < 1e-5
+
+
+def test_bragg20_level1_against_no_preconditioner(bragg20):
+    p, G, idx, op = bragg20
+    b = vb.jvie_rhs(p.e_r, geo.plane_wave(p), p.Gram, p.freq, idx)
+    pc = vb.Preconditioner.level1(op, G, p.e_r)
+    x1, f1, r1, it1, _ = vb.pgmres(op, b, restart=50, tol=1e-5, maxit=40, R1=pc, prec="c128")
+    x0, f0, r0, it0, _ = vb.pgmres(op, b, restart=50, tol=1e-5, maxit=200, prec="c128")
+    assert f1 == 0 and f0 == 0 and r1 <= 1e-5 and r0 <= 1e-5
+    n1 = (it1[1] - 1) * 50 + it1[0]
+    n0 = (it0[1] - 1) * 50 + it0[0]
+    assert n1 < n0 / 3  # the circulant preconditioner cuts the iterations
+    # both solve the same system to 1e-5: the solutions agree to that order
+    # (scaled by the conditioning, bounded here by 1e-3)
+    assert _rel(x1, x0) < 1e-3
+    pc.close()
+
+
+@pytest.fixture(scope="module")
+def bragg10():
+    p = geo.bragg_config("bragg10")
+    G = vb.assemble_toeplitz(p.shape, p.ko, p.res)
+    idx = p.idxS3()
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=G)
+    yield p, G, idx, op
+    op.close()
+
+
+def test_bragg10_matvec_c64_against_oracle_and_100_inputs(bragg10):
+    p, G, idx, op = bragg10
+    rng = np.random.default_rng(0)
+    xs = [_rand(idx.size, rng) for _ in range(100)]
+    fN = ov.fN_from_toeplitz(G)
+    ref = ov.mv_AN_const(xs[0], fN, np.ones(p.shape), p.Mop(), p.Gram, "notransp", idx)
+    del fN
+    assert _rel(op.mv_AN(xs[0], prec="c128"), ref) < 1e-12
+    assert _rel(op.mv_AN(xs[0], prec="c64"), ref) < 1e-5
+    worst = max(_rel(op.mv_AN(x, prec="c64"), op.mv_AN(x, prec="c128")) for x in xs)
+    assert worst < 1e-5
+
+
+@pytest.mark.parametrize("tol", [1e-5, 1e-8])
+def test_bragg10_refined_solve_against_plain_fp64(bragg10, tol):
+    p, G, idx, op = bragg10
+    b = vb.jvie_rhs(p.e_r, geo.plane_wave(p), p.Gram, p.freq, idx)
+    x, info = vb.solve_refined(op, b, tol=tol, restart=50, maxit_inner=60, inner_tol=0.0,
+                               max_refine=20)
+    assert info["flag"] == 0 and info["relres"] <= tol
+    # the true residual in FP64
+    assert _rel(op.mv_AN(x, prec="c128"), b) <= tol * 1.0001
+    x64, flag, relres, it, _ = vb.pgmres(op, b, restart=50, tol=tol, maxit=200, prec="c128")
+    assert flag == 0 and relres <= tol
+    # two solutions with residuals below tol: agreement up to the conditioning
+    assert _rel(x, x64) < max(1e-3, 1e4 * tol)

@@ -1,6 +1,7 @@
 """GPU tests of the sweep serving pieces: operator interpolation in wavelength
 (vox_op_interp), shared preconditioner handles (vox_precond_share), and that
-every request's result is the same alone and in the concurrent mix."""
+every request's result is the same alone and in the concurrent mix (lanes of
+two-member batches, so requests are solved together in lockstep)."""
 import numpy as np
 import pytest
 
@@ -59,7 +60,7 @@ def test_shared_preconditioner_matches_its_source():
 
 def test_results_are_the_same_alone_and_in_the_mix():
     band = (1500e-9, 1600e-9)
-    fams = [sv.Family(k, small(k), band, nG=3) for k in (2, 4)]
+    fams = [sv.Family(k, small(k), band, nG=3, members=2) for k in (2, 4)]
     for f in fams:
         f.add_slot()
         f.add_slot()
@@ -81,6 +82,6 @@ def test_results_are_the_same_alone_and_in_the_mix():
         a = alone[m.rid]
         assert m.flag == 0 and a.flag == 0 and m.relres <= 1e-5
         assert m.iters == a.iters
-        assert np.linalg.norm(m.x - a.x) / np.linalg.norm(a.x) < 1e-12
+        assert np.array_equal(m.x, a.x)
     for f in fams:
         f.close()

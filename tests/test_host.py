@@ -90,3 +90,15 @@ def test_operator_fails_loudly_without_gpu():
         pass
     with pytest.raises(_lib.VoxError):
         vb.Operator(np.ones((4, 4, 4)), 1.0, [1, 2, 3], G=np.zeros((4, 4, 4, 6)))
+
+
+def test_transmitted_power_slice_follows_the_reference_example():
+    # example_Bragg_1500nm_to_1600nm.m:107-113: x = L - round((len_abs+450nm)/res),
+    # all of y (round(delW/2) of a length in metres is 0), all z, all components
+    import voxphoton_b200 as vb
+    rng = np.random.default_rng(0)
+    E = rng.standard_normal((40, 6, 3, 3)) + 1j * rng.standard_normal((40, 6, 3, 3))
+    P = vb.transmitted_power(E, 20e-9, 0.3e-6, 50e-9)
+    x = 40 - int(round((0.3e-6 + 450e-9) / 20e-9))
+    assert x == 2
+    assert np.isclose(P, np.sum(np.abs(E[x - 1]) ** 2), rtol=1e-14)

@@ -112,38 +112,6 @@ __global__ void __launch_bounds__(256) k_pc_xinv(PcGeom g, FftPlan pl, const Cx<
   }
 }
 
-// --------------------------------------------------------- apply: block GEMV
-// T_i <- B_i T_i with B_i column-major n3 x n3 (explicit inverse blocks).
-template <typename R>
-__global__ void __launch_bounds__(256) k_pc_gemv(PcGeom g, const Cx<R>* __restrict__ B,
-                                                 const Cx<R>* __restrict__ Tin,
-                                                 Cx<R>* __restrict__ Tout, const int* skip,
-                                                 int fs) {
-  using C = Cx<R>;
-  const int mb = blockIdx.y;
-  if (skip && skip[(long long)mb * fs]) return;
-  Tin += mb * pc_work_elems(g);
-  Tout += mb * pc_work_elems(g);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* xs = reinterpret_cast<C*>(smem_raw);
-  const int n3 = g.n3;
-  const int tilesR = (n3 + blockDim.x - 1) / blockDim.x;
-  const int i = blockIdx.x / tilesR;
-  const int r = (blockIdx.x % tilesR) * blockDim.x + threadIdx.x;
-  for (int c = threadIdx.x; c < n3; c += blockDim.x) xs[c] = Tin[(long long)i * n3 + c];
-  __syncthreads();
-  if (r >= n3) return;
-  const C* Bi = B + (long long)i * n3 * n3;
-  C acc0 = czero<C>(), acc1 = czero<C>();
-  int c = 0;
-  for (; c + 1 < n3; c += 2) {
-    cfma(acc0, Bi[(long long)c * n3 + r], xs[c]);
-    cfma(acc1, Bi[(long long)(c + 1) * n3 + r], xs[c + 1]);
-  }
-  if (c < n3) cfma(acc0, Bi[(long long)c * n3 + r], xs[c]);
-  Tout[(long long)i * n3 + r] = cadd(acc0, acc1);
-}
-
 // ------------------------------------------------------------------- build
 // Chan circulant along x of each component: src/dst [comp][z][y][x] (x fastest).
 __global__ void k_chan(int L, long long V, const double2* __restrict__ G, double2* out) {
@@ -564,16 +532,13 @@ __global__ void k_tile_pack(int nb, int ld, const double2* __restrict__ A,
   }
 }
 
-// Second form of the streamed solve, with less issue overhead per tile: a tile
-// is consumed by one warp (lane = tile row, 32 column steps, no cross-lane
-// reduction), and up to kRoundTiles independent panel tiles of one block column
-// are consumed per barrier round, one per warp.  The right-hand sides are
-// interleaved in shared memory (P columns: modes f and L-f of each member), so
-// each factor value is read once from shared memory for all of them, and from
-// HBM once for every member of a batch.  Each column's arithmetic is a fixed
-// sequence of fused multiply-adds, so its result does not depend on P or on
-// the other columns.  Tiles keep their HBM layout in shared memory (32 x 32,
-// column-major).
+// The streamed triangular solve, used once per preconditioner to form the
+// explicit inverse blocks: a tile is consumed by one warp (lane = tile row,
+// 32 column steps, no cross-lane reduction), and up to kRoundTiles
+// independent panel tiles of one block column are consumed per barrier round,
+// one per warp.  The P right-hand sides are interleaved in shared memory, so
+// each factor value is read once from shared memory for all of them.  Tiles
+// keep their HBM layout in shared memory (32 x 32, column-major).
 constexpr int kRoundTiles = 4;  // warps per CTA = panel tiles per round
 template <typename R> struct Ring2;
 template <> struct Ring2<float> { static constexpr int value = 8; };
@@ -617,7 +582,7 @@ __device__ __forceinline__ void cmsub(C& acc, C a, C b) {
   acc.y = fmaR(-a.y, b.x, acc.y);
 }
 
-// two adjacent complex values from shared memory in one access where possible
+// two adjacent complex values in one access where possible (16-byte aligned)
 __device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
   const float4 q = *reinterpret_cast<const float4*>(p);
   a = make_float2(q.x, q.y);
@@ -628,72 +593,28 @@ __device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b
   b = p[1];
 }
 
-// One CTA per factored mode f, for km members (P/2 >= km column pairs; the
-// unused pairs are zero and not written back).  Member b's work is
-// T + b * L * n3; its skip flag is skip[b * fs]; the launch is skipped when
-// every member's flag is set.
+// t (npad x P, interleaved) <- U^{-1} L^{-1} t for the mode whose tile stream
+// starts at tf (tiles in consumption order).  ring / xb: shared-memory work.
 template <typename R, int P>
-__global__ void __launch_bounds__(32 * kRoundTiles) k_pc_lu_stream2(
-    PcGeom g, int paired, const Cx<R>* __restrict__ tiles, const int* __restrict__ perm,
-    Cx<R>* T, const int* skip, int fs, int km) {
+__device__ void lu_stream_core(const Cx<R>* __restrict__ tf, int nb, Cx<R>* ring, Cx<R>* t,
+                               Cx<R>* xb) {
   using C = Cx<R>;
   constexpr int B = kTrsvNb;
   constexpr int S = Ring2<R>::value;
   constexpr int TILE = B * B;
   constexpr int PER = 16 / (int)sizeof(C);  // values per 16-byte piece
-  constexpr int KS = P / 2;                 // member slots
-  static_assert(P % 2 == 0, "columns come in mode pairs");
-  if (skip) {
-    bool all = true;
-    for (int b = 0; b < km; b++) all = all && skip[(long long)b * fs] != 0;
-    if (all) return;
-  }
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* ring = reinterpret_cast<C*>(smem_raw);
-  const int n = g.n3;
-  const int MN = n / 3;
-  const int nb = (n + B - 1) / B;
-  const int npad = nb * B;
-  C* t = ring + S * TILE;  // t[P*i + 2b] mode f, t[P*i + 2b + 1] mode L-f of member b
-  C* xb = t + P * npad;    // xb[P*j + col]
-  const int f = blockIdx.x;
-  const int i2 = g.L - f;
-  const bool two = paired && f != 0 && i2 != f;
   const int total = lu_tiles(nb);
-  const C* tf = tiles + (long long)f * total * TILE;
-  const int* pm = perm + (long long)f * n;
-  const long long wstride = pc_work_elems(g);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nthr = blockDim.x;
-
   auto issue = [&](int i) {
     const C* src = tf + (long long)i * TILE;
     C* dst = ring + (i % S) * TILE;
     for (int p = tid; p < TILE / PER; p += nthr) cp_async16(dst + p * PER, src + p * PER);
     cp_async_commit();
   };
-
-  for (int b = 0; b < KS; b++) {
-    for (int k = tid; k < npad; k += nthr) {
-      C v1 = czero<C>(), v2 = czero<C>();
-      if (b < km && k < n) {
-        const C* T1 = T + b * wstride + (long long)f * n;
-        const C* T2 = T + b * wstride + (long long)(two ? i2 : f) * n;
-        const int p = pm[k];
-        v1 = T1[p];
-        if (two) {
-          v2 = T2[p];
-          if (p < MN) v2 = cscale(v2, (R)-1);
-        }
-      }
-      t[P * k + 2 * b] = v1;
-      t[P * k + 2 * b + 1] = v2;
-    }
-  }
   int issued = 0;
   while (issued < total && issued < S) issue(issued++);
   __syncthreads();
-
   // at most half the ring is consumed per round, so the other half streams in
   constexpr int RMAX = (S / 2 < kRoundTiles) ? S / 2 : kRoundTiles;
   int ci = 0;
@@ -764,12 +685,150 @@ __global__ void __launch_bounds__(32 * kRoundTiles) k_pc_lu_stream2(
     while (issued < total && issued < ci + S) issue(issued++);
   }
   cp_async_wait<0>();
-  for (int b = 0; b < km; b++) {
-    C* T1 = T + b * wstride + (long long)f * n;
-    C* T2 = T + b * wstride + (long long)(two ? i2 : f) * n;
-    for (int k = tid; k < n; k += nthr) {
-      T1[k] = t[P * k + 2 * b];
-      if (two) T2[k] = (k < MN) ? cscale(t[P * k + 2 * b + 1], (R)-1) : t[P * k + 2 * b + 1];
+  __syncthreads();
+}
+
+// Columns c0 .. c0+P-1 of inv(B_f) = U^{-1} L^{-1} P for every factored mode
+// f (grid (ceil(n3 / P), Lf)): the right-hand sides are the permuted unit
+// vectors, (P e_j)[k] = [perm[k] == j].  Output column-major, leading
+// dimension ld, one ld x ld block per mode (rows >= n3 left untouched).
+constexpr int kInvBuildCols = 8;  // inverse columns per CTA in the build
+
+template <int P>
+__global__ void __launch_bounds__(32 * kRoundTiles) k_lu_inv_cols(
+    PcGeom g, const double2* __restrict__ tiles, const int* __restrict__ perm, int ld,
+    double2* __restrict__ Binv) {
+  using C = double2;
+  constexpr int B = kTrsvNb;
+  constexpr int S = Ring2<double>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* ring = reinterpret_cast<C*>(smem_raw);
+  const int n = g.n3;
+  const int nb = (n + B - 1) / B;
+  const int npad = nb * B;
+  C* t = ring + S * B * B;
+  C* xb = t + P * npad;
+  const int c0 = blockIdx.x * P;
+  const int f = blockIdx.y;
+  const int* pm = perm + (long long)f * n;
+  for (int k = threadIdx.x; k < npad; k += blockDim.x) {
+    const int p = (k < n) ? pm[k] : -1;
+#pragma unroll
+    for (int q = 0; q < P; q++) t[P * k + q] = make_double2(p == c0 + q ? 1.0 : 0.0, 0.0);
+  }
+  lu_stream_core<double, P>(tiles + (long long)f * lu_tiles(nb) * B * B, nb, ring, t, xb);
+  double2* out = Binv + (long long)f * ld * ld;
+  for (int q = 0; q < P; q++) {
+    if (c0 + q >= n) break;
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+      out[(long long)(c0 + q) * ld + k] = t[P * k + q];
+  }
+}
+
+// ------------------------------------------- apply: per-mode inverse blocks
+// T2_f = inv(B_f) T_f for every mode, with P right-hand-side columns per mode:
+// for each of km members, mode f and (paired) mode L-f through
+// inv(B_{L-f}) = D inv(B_f) D, so every block is read from HBM once for all
+// members and both modes.  Blocks are column-major with leading dimension ld
+// (a multiple of 32, zero padded); block f of Binv serves mode f (and L-f).
+// One CTA per (128-row chunk, block): 64 row pairs x 4 column groups; the
+// group g sums columns k = g, g+4, ... and the four partial sums are added in
+// that fixed order, so each column's result does not depend on P or on the
+// other members.  grid (ld / 128 rounded up, nblocks); shared memory
+// max(n3, 512) * P complex values.
+constexpr int kInvRows = 128;
+constexpr int kInvKG = 4;
+constexpr int kInvThreads = (kInvRows / 2) * kInvKG;
+
+template <typename R>
+constexpr size_t inv_apply_smem(int n3, int P) {
+  return (size_t)(n3 > kInvKG * kInvRows ? n3 : kInvKG * kInvRows) * P * sizeof(Cx<R>);
+}
+
+template <typename R, int P>
+__global__ void __launch_bounds__(kInvThreads) k_pc_inv_apply(
+    PcGeom g, int paired, int ld, const Cx<R>* __restrict__ Binv, const Cx<R>* __restrict__ Tin,
+    Cx<R>* __restrict__ Tout, const int* skip, int fs, int km) {
+  using C = Cx<R>;
+  constexpr int KS = P / 2;
+  static_assert(P % 2 == 0, "columns come in mode pairs");
+  if (skip) {
+    bool all = true;
+    for (int b = 0; b < km; b++) all = all && skip[(long long)b * fs] != 0;
+    if (all) return;
+  }
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* X = reinterpret_cast<C*>(smem_raw);  // X[k * P + col]; later the partial sums
+  const int n = g.n3;
+  const int MN = n / 3;
+  const int f = blockIdx.y;
+  const int i2 = g.L - f;
+  const bool two = paired && f != 0 && i2 != f;
+  const long long wstride = pc_work_elems(g);
+  const int tid = threadIdx.x;
+  for (int b = 0; b < KS; b++) {
+    const C* T1 = Tin + b * wstride + (long long)f * n;
+    const C* T2 = Tin + b * wstride + (long long)(two ? i2 : f) * n;
+    for (int k = tid; k < n; k += blockDim.x) {
+      C v1 = czero<C>(), v2 = czero<C>();
+      if (b < km) {
+        v1 = T1[k];
+        if (two) {
+          v2 = T2[k];
+          if (k < MN) v2 = cscale(v2, (R)-1);
+        }
+      }
+      X[P * k + 2 * b] = v1;
+      X[P * k + 2 * b + 1] = v2;
+    }
+  }
+  __syncthreads();
+  const int rp = tid % (kInvRows / 2);  // row pair within the chunk
+  const int kg = tid / (kInvRows / 2);  // column group
+  const int r = blockIdx.x * kInvRows + 2 * rp;
+  C a0[P], a1[P];
+#pragma unroll
+  for (int q = 0; q < P; q++) a0[q] = a1[q] = czero<C>();
+  if (r < ld) {
+    const C* Bf = Binv + (long long)f * ld * ld + r;
+#pragma unroll 4
+    for (int k = kg; k < n; k += kInvKG) {
+      C b0, b1;
+      ld_pair(Bf + (long long)k * ld, b0, b1);
+      const C* xk = X + P * k;
+#pragma unroll
+      for (int q = 0; q < P; q += 2) {
+        C x0, x1;
+        ld_pair(xk + q, x0, x1);
+        cmac(a0[q], b0, x0);
+        cmac(a0[q + 1], b0, x1);
+        cmac(a1[q], b1, x0);
+        cmac(a1[q + 1], b1, x1);
+      }
+    }
+  }
+  __syncthreads();
+  // partial sums: red[(kg * kInvRows + row) * P + col]
+  C* red = X;
+#pragma unroll
+  for (int q = 0; q < P; q++) {
+    red[(kg * kInvRows + 2 * rp) * P + q] = a0[q];
+    red[(kg * kInvRows + 2 * rp + 1) * P + q] = a1[q];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < kInvRows * P; idx += blockDim.x) {
+    const int q = idx / kInvRows;
+    const int rl = idx - q * kInvRows;
+    const int row = blockIdx.x * kInvRows + rl;
+    const int b = q >> 1;
+    if (row >= n || b >= km) continue;
+    C s = red[rl * P + q];
+#pragma unroll
+    for (int gg = 1; gg < kInvKG; gg++) s = cadd(s, red[(gg * kInvRows + rl) * P + q]);
+    if ((q & 1) == 0) {
+      Tout[b * wstride + (long long)f * n + row] = s;
+    } else if (two) {
+      Tout[b * wstride + (long long)i2 * n + row] = (row < MN) ? cscale(s, (R)-1) : s;
     }
   }
 }

@@ -10,13 +10,13 @@ struct vox_precond_s {
   vox_op_s* op = nullptr;
   PcGeom g{};
   FftPlan pl{};
-  bool lu = true;              // LU factors (true) or explicit inverse blocks (false)
-  double2* Ad = nullptr;       // c128 blocks / factors, L * n3 * n3
-  float2* Af = nullptr;        // c64 copy (blocks scaled for the A/Gram operator)
+  double2* Ad = nullptr;       // c128 inverse blocks, Lf blocks of ld x ld (column-major)
+  float2* Af = nullptr;        // c64 copy (Gram * inverse, for the A/Gram operator)
+  int ld = 0;                  // leading dimension of the blocks (3MN rounded up to 32)
   int* piv = nullptr;          // Lf * n3 getrf pivots
   int* perm = nullptr;         // Lf * n3 row permutation of the pivots
-  int Lf = 0;                  // factored modes (L, or L/2+1 with pairing)
-  int paired = 0;              // mode L-f solved with the factors of mode f
+  int Lf = 0;                  // stored blocks (L, or L/2+1 with pairing)
+  int paired = 0;              // mode L-f applied with the block of mode f
   double2* Dld = nullptr;      // inverted diagonal blocks of L and U (c128)
   double2* Dud = nullptr;
   float2* Dlf = nullptr;       // ... and of the c64 copy
@@ -30,6 +30,7 @@ struct vox_precond_s {
   float2* Tf = nullptr;
   float2* Tf2 = nullptr;
   double f_scale = 1.0;        // the c64 copy applies f_scale * M^{-1}
+  int K = 0;                   // members whose work the T* buffers hold
   // Owner of the factor arrays above (Ad/Af/piv/perm/D*/tiles/tw): set once
   // construction succeeds; views made by vox_precond_share hold a copy, and the
   // arrays are freed with the last holder.  Work buffers T* are per handle.
@@ -46,9 +47,6 @@ template <> float2* pc_A<float>(vox_precond_s* p) { return p->Af; }
 template <typename R> Cx<R>* pc_T(vox_precond_s* p, int which);
 template <> double2* pc_T<double>(vox_precond_s* p, int w) { return w ? p->Td2 : p->Td; }
 template <> float2* pc_T<float>(vox_precond_s* p, int w) { return w ? p->Tf2 : p->Tf; }
-template <typename R> Cx<R>* pc_tiles(vox_precond_s* p);
-template <> double2* pc_tiles<double>(vox_precond_s* p) { return p->tiles_d; }
-template <> float2* pc_tiles<float>(vox_precond_s* p) { return p->tiles_f; }
 template <typename R> Cx<R>* pc_Dl(vox_precond_s* p);
 template <> double2* pc_Dl<double>(vox_precond_s* p) { return p->Dld; }
 template <> float2* pc_Dl<float>(vox_precond_s* p) { return p->Dlf; }
@@ -59,37 +57,48 @@ template <typename R> Cx<R>* pc_tw(vox_precond_s* p);
 template <> double2* pc_tw<double>(vox_precond_s* p) { return p->twd; }
 template <> float2* pc_tw<float>(vox_precond_s* p) { return p->twf; }
 
-// Right-hand-side columns of the streamed solve for km members: two per
+// Right-hand-side columns of one inverse-block apply for km members: two per
 // member slot, slots rounded up to a power of two (one instantiation each).
 static int lu_cols(int km) {
   int ks = 1;
   while (ks < km) ks *= 2;
   return 2 * ks;
 }
-constexpr int kMaxLuCols = 16;  // up to 8 members in one streamed solve
+// Members per launch: at 8 columns a block is still streamed at close to the
+// HBM rate (the FMAs per byte fit the SM), and shared memory allows three
+// CTAs per SM; more members are applied in groups of this size.
+constexpr int kApplyMembers = 4;
 
 template <typename R, int P>
-static void launch_lu_stream(vox_precond_s* p, Cx<R>* T, cudaStream_t st, const int* skip,
-                             int fs, int km) {
+static void launch_inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStream_t st,
+                             const int* skip, int fs, int km) {
   const PcGeom& g = p->g;
-  k_pc_lu_stream2<R, P><<<p->Lf, 32 * kRoundTiles, lu_stream2_smem<R>(lu_npad(g.n3), P), st>>>(
-      g, p->paired, pc_tiles<R>(p), p->perm, T, skip, fs, km);
+  const dim3 grid((p->ld + kInvRows - 1) / kInvRows, p->Lf);
+  k_pc_inv_apply<R, P><<<grid, kInvThreads, inv_apply_smem<R>(g.n3, P), st>>>(
+      g, p->paired, p->ld, pc_A<R>(p), T, T2, skip, fs, km);
 }
 
-// Streamed LU solve of the x-transformed work T for km members.
+// T2 = per-mode inverse blocks applied to T, for km members (in groups of
+// kApplyMembers, each group one launch).
 template <typename R>
-static vox_status lu_stream(vox_precond_s* p, Cx<R>* T, cudaStream_t st, const int* skip, int fs,
-                            int km) {
-  const int P = lu_cols(km);
-  if (P > kMaxLuCols || lu_stream2_smem<R>(lu_npad(p->g.n3), P) > (size_t)kSmemCap) {
-    set_error("preconditioner: too many members for one streamed solve in this precision");
-    return VOX_ERR_UNSUPPORTED;
-  }
-  switch (P) {
-    case 2: launch_lu_stream<R, 2>(p, T, st, skip, fs, km); break;
-    case 4: launch_lu_stream<R, 4>(p, T, st, skip, fs, km); break;
-    case 8: launch_lu_stream<R, 8>(p, T, st, skip, fs, km); break;
-    default: launch_lu_stream<R, 16>(p, T, st, skip, fs, km); break;
+static vox_status inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStream_t st,
+                            const int* skip, int fs, int km) {
+  const long long ws = pc_work_elems(p->g);
+  for (int m0 = 0; m0 < km; m0 += kApplyMembers) {
+    const int kg = std::min(kApplyMembers, km - m0);
+    const int P = lu_cols(kg);
+    if (inv_apply_smem<R>(p->g.n3, P) > (size_t)kSmemCap) {
+      set_error("preconditioner: too many members for one apply in this precision");
+      return VOX_ERR_UNSUPPORTED;
+    }
+    const Cx<R>* Tg = T + m0 * ws;
+    Cx<R>* T2g = T2 + m0 * ws;
+    const int* sg = skip ? skip + (long long)m0 * fs : nullptr;
+    switch (P) {
+      case 2: launch_inv_apply<R, 2>(p, Tg, T2g, st, sg, fs, kg); break;
+      case 4: launch_inv_apply<R, 4>(p, Tg, T2g, st, sg, fs, kg); break;
+      default: launch_inv_apply<R, 8>(p, Tg, T2g, st, sg, fs, kg); break;
+    }
   }
   return VOX_OK;
 }
@@ -100,23 +109,21 @@ static vox_status lu_stream(vox_precond_s* p, Cx<R>* T, cudaStream_t st, const i
 template <typename R>
 static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaStream_t st,
                            const int* skip, Members mm = Members()) {
+  if (mm.m0 + mm.km > p->K) {
+    set_error("preconditioner: this handle holds work for " + std::to_string(p->K) +
+              " member(s); share it with the batched operator (vox_precond_share)");
+    return VOX_ERR_BAD_ARG;
+  }
   const PcGeom& g = p->g;
   const size_t cs = sizeof(Cx<R>);
   const int nb = (g.n3 + g.ybx - 1) / g.ybx;
   const dim3 gx(nb, mm.km);
   Cx<R>* T = pc_T<R>(p, 0) + mm.m0 * pc_work_elems(g);
+  Cx<R>* T2 = pc_T<R>(p, 1) + mm.m0 * pc_work_elems(g);
   k_pc_xfwd<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip,
                                                   mm.vs, mm.fs);
-  if (p->lu) {
-    VOX_TRY(lu_stream<R>(p, T, st, skip, mm.fs, mm.km));
-  } else {
-    Cx<R>* T2 = pc_T<R>(p, 1) + mm.m0 * pc_work_elems(g);
-    const int tiles = (g.n3 + 255) / 256;
-    k_pc_gemv<R><<<dim3(g.L * tiles, mm.km), 256, (size_t)g.n3 * cs, st>>>(g, pc_A<R>(p), T, T2,
-                                                                          skip, mm.fs);
-    T = T2;
-  }
-  k_pc_xinv<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T, p->op->vmap,
+  VOX_TRY(inv_apply<R>(p, T, T2, st, skip, mm.fs, mm.km));
+  k_pc_xinv<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T2, p->op->vmap,
                                                   (R)(1.0 / g.L), out, skip, mm.vs, mm.fs);
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
@@ -126,11 +133,9 @@ template <typename R>
 static vox_status pc_attrs() {
   VOX_TRY(smem_cap(k_pc_xfwd<R>));
   VOX_TRY(smem_cap(k_pc_xinv<R>));
-  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 2>));
-  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 4>));
-  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 8>));
-  VOX_TRY(smem_cap(k_pc_lu_stream2<R, 16>));
-  VOX_TRY(smem_cap(k_pc_gemv<R>));
+  VOX_TRY(smem_cap(k_pc_inv_apply<R, 2>));
+  VOX_TRY(smem_cap(k_pc_inv_apply<R, 4>));
+  VOX_TRY(smem_cap(k_pc_inv_apply<R, 8>));
   VOX_TRY(smem_cap(k_lu_batched<R>));
   return VOX_OK;
 }
@@ -142,6 +147,7 @@ static vox_status pc_alloc_work(vox_precond_s* p, int K) {
   VOX_TRY(dalloc(&p->Td2, LT));
   VOX_TRY(dalloc(&p->Tf, LT));
   VOX_TRY(dalloc(&p->Tf2, LT));
+  p->K = K;
   return VOX_OK;
 }
 
@@ -233,7 +239,8 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   // the LU panel bound (n3 <= 1760) also keeps the streamed solve's
   // ring + right-hand sides (64 KiB + 32 B * n3) under the cap
   if ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
-      lu_stream2_smem<double>(lu_npad(g.n3), 2) > (size_t)kSmemCap) {
+      lu_stream2_smem<double>(lu_npad(g.n3), kInvBuildCols) > (size_t)kSmemCap ||
+      inv_apply_smem<double>(g.n3, 2) > (size_t)kSmemCap) {
     set_error("preconditioner: 3*M*N too large for the batched LU panel");
     return VOX_ERR_UNSUPPORTED;
   }
@@ -247,6 +254,8 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   VOX_TRY(pc_alloc_work(p, op->K));
   VOX_TRY(pc_attrs<double>());
   VOX_TRY(pc_attrs<float>());
+  VOX_TRY(smem_cap(k_lu_inv_cols<kInvBuildCols>));
+  p->ld = lu_npad(g.n3);
   return VOX_OK;
 }
 
@@ -332,27 +341,31 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   k_lu_perm<<<Lf, 32, 0, st>>>(g.n3, p->piv, p->perm);
   k_tri_inv_blocks<<<dim3(nbd, Lf), 64, 0, st>>>(g.n3, ld, p->Ad, p->Dld, p->Dud);
   VOX_CUDA(cudaGetLastError());
-  // c64 copy: factors of B/Gram (the c64 operator is A/Gram): L unchanged,
-  // U / Gram (so inv(U) * Gram), so the copy applies Gram * M^{-1}
-  p->lu = true;
-  p->f_scale = op->gram;
-  // repack into per-mode tile streams in consumption order; the c64 stream
-  // holds U/Gram and Gram*inv(U_kk), so it applies Gram * M^{-1}
+  // repack the factors into per-mode tile streams in consumption order, then
+  // solve for the explicit inverse blocks (the reference's circ_inv) column
+  // group by column group into the factors' own buffer, which the tiles no
+  // longer need
   const long long tsz = (long long)Lf * lu_tiles(nbd) * kTrsvNb * kTrsvNb;
   VOX_TRY(dalloc(&p->tiles_d, tsz));
   k_tile_pack<double><<<dim3(lu_tiles(nbd), Lf), 256, 0, st>>>(nbd, ld, p->Ad, p->Dld, p->Dud,
                                                                1.0, 1.0, p->tiles_d);
-  if (op->has_f) {
-    VOX_TRY(dalloc(&p->tiles_f, tsz));
-    k_tile_pack<float><<<dim3(lu_tiles(nbd), Lf), 256, 0, st>>>(
-        nbd, ld, p->Ad, p->Dld, p->Dud, 1.0 / op->gram, op->gram, p->tiles_f);
-  }
+  VOX_CUDA(cudaMemsetAsync(p->Ad, 0, Lf * perp * sizeof(double2), st));
+  k_lu_inv_cols<kInvBuildCols>
+      <<<dim3((g.n3 + kInvBuildCols - 1) / kInvBuildCols, Lf), 32 * kRoundTiles,
+         lu_stream2_smem<double>(ld, kInvBuildCols), st>>>(g, p->tiles_d, p->perm, ld, p->Ad);
   VOX_CUDA(cudaGetLastError());
+  // c64 copy of Gram * inverse: it preconditions the c64 operator A/Gram
+  p->f_scale = op->gram;
+  if (op->has_f) {
+    VOX_TRY(dalloc(&p->Af, Lf * perp));
+    k_cast_scale<float><<<nblk(Lf * perp), 256, 0, st>>>(Lf * perp, p->Ad, op->gram, p->Af);
+    VOX_CUDA(cudaGetLastError());
+  }
   VOX_CUDA(cudaStreamSynchronize(st));
-  cudaFree(p->Ad);
+  cudaFree(p->tiles_d);
   cudaFree(p->Dld);
   cudaFree(p->Dud);
-  p->Ad = nullptr;
+  p->tiles_d = nullptr;
   p->Dld = p->Dud = nullptr;
   (void)dsz;
   pc_seal(p.get());
@@ -372,12 +385,21 @@ vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const do
   std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
   VOX_TRY(pc_common(op, p.get()));
   const PcGeom& g = p->g;
-  const long long tot = (long long)g.L * g.n3 * g.n3;
-  std::vector<double2> B(tot);
-  for (long long i = 0; i < tot; i++) B[i] = make_double2(blk_re[i], blk_im ? blk_im[i] : 0.0);
+  // every mode's block, stored at the padded leading dimension (zeros beyond n3)
+  const int ld = p->ld;
+  const long long per = (long long)ld * ld;
+  const long long tot = (long long)g.L * per;
+  std::vector<double2> B(tot, make_double2(0.0, 0.0));
+  for (long long i = 0; i < g.L; i++)
+    for (long long c = 0; c < g.n3; c++)
+      for (long long r = 0; r < g.n3; r++) {
+        const long long s = (i * g.n3 + c) * g.n3 + r;
+        B[i * per + c * ld + r] = make_double2(blk_re[s], blk_im ? blk_im[s] : 0.0);
+      }
   VOX_TRY(dalloc(&p->Ad, tot));
   VOX_CUDA(cudaMemcpy(p->Ad, B.data(), tot * sizeof(double2), cudaMemcpyHostToDevice));
-  p->lu = false;
+  p->Lf = g.L;
+  p->paired = 0;
   p->f_scale = op->gram;
   if (op->has_f) {
     VOX_TRY(dalloc(&p->Af, tot));
@@ -846,9 +868,16 @@ static vox_status refined_run(vox_op_s* op, vox_precond_s* pc, int side, int cou
       active[b] = rel[b] > tol;
     }
   }
-  std::vector<vox_gmres_info> ii(count);
-  std::vector<vox_gmres_info*> iip(count);
-  for (int b = 0; b < count; b++) iip[b] = &ii[b];
+  // the inner solves run over every member of the operator (members beyond
+  // count or already done are frozen), so one captured cycle serves every
+  // batch size
+  const int K = op->K;
+  std::vector<vox_gmres_info> ii(K);
+  std::vector<vox_gmres_info*> iip(K);
+  std::vector<std::vector<double>> rvi(K);
+  std::vector<char> take(K, 0);
+  itol.resize(K, 0.0);
+  for (int b = 0; b < K; b++) iip[b] = &ii[b];
   for (int it = 0; it < max_refine; it++) {
     bool anyact = false;
     for (int b = 0; b < count; b++) anyact = anyact || active[b];
@@ -864,8 +893,12 @@ static vox_status refined_run(vox_op_s* op, vox_precond_s* pc, int side, int cou
                          : std::min(0.5, std::max(inner_tol, 0.5 * tol * bn[b] / rn[b]));
       op->launches += 1;
     }
-    VOX_TRY(pgmres_dev<float>(op, pc, side, count, itol.data(), maxit_inner, iip.data(),
-                              rv.data(), active.data()));
+    for (int b = 0; b < K; b++) take[b] = b < count && active[b];
+    for (int b = 0; b < K; b++) rvi[b].clear();
+    VOX_TRY(pgmres_dev<float>(op, pc, side, K, itol.data(), maxit_inner, iip.data(),
+                              rvi.data(), take.data()));
+    for (int b = 0; b < count; b++)
+      if (active[b]) rv[b].insert(rv[b].end(), rvi[b].begin(), rvi[b].end());
     for (int b = 0; b < count; b++) {
       if (!active[b]) continue;
       info[b]->total_iters += ii[b].total_iters;
@@ -1097,18 +1130,14 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     });
     vox_status ps = VOX_OK;
     out[4] = timeit([&] {
-      if (pc->lu) {
-        ps = lu_stream<R>(pc, T, st, nullptr, 0, km);
-      } else {
-        k_pc_gemv<R><<<dim3(pg.L * ((pg.n3 + 255) / 256), km), 256, (size_t)pg.n3 * cs, st>>>(
-            pg, pc_A<R>(pc), T, pc_T<R>(pc, 1), nullptr, 0);
-      }
+      ps = inv_apply<R>(pc, T, pc_T<R>(pc, 1), st, nullptr, 0, km);
     });
     if (ps != VOX_OK) return ps;
     out[5] = timeit([&] {
-      k_pc_xinv<R><<<dim3(nb, km), 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), T,
-                                                                 op->vmap, (R)(1.0 / pg.L), w.t,
-                                                                 nullptr, w.vs, 0);
+      k_pc_xinv<R><<<dim3(nb, km), 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc),
+                                                                 pc_T<R>(pc, 1), op->vmap,
+                                                                 (R)(1.0 / pg.L), w.t, nullptr,
+                                                                 w.vs, 0);
     });
   }
   // Gram-Schmidt at basis size kgs+1 (done flag cleared before every launch)
@@ -1198,14 +1227,14 @@ vox_status vox_precond_share(vox_precond_t src, vox_op_t op, vox_precond_t* out)
   return VOX_OK;
 }
 
-vox_status vox_precond_info(vox_precond_t p, int* n_factored, int* ld, int* is_lu) {
+vox_status vox_precond_info(vox_precond_t p, int* n_blocks, int* ld, int* paired) {
   if (!p) {
     set_error("vox_precond_info: NULL preconditioner");
     return VOX_ERR_BAD_ARG;
   }
-  if (n_factored) *n_factored = p->lu ? p->Lf : p->g.L;
-  if (ld) *ld = p->lu ? lu_npad(p->g.n3) : p->g.n3;
-  if (is_lu) *is_lu = p->lu ? 1 : 0;
+  if (n_blocks) *n_blocks = p->Lf;
+  if (ld) *ld = p->ld;
+  if (paired) *paired = p->paired;
   return VOX_OK;
 }
 

@@ -9,17 +9,24 @@ Per device length (a "family") the loop keeps resident on the device:
 * one level-1 circulant preconditioner built at the band centre and shared by
   every wavelength of that length (vox_precond_share: one factor copy, per-slot
   work buffers);
-* a number of solve slots, each an operator + GMRES state + its own CUDA
-  stream.  The number of slots is set by the HBM footprint of one slot
+* a number of solve slots ("lanes"), each a batched operator of K members
+  (vox_op_create_batch: K copies of fN and of the GMRES state) + its own CUDA
+  stream.  The number of lanes is set by the HBM footprint of one lane
   against a memory budget ("admission by footprint").
 
-A request (length, wavelength) waits until it has arrived and a slot of its
-length is free; the slot then interpolates fN to the request's wavelength on
-the device (vox_op_interp), forms the right-hand side for the plane wave at
-that wavelength and runs the complex64 + FP64-refinement solve (or the plain
-complex128 GMRES for the baseline) through the C-ABI with host buffers.  Slots
-run in host threads (the C calls release the GIL), so solves of different
-lengths and wavelengths overlap on the GPU.  Latency = completion - arrival.
+A request (length, wavelength) waits until it has arrived and a lane of its
+length is free.  The lane then takes every request of its length that has
+arrived by then, up to K (continuous batching: requests that arrive while the
+lanes are busy join the next batch), interpolates each member's fN to its
+request's wavelength on the device (vox_op_interp_member), forms the
+right-hand sides for the plane wave at those wavelengths and runs the
+complex64 + FP64-refinement solve of the whole batch in lockstep
+(vox_solve_refined_batch: one launch per kernel for all members, the
+preconditioner's factors streamed once for all of them) through the C-ABI
+with host buffers.  Each result is identical to solving that request alone.
+Lanes run in host threads (the C calls release the GIL), so batches of
+different lengths overlap on the GPU.  Latency = completion - arrival.  The
+plain complex128 GMRES baseline solves one request at a time.
 """
 from __future__ import annotations
 
@@ -129,8 +136,11 @@ class _RhsBuilder:
 class Family:
     """Resident state of one device length."""
 
-    def __init__(self, key, problem: geo.Problem, band, nG=5, precond=True, device=0):
+    def __init__(self, key, problem: geo.Problem, band, nG=5, precond=True, device=0, members=1,
+                 G_nodes=None):
+        """G_nodes: the Toeplitz tensors at the nG nodes, if already assembled."""
         self.key = key
+        self.members = int(members)
         self.p = problem
         self.nodes = legendre_nodes(band[0], band[1], nG)
         self.idx = problem.idxS3()
@@ -140,7 +150,7 @@ class Family:
         Gc = None
         for j, lam in enumerate(self.nodes):
             pj = problem.with_wavelength(lam)
-            G = assemble_toeplitz(pj.shape, pj.ko, pj.res)
+            G = G_nodes[j] if G_nodes is not None else assemble_toeplitz(pj.shape, pj.ko, pj.res)
             self.node_ops.append(Operator(self.mop, pj.Gram, self.idx, G=G, device=device))
             if j == nG // 2:
                 Gc = G
@@ -155,8 +165,15 @@ class Family:
         self.device = device
         self.slots = []
 
-    def add_slot(self):
-        op = Operator(self.mop, self.p.Gram, self.idx, G=self._Gc, device=self.device)
+    def add_slot(self, stream=None):
+        """One more lane: a batched operator of `members` members, on its own
+        CUDA stream (a torch.cuda.Stream when given, needed for device-resident
+        right-hand sides)."""
+        op = Operator(self.mop, self.p.Gram, self.idx, G=self._Gc, device=self.device,
+                      members=self.members)
+        op.torch_stream = stream
+        if stream is not None:
+            op.set_stream(stream.cuda_stream)
         pc = self.pc.share(op) if self.pc is not None else None
         self.slots.append((op, pc))
         return self.slots[-1]
@@ -180,6 +197,8 @@ class ServeConfig:
     mode: str = "mixed"          # "mixed" (c64 + FP64 refinement) or "fp64" (plain c128 GMRES)
     maxit_fp64: int = 40
     keep_x: bool = False         # return each solution with its result
+    side: str = "left"           # preconditioning of the mixed-precision inner solves
+                                 # ("left" as the reference's L1, or "right")
 
 
 class SweepServer:
@@ -188,6 +207,35 @@ class SweepServer:
     def __init__(self, families, cfg: ServeConfig = None):
         self.families = {f.key: f for f in families}
         self.cfg = cfg or ServeConfig()
+        self._bufs = {}
+
+    def _solve_batch(self, fam: Family, op, pc, reqs):
+        """Mixed-precision solves of reqs (len <= members) in lockstep on one
+        lane; returns [(info, x)]."""
+        import ctypes
+        from . import _lib
+        if self.cfg.mode != "mixed":
+            return [self._solve(fam, op, pc, r) for r in reqs]
+        lib = _lib.lib()
+        n = op.n
+        count = len(reqs)
+        bre = np.empty((count, n))
+        bim = np.empty((count, n))
+        for i, req in enumerate(reqs):
+            op.interp(fam.node_ops, lagrange_weights(req.lam, fam.nodes), member=i)
+            b = fam.rhs(geo.C0 / req.lam * geo.N_EXT)
+            bre[i] = b.real
+            bim[i] = b.imag
+        xre = np.empty((count, n))
+        xim = np.empty((count, n))
+        infos = (_lib.GmresInfo * count)()
+        c = self.cfg
+        side = (1 if c.side == "left" else 2) if pc is not None else 0
+        _lib.check(lib.vox_solve_refined_batch(op.handle, pc.handle if pc is not None else None,
+                                               side, count, _lib.dptr(bre), _lib.dptr(bim),
+                                               c.tol, c.restart, c.maxit_inner, 0.0, 10,
+                                               _lib.dptr(xre), _lib.dptr(xim), infos))
+        return [(infos[i], (xre[i] + 1j * xim[i]) if c.keep_x else None) for i in range(count)]
 
     def _solve(self, fam: Family, op, pc, req: Request):
         import ctypes
@@ -224,8 +272,56 @@ class SweepServer:
         return Result(req.rid, req.key, req.lam, 0.0, 0.0, t1 - t0, info.total_iters,
                       info.relres, info.flag, x)
 
-    def serve(self, requests, realtime=True):
-        """Run the stream; returns (results, wall seconds)."""
+    def _solve_batch_device(self, fam: Family, op, pc, reqs, dev_b, dev_x):
+        """As _solve_batch with right-hand sides and solutions in device memory
+        (dev_b / dev_x: request id -> complex128 torch tensor), staged through the
+        lane's buffers on the lane's stream."""
+        import torch
+        c = self.cfg
+        n = op.n
+        s = op.torch_stream
+        key = id(op)
+        with torch.cuda.stream(s):
+            if key not in self._bufs:
+                self._bufs[key] = (torch.empty(op.members * n, dtype=torch.complex128,
+                                               device="cuda"),
+                                   torch.empty(op.members * n, dtype=torch.complex128,
+                                               device="cuda"))
+            bbuf, xbuf = self._bufs[key]
+            for i, req in enumerate(reqs):
+                op.interp(fam.node_ops, lagrange_weights(req.lam, fam.nodes), member=i)
+                bbuf[i * n:(i + 1) * n].copy_(dev_b[req.rid])
+            infos = op.solve_refined_batch_device(
+                bbuf.data_ptr(), xbuf.data_ptr(), len(reqs), pc=pc, side=c.side,
+                tol=c.tol, restart=c.restart, maxit_inner=c.maxit_inner, inner_tol=0.0,
+                max_refine=10)
+            for i, req in enumerate(reqs):
+                dev_x[req.rid].copy_(xbuf[i * n:(i + 1) * n])
+        return [(inf, None) for inf in infos]
+
+    def prepare_device(self):
+        """Allocate every lane's staging buffers for device-resident serving."""
+        import torch
+        for fam in self.families.values():
+            for op, pc in fam.slots:
+                with torch.cuda.stream(op.torch_stream):
+                    self._bufs[id(op)] = (
+                        torch.empty(op.members * op.n, dtype=torch.complex128, device="cuda"),
+                        torch.empty(op.members * op.n, dtype=torch.complex128, device="cuda"))
+
+    def warm(self):
+        """One full batch on every lane of every family (captures each lane's
+        restart-cycle graph before any timed work)."""
+        for fam in self.families.values():
+            lam = float(np.mean(fam.nodes))
+            reqs = [Request(-1, fam.key, lam, 0.0)] * fam.members
+            for op, pc in fam.slots:
+                self._solve_batch(fam, op, pc, reqs)
+
+    def serve(self, requests, realtime=True, device_io=None):
+        """Run the stream; returns (results, wall seconds).  device_io =
+        (dev_b, dev_x) serves right-hand sides already in device memory and
+        leaves the solutions there."""
         queues = {k: deque() for k in self.families}
         for r in sorted(requests, key=lambda r: r.arrival):
             queues[r.key].append(r)
@@ -237,25 +333,36 @@ class SweepServer:
 
         def worker(fam, op, pc):
             q = queues[fam.key]
+            K = getattr(op, "members", 1)
             while True:
                 with locks[fam.key]:
                     if not q:
                         return
-                    req = q.popleft()
+                    first = q.popleft()
                 now = time.perf_counter() - t0
-                if realtime and req.arrival > now:
-                    time.sleep(req.arrival - now)
+                if realtime and first.arrival > now:
+                    time.sleep(first.arrival - now)
+                # every request of this length that has arrived by now, up to K
+                batch = [first]
+                with locks[fam.key]:
+                    now = time.perf_counter() - t0
+                    while q and len(batch) < K and (not realtime or q[0].arrival <= now):
+                        batch.append(q.popleft())
                 start = time.perf_counter() - t0
                 try:
-                    info, x = self._solve(fam, op, pc, req)
+                    if device_io is not None:
+                        out = self._solve_batch_device(fam, op, pc, batch, *device_io)
+                    else:
+                        out = self._solve_batch(fam, op, pc, batch)
                 except Exception as e:  # surfaced after the threads join
                     errors.append(e)
                     return
                 done = time.perf_counter() - t0
                 with res_lock:
-                    results.append(Result(req.rid, req.key, req.lam, req.arrival if realtime
-                                          else 0.0, start, done, info.total_iters, info.relres,
-                                          info.flag, x))
+                    for req, (info, x) in zip(batch, out):
+                        results.append(Result(req.rid, req.key, req.lam,
+                                              req.arrival if realtime else 0.0, start, done,
+                                              info.total_iters, info.relres, info.flag, x))
 
         threads = [threading.Thread(target=worker, args=(fam, op, pc), daemon=True)
                    for fam in self.families.values() for (op, pc) in fam.slots]

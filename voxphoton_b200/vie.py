@@ -36,11 +36,14 @@ class Operator:
 
     Give either ``fN`` (2L x 2M x 2N x 6, the circulant FFT from
     getOPERATORS_SAM) or ``G`` (L x M x N x 6 Toeplitz, opToeplitz).
-    ``Mr=None`` means Mr == 1 (the JVIE-II form).
+    ``Mr=None`` means Mr == 1 (the JVIE-II form).  ``members=K`` makes a
+    batched operator: K independent copies of fN and of the solve state on one
+    grid and support (vox_op_create_batch), solved together by
+    ``solve_refined_batch``.
     """
 
     def __init__(self, Mc, Gram, idx, fN=None, G=None, Mr=None, precisions=("c128", "c64"),
-                 device=0):
+                 device=0, members=1):
         Mc = np.asarray(Mc)
         if Mc.ndim != 3:
             raise ValueError("Mc must be L x M x N")
@@ -79,8 +82,12 @@ class Operator:
         d.precisions = (1 if "c128" in precisions else 0) | (2 if "c64" in precisions else 0)
         d.device = device
         h = ctypes.c_void_p()
-        check(lib().vox_op_create(ctypes.byref(d), ctypes.byref(h)))
+        if members == 1:
+            check(lib().vox_op_create(ctypes.byref(d), ctypes.byref(h)))
+        else:
+            check(lib().vox_op_create_batch(ctypes.byref(d), int(members), ctypes.byref(h)))
         self._h = h
+        self.members = int(members)
         self._keep = []
         self._pcs = weakref.WeakSet()
         self.n = ia.size
@@ -132,11 +139,12 @@ class Operator:
         return self.mv_AN(JIn0)
 
     # ----------------------------------------------- device-resident calls
-    def interp(self, srcs, weights):
-        """fN <- sum_i weights[i] * srcs[i].fN on the device (lagrange_int.m)."""
+    def interp(self, srcs, weights, member=0):
+        """fN <- sum_i weights[i] * srcs[i].fN on the device (lagrange_int.m),
+        for one member of a batched operator."""
         arr = (ctypes.c_void_p * len(srcs))(*[s.handle for s in srcs])
         w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
-        check(lib().vox_op_interp(self._h, arr, dptr(w), len(srcs)))
+        check(lib().vox_op_interp_member(self._h, int(member), arr, dptr(w), len(srcs)))
 
     def set_stream(self, stream_ptr):
         """Run on the caller's cudaStream_t (an int handle; 0 restores the op's)."""
@@ -165,6 +173,17 @@ class Operator:
             ctypes.c_void_p(b_ptr), tol, restart, maxit_inner, inner_tol, max_refine,
             ctypes.c_void_p(x_ptr), ctypes.byref(info)))
         return info
+
+    def solve_refined_batch_device(self, b_ptr, x_ptr, count, pc=None, side=None, tol=1e-5,
+                                   restart=50, maxit_inner=20, inner_tol=1e-3, max_refine=10):
+        """vox_solve_refined_batch_device: `count` right-hand sides (member-major
+        interleaved complex128 device vectors) on members 0..count-1."""
+        infos = (_lib.GmresInfo * count)()
+        check(lib().vox_solve_refined_batch_device(
+            self._h, pc.handle if pc else None, _lib.SIDE[side] if pc else 0, int(count),
+            ctypes.c_void_p(b_ptr), tol, restart, maxit_inner, inner_tol, max_refine,
+            ctypes.c_void_p(x_ptr), infos))
+        return list(infos)
 
     def pgmres_device(self, b_ptr, x_ptr, pc=None, side=None, prec="c128", restart=50,
                       tol=1e-5, maxit=20):
@@ -247,10 +266,10 @@ class Preconditioner:
         return Preconditioner(op, h)
 
     def info(self):
-        nf, ld, lu = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        nf, ld, pr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(lib().vox_precond_info(self._h, ctypes.byref(nf), ctypes.byref(ld),
-                                     ctypes.byref(lu)))
-        return {"n_factored": nf.value, "ld": ld.value, "lu": bool(lu.value)}
+                                     ctypes.byref(pr)))
+        return {"n_blocks": nf.value, "ld": ld.value, "paired": bool(pr.value)}
 
     def apply(self, JIn, prec="c128"):
         re, im = split(JIn, self.op.n)
@@ -332,6 +351,73 @@ def solve_refined(A: Operator, b, tol=1e-5, restart=50, maxit_inner=20, inner_to
         "flag": info.flag, "relres": info.relres, "iters": info.total_iters,
         "refinements": info.refinements, "seconds": info.seconds,
         "resvec": buf[:min(info.n_resvec, buf.size)].copy()}
+
+
+def solve_refined_batch(A: Operator, bs, tol=1e-5, restart=50, maxit_inner=20, inner_tol=1e-3,
+                        max_refine=10, L1=None, R1=None):
+    """solve_refined for several right-hand sides at once on the members of a
+    batched operator (member i solves bs[i]); returns [(x, info dict)]."""
+    pc = L1 if L1 is not None else R1
+    side = 1 if L1 is not None else (2 if R1 is not None else 0)
+    count = len(bs)
+    B = np.stack([np.asarray(b, dtype=np.complex128).reshape(-1) for b in bs])
+    if B.shape[1] != A.n:
+        raise ValueError("right-hand sides must have length n")
+    re = np.ascontiguousarray(B.real)
+    im = np.ascontiguousarray(B.imag)
+    xre = np.empty((count, A.n))
+    xim = np.empty((count, A.n))
+    cap = restart * maxit_inner * max_refine + max_refine + 1
+    infos = (_lib.GmresInfo * count)()
+    bufs = [np.zeros(cap) for _ in range(count)]
+    for i in range(count):
+        infos[i].resvec = dptr(bufs[i])
+        infos[i].resvec_cap = cap
+    check(lib().vox_solve_refined_batch(A.handle, pc.handle if pc else None, side, count,
+                                        dptr(re), dptr(im), tol, restart, maxit_inner, inner_tol,
+                                        max_refine, dptr(xre), dptr(xim), infos))
+    out = []
+    for i in range(count):
+        inf = infos[i]
+        out.append((xre[i] + 1j * xim[i], {
+            "flag": inf.flag, "relres": inf.relres, "iters": inf.total_iters,
+            "refinements": inf.refinements, "seconds": inf.seconds,
+            "resvec": bufs[i][:min(inf.n_resvec, cap)].copy()}))
+    return out
+
+
+def E_field_Nop_const(J, op_full: Operator, Gram, freq, Einc=None, prec="c128"):
+    """E_field_Nop_const.m:59-84: the total field on the whole grid,
+    Etot = Einc + (N J - Gram J) / (Gram j omega eo).
+
+    J: L x M x N x 3 polarisation currents (zero outside the scatterer).
+    op_full: an Operator whose support is the whole grid (idx = 1..3LMN, as the
+    reference passes to mv_L_const) holding this wavelength's fN."""
+    J = np.asarray(J)
+    L, M, N, _ = J.shape
+    if op_full.n != 3 * L * M * N:
+        raise ValueError("op_full must be built on the whole grid (idx = 1..3*L*M*N)")
+    mu = 4 * np.pi * 1e-7
+    co = 299792458.0
+    eo = 1.0 / co ** 2 / mu
+    omega = 2 * np.pi * freq
+    E = op_full.mv_L(J.reshape(-1, order="F"), prec=prec).reshape((L, M, N, 3), order="F")
+    E = E / (Gram * 1j * omega * eo)
+    return E if Einc is None else Einc + E
+
+
+def transmitted_power(E, res, len_abs, delW):
+    """example_Bragg_1500nm_to_1600nm.m:107-113: sum of |E|^2 over the voxel
+    slice x = L - round((len_abs + 450 nm) / res) (1-based), trimmed by
+    round(delW / 2) / res voxels at each y edge.  The rounding is of a length
+    in metres, as in the reference, so for nanometre corrugations nothing is
+    trimmed."""
+    E = np.asarray(E)
+    L, M = E.shape[:2]
+    x_thru = L - int(np.round((len_abs + 450e-9) / res))
+    vox = int(np.round(np.round(delW / 2) / res))
+    e = E[x_thru - 1, vox:M - vox, :, :]
+    return float(np.sum((e * np.conj(e)).real))
 
 
 def jvie_rhs(e_r, Einc, Gram, freq, idx):
