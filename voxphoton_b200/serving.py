@@ -250,9 +250,9 @@ class SweepServer:
         xre = np.empty(op.n)
         xim = np.empty(op.n)
         info = _lib.GmresInfo()
-        side = 1 if pc is not None else 0
-        pch = pc.handle if pc is not None else None
         c = self.cfg
+        side = (1 if c.side == "left" else 2) if pc is not None else 0
+        pch = pc.handle if pc is not None else None
         if c.mode == "mixed":
             _lib.check(lib.vox_solve_refined(op.handle, pch, side, _lib.dptr(bre), _lib.dptr(bim),
                                              c.tol, c.restart, c.maxit_inner, 0.0, 10,
