@@ -231,6 +231,39 @@ vox_status vox_solve_refined_batch_device(vox_op_t op, vox_precond_t pc, int sid
                                           int maxit_inner, double inner_tol, int max_refine,
                                           void* x, vox_gmres_info* infos);
 
+/* Continuous batching on a batched operator (no reference counterpart: the
+ * reference solves one system per call).  A lane runs, for each member of the
+ * operator, the solve of vox_solve_refined on that member's right-hand side;
+ * every restart cycle is one launch per kernel for all members solving, and
+ * a member takes a new right-hand side as soon as its previous solve has
+ * finished and been collected, without waiting for the other members.  Each
+ * result is identical to vox_solve_refined on that member alone.  The lane
+ * owns the operator's solve state while members are solving (do not call the
+ * other solver entry points on that operator meanwhile); destroying the
+ * operator destroys its lanes.  pc must be a handle made or shared for this
+ * operator (vox_precond_share), side as for vox_pgmres. */
+typedef struct vox_lane_s* vox_lane_t;
+vox_status vox_lane_create(vox_op_t op, vox_precond_t pc, int side, double tol, int restart,
+                           int maxit_inner, double inner_tol, int max_refine, vox_lane_t* out);
+void vox_lane_destroy(vox_lane_t lane);
+/* Start a solve on a free member: b and x are interleaved double2 device
+ * vectors of n_idx (x receives the solution; both must stay valid until the
+ * member is collected). */
+vox_status vox_lane_submit_device(vox_lane_t lane, int member, const void* b, void* x);
+/* The same from host buffers (split complex, length n_idx); the solution is
+ * returned by vox_lane_collect. */
+vox_status vox_lane_submit(vox_lane_t lane, int member, const double* b_re, const double* b_im);
+/* One restart cycle for every solving member plus their refinement steps;
+ * the members that finished are written to done (room for `members`
+ * entries), their count to *n_done. */
+vox_status vox_lane_step(vox_lane_t lane, int* done, int* n_done);
+/* Result of a finished member (x_re/x_im: host copy of the solution for host
+ * submissions, or NULL), which then becomes free. */
+vox_status vox_lane_collect(vox_lane_t lane, int member, double* x_re, double* x_im,
+                            vox_gmres_info* info);
+/* Per member: 0 free, 1 solving, 2 finished and not yet collected. */
+vox_status vox_lane_state(vox_lane_t lane, int* states);
+
 /* Vrhs = Gram * (j omega eo Mc_raw) .* Einc(idx) ./ Mr(idx)  (JVIE-II), with
  * Mc_raw = e_r - 1, Mr = e_r; e_r and Einc column-major (L x M x N, x3 for Einc). */
 vox_status vox_jvie_rhs(int L, int M, int N, const double* er_re, const double* er_im,

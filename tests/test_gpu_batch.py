@@ -114,3 +114,35 @@ def test_stage_profile_of_a_batch(family):
     assert all(v > 0 for v in st.values())
     pcb.close()
     op.close()
+
+
+def test_lane_refills_members_and_matches_solo_solves(family):
+    # 5 requests on 3 members: slots are refilled while other members are
+    # mid-solve; every result must equal the single-right-hand-side solve
+    p, idx, Gs, nodes, pc, rhs = family
+    lams = np.linspace(1502e-9, 1598e-9, 5)
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=Gs[1], members=3)
+    pcb = pc.share(op)
+    lane = vb.Lane(op, pcb, side="left", tol=1e-5, restart=50, maxit_inner=40)
+    queue = list(range(len(lams)))
+    inflight, out = {}, {}
+    while queue or inflight:
+        for m in range(3):
+            if m not in inflight and queue:
+                i = queue.pop(0)
+                op.interp(nodes, sv.lagrange_weights(lams[i], NODES), member=m)
+                lane.submit(m, rhs(geo.C0 / lams[i] * geo.N_EXT))
+                inflight[m] = i
+        for m in lane.step():
+            out[inflight.pop(m)] = lane.collect(m)
+    assert sorted(out) == list(range(len(lams)))
+    for i, l in enumerate(lams):
+        x, info = out[i]
+        xs, is_ = _solo(p, idx, Gs, nodes, pc, l, rhs(geo.C0 / l * geo.N_EXT))
+        assert info["flag"] == 0 and info["relres"] <= 1e-5
+        assert info["iters"] == is_["iters"] and info["refinements"] == is_["refinements"]
+        assert np.array_equal(x, xs)
+        assert np.array_equal(info["resvec"], is_["resvec"])
+    lane.close()
+    pcb.close()
+    op.close()

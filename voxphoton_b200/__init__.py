@@ -5,10 +5,10 @@ FFT-circulant matvec, level-1 circulant preconditioner and device GMRES with
 an FP32 + FP64-refinement solver.  See voxphoton_b200.vie for the
 MATLAB-facing calls (mv_AN_const, chan_mvp_idx, pgmres).
 """
-from .vie import (E_field_Nop_const, Operator, Preconditioner, assemble_toeplitz, chan_mvp_idx,
+from .vie import (E_field_Nop_const, Lane, Operator, Preconditioner, assemble_toeplitz, chan_mvp_idx,
                   face3_from_Mr, jvie_rhs, mv_AN_const, mv_L_const, pgmres, singular_integrals,
                   solve_refined, solve_refined_batch, transmitted_power)
 
-__all__ = ["E_field_Nop_const", "transmitted_power", "Operator", "Preconditioner", "assemble_toeplitz", "chan_mvp_idx", "face3_from_Mr",
+__all__ = ["E_field_Nop_const", "Lane", "transmitted_power", "Operator", "Preconditioner", "assemble_toeplitz", "chan_mvp_idx", "face3_from_Mr",
            "jvie_rhs", "mv_AN_const", "mv_L_const", "pgmres", "singular_integrals",
            "solve_refined", "solve_refined_batch"]

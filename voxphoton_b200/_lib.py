@@ -133,6 +133,19 @@ SIGNATURES = [
                                                ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_int, _dp, _dp,
                                                ctypes.POINTER(GmresInfo)]),
+    ("vox_lane_create", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    ("vox_lane_destroy", None, [ctypes.c_void_p]),
+    ("vox_lane_submit_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_void_p]),
+    ("vox_lane_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp]),
+    ("vox_lane_step", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int)]),
+    ("vox_lane_collect", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp,
+                                        ctypes.POINTER(GmresInfo)]),
+    ("vox_lane_state", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("vox_solve_refined_batch_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                                       ctypes.c_int, ctypes.c_int,
                                                       ctypes.c_void_p, ctypes.c_double,

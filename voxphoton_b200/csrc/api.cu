@@ -183,6 +183,8 @@ static_assert(sizeof(GmresDev) % sizeof(int) == 0, "GmresDev size");
 
 using namespace vox;
 
+struct vox_lane_s;
+
 struct vox_op_s {
   int device = 0;
   int K = 1;                          // members (independent solves of this shape)
@@ -208,6 +210,7 @@ struct vox_op_s {
   GmresWork<double> wd;
   GmresWork<float> wf;
   std::vector<vox_precond_s*> pcs;
+  std::vector<vox_lane_s*> lanes;  // continuous-batching lanes on this operator
 };
 
 namespace vox {
@@ -436,11 +439,14 @@ static void free_bufs(OpBuffers<R>& b) {
 }
 
 static void pc_release(vox_precond_s* p);
+static void lanes_release(vox_op_s* op);
 
 static void destroy_op(vox_op_s* op) {
   if (!op) return;
   DeviceGuard dg(op->device);
   cudaDeviceSynchronize();
+  // lanes and preconditioners use the operator's state: they go with it
+  lanes_release(op);
   // preconditioners hold the operator's index map: they go with it
   std::vector<vox_precond_s*> pcs = op->pcs;
   for (vox_precond_s* p : pcs) pc_release(p);
@@ -775,6 +781,15 @@ vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* 
 }  // extern "C"
 
 #include "solver.cuh"
+#include "lane.cuh"
+
+namespace vox {
+static void lanes_release(vox_op_s* op) {
+  std::vector<vox_lane_s*> ls = op->lanes;
+  for (vox_lane_s* l : ls) delete l;
+  op->lanes.clear();
+}
+}  // namespace vox
 
 // ------------------------------------------------ matvec without allocation
 // Some callers cannot call cudaMalloc at the point where they need a product:

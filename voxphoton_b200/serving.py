@@ -38,7 +38,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import geometry as geo
-from .vie import Operator, Preconditioner, assemble_toeplitz
+from .vie import Lane, Operator, Preconditioner, assemble_toeplitz
 
 
 def legendre_nodes(lam_lo, lam_hi, nG):
@@ -199,6 +199,9 @@ class ServeConfig:
     keep_x: bool = False         # return each solution with its result
     side: str = "left"           # preconditioning of the mixed-precision inner solves
                                  # ("left" as the reference's L1, or "right")
+    batching: str = "continuous"  # "continuous" (a member slot is refilled as soon as
+                                  # its solve ends) or "lockstep" (a lane's batch
+                                  # starts and ends together)
 
 
 class SweepServer:
@@ -208,6 +211,7 @@ class SweepServer:
         self.families = {f.key: f for f in families}
         self.cfg = cfg or ServeConfig()
         self._bufs = {}
+        self._lanes = {}
 
     def _solve_batch(self, fam: Family, op, pc, reqs):
         """Mixed-precision solves of reqs (len <= members) in lockstep on one
@@ -318,6 +322,19 @@ class SweepServer:
             for op, pc in fam.slots:
                 self._solve_batch(fam, op, pc, reqs)
 
+    def _lane(self, fam: Family, op, pc):
+        key = id(op)
+        if key not in self._lanes:
+            c = self.cfg
+            self._lanes[key] = Lane(op, pc, side=c.side, tol=c.tol, restart=c.restart,
+                                    maxit_inner=c.maxit_inner, inner_tol=0.0, max_refine=10)
+        return self._lanes[key]
+
+    def close(self):
+        for ln in self._lanes.values():
+            ln.close()
+        self._lanes = {}
+
     def serve(self, requests, realtime=True, device_io=None):
         """Run the stream; returns (results, wall seconds).  device_io =
         (dev_b, dev_x) serves right-hand sides already in device memory and
@@ -364,7 +381,51 @@ class SweepServer:
                                               req.arrival if realtime else 0.0, start, done,
                                               info.total_iters, info.relres, info.flag, x))
 
-        threads = [threading.Thread(target=worker, args=(fam, op, pc), daemon=True)
+        def lane_worker(fam, op, pc):
+            # continuous batching: admit arrived requests into free members,
+            # run one restart cycle of every solving member, collect the
+            # finished ones, repeat
+            q = queues[fam.key]
+            lane = self._lane(fam, op, pc)
+            inflight = {}  # member -> (request, start time)
+            try:
+                while True:
+                    free = [m for m in range(lane.members) if m not in inflight]
+                    admit = []
+                    with locks[fam.key]:
+                        now = time.perf_counter() - t0
+                        while free and q and (not realtime or q[0].arrival <= now):
+                            admit.append((free.pop(0), q.popleft()))
+                        nxt = q[0].arrival if q else None
+                    for m, req in admit:
+                        op.interp(fam.node_ops, lagrange_weights(req.lam, fam.nodes), member=m)
+                        if device_io is not None:
+                            dev_b, dev_x = device_io
+                            lane.submit_device(m, dev_b[req.rid].data_ptr(),
+                                               dev_x[req.rid].data_ptr())
+                        else:
+                            lane.submit(m, fam.rhs(geo.C0 / req.lam * geo.N_EXT))
+                        inflight[m] = (req, time.perf_counter() - t0)
+                    if not inflight:
+                        if nxt is None:
+                            return
+                        time.sleep(max(0.0, nxt - (time.perf_counter() - t0)))
+                        continue
+                    for m in lane.step():
+                        req, start = inflight.pop(m)
+                        x, info = lane.collect(m, host=device_io is None)
+                        done = time.perf_counter() - t0
+                        with res_lock:
+                            results.append(Result(req.rid, req.key, req.lam,
+                                                  req.arrival if realtime else 0.0, start, done,
+                                                  info["iters"], info["relres"], info["flag"],
+                                                  x if self.cfg.keep_x else None))
+            except Exception as e:  # surfaced after the threads join
+                errors.append(e)
+
+        target = lane_worker if (self.cfg.batching == "continuous" and self.cfg.mode == "mixed") \
+            else worker
+        threads = [threading.Thread(target=target, args=(fam, op, pc), daemon=True)
                    for fam in self.families.values() for (op, pc) in fam.slots]
         for t in threads:
             t.start()

@@ -353,6 +353,67 @@ def solve_refined(A: Operator, b, tol=1e-5, restart=50, maxit_inner=20, inner_to
         "resvec": buf[:min(info.n_resvec, buf.size)].copy()}
 
 
+class Lane:
+    """Continuous batching on a batched operator (vox_lane_*): every member
+    runs its own complex64 + FP64-refinement solve, all members' restart
+    cycles share one launch per kernel, and a member takes a new right-hand
+    side as soon as its previous solve is collected.  Each result equals
+    solve_refined on that member alone."""
+
+    def __init__(self, op: Operator, pc=None, side="left", tol=1e-5, restart=50, maxit_inner=40,
+                 inner_tol=0.0, max_refine=10):
+        h = ctypes.c_void_p()
+        check(lib().vox_lane_create(op.handle, pc.handle if pc else None,
+                                    _lib.SIDE[side] if pc else 0, tol, restart, maxit_inner,
+                                    inner_tol, max_refine, ctypes.byref(h)))
+        self._h = h
+        self.op = op
+        self.members = op.members
+        self._cap = restart * maxit_inner * max_refine + max_refine + 1
+        self._done = (ctypes.c_int * op.members)()
+        op._lanes = getattr(op, "_lanes", []) + [self]
+
+    def submit(self, member, b):
+        """Start a solve of b (host vector) on a free member."""
+        re, im = split(b, self.op.n)
+        check(lib().vox_lane_submit(self._h, int(member), dptr(re), dptr(im)))
+
+    def submit_device(self, member, b_ptr, x_ptr):
+        """Start a solve with device vectors (interleaved complex128)."""
+        check(lib().vox_lane_submit_device(self._h, int(member), ctypes.c_void_p(b_ptr),
+                                           ctypes.c_void_p(x_ptr)))
+
+    def step(self):
+        """One restart cycle of every solving member; returns the members that
+        finished."""
+        nd = ctypes.c_int()
+        check(lib().vox_lane_step(self._h, self._done, ctypes.byref(nd)))
+        return [self._done[i] for i in range(nd.value)]
+
+    def collect(self, member, host=True):
+        """(x or None, info dict) of a finished member, which becomes free."""
+        info, buf = _info(self._cap)
+        n = self.op.n
+        xre = np.empty(n) if host else None
+        xim = np.empty(n) if host else None
+        check(lib().vox_lane_collect(self._h, int(member), dptr(xre) if host else None,
+                                     dptr(xim) if host else None, ctypes.byref(info)))
+        x = xre + 1j * xim if host else None
+        return x, {"flag": info.flag, "relres": info.relres, "iters": info.total_iters,
+                   "refinements": info.refinements,
+                   "resvec": buf[:min(info.n_resvec, buf.size)].copy()}
+
+    def state(self):
+        st = (ctypes.c_int * self.members)()
+        check(lib().vox_lane_state(self._h, st))
+        return list(st)
+
+    def close(self):
+        if getattr(self, "_h", None) and getattr(self.op, "_h", None):
+            lib().vox_lane_destroy(self._h)
+        self._h = None
+
+
 def solve_refined_batch(A: Operator, bs, tol=1e-5, restart=50, maxit_inner=20, inner_tol=1e-3,
                         max_refine=10, L1=None, R1=None):
     """solve_refined for several right-hand sides at once on the members of a
