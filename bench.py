@@ -60,6 +60,8 @@ def parse():
                     help="solves per lane advanced in lockstep (batched operator members)")
     ap.add_argument("--sweep-side", default="left", choices=["left", "right"],
                     help="preconditioning side of the mixed-precision inner solves")
+    ap.add_argument("--sweep-batching", default="continuous", choices=["continuous", "lockstep"],
+                    help="member slots refilled as solves finish, or whole batches")
     ap.add_argument("--sweep-fp64", type=int, default=10,
                     help="requests solved one at a time in plain complex128 for the baseline")
     ap.add_argument("--seed", type=int, default=0)
@@ -359,7 +361,7 @@ def run_sweep(args, world, rank, local):
             op.set_stream(op.torch_stream.cuda_stream)
     items = [(pr, lam) for lam in lams for pr in periods]
     reqs = sv.poisson_stream(items, rate=args.sweep_rate, seed=args.seed + rank)
-    cfg = sv.ServeConfig(tol=args.tol, side=args.sweep_side)
+    cfg = sv.ServeConfig(tol=args.tol, side=args.sweep_side, batching=args.sweep_batching)
     srv = sv.SweepServer(fams, cfg)
     srv.prepare_device()
     # warm-up: a full batch on every lane (captures the cycle graphs), then W
@@ -430,6 +432,7 @@ def run_sweep(args, world, rank, local):
     # the lanes are done: free them and the staged vectors before the baseline
     del dev_b, dev_x
     srv._bufs.clear()
+    srv.close()
     for f in fams:
         for op, pc in f.slots:
             pc.close()
@@ -494,7 +497,8 @@ def run_sweep(args, world, rank, local):
                                        f"{args.sweep_rate}/s (seed {args.seed + rank}), sizes "
                                        f"interleaved; one step = one wavelength at all lengths",
                            "tol": args.tol, "restart": args.restart,
-                           "solver": "complex64 GMRES + FP64 refinement, lockstep batches",
+                           "solver": f"complex64 GMRES + FP64 refinement, {args.sweep_batching} "
+                                     f"batching",
                            "lanes_per_length": nslots, "members_per_lane": K,
                            "lane_bytes": int(lane_bytes), "setup_s": round(setup_s, 1),
                            "operator": "Lagrange interpolation of fN over 5 Legendre wavelengths",

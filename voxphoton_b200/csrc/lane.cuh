@@ -226,10 +226,16 @@ static vox_status lane_step(vox_lane_s* L, int* done, int* n_done) {
   bool any = false;
   for (int b = 0; b < K; b++) any = any || (L->m[b].state == 1 && L->m[b].inner);
   if (any) {
-    cudaGraphExec_t cyc = nullptr;
-    VOX_TRY(get_cycle_graph<float>(op, L->pc, L->side, K, &cyc));
-    VOX_CUDA(cudaGraphLaunch(cyc, st));
-    op->launches += op->graph_nodes[cyc];
+    if (use_cycle_graphs()) {
+      cudaGraphExec_t cyc = nullptr;
+      VOX_TRY(get_cycle_graph<float>(op, L->pc, L->side, K, &cyc));
+      VOX_CUDA(cudaGraphLaunch(cyc, st));
+      op->launches += op->graph_nodes[cyc];
+    } else {
+      int nk = 0;
+      VOX_TRY(enqueue_cycle<float>(op, L->pc, L->side, K, st, &nk));
+      op->launches += nk;
+    }
     for (int b = 0; b < K; b++)
       if (L->m[b].state == 1 && L->m[b].inner)
         VOX_CUDA(cudaMemcpyAsync(wf.hdr(b), &wf.st[b], offsetof(GmresDev, sn),
@@ -308,8 +314,10 @@ vox_status vox_lane_create(vox_op_t op, vox_precond_t pc, int side, double tol, 
   // every member frozen until it takes a right-hand side
   for (int b = 0; b < op->K; b++) VOX_TRY(lane_header(L.get(), b, 0.0, 1));
   VOX_CUDA(cudaStreamSynchronize(op->stream));
-  cudaGraphExec_t cyc = nullptr;
-  VOX_TRY(get_cycle_graph<float>(op, pc, L->side, op->K, &cyc));
+  if (use_cycle_graphs()) {
+    cudaGraphExec_t cyc = nullptr;
+    VOX_TRY(get_cycle_graph<float>(op, pc, L->side, op->K, &cyc));
+  }
   op->lanes.push_back(L.get());
   *out = L.release();
   return VOX_OK;

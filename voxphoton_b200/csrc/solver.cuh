@@ -617,6 +617,17 @@ __global__ void k_sub(long long n, const Cx<R>* __restrict__ b, const Cx<R>* __r
     r[i] = csub(b[i], ax[i]);
 }
 
+// VOX_GRAPHS=0 enqueues each cycle's kernels directly instead of replaying the
+// captured graph (same kernels and order; for profilers that cannot follow
+// stream capture)
+static bool use_cycle_graphs() {
+  static const bool on = [] {
+    const char* e = std::getenv("VOX_GRAPHS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 // st[b].scal[slot] of the members with use[b] (all when use is null), one sync
 template <typename R>
 static vox_status read_scals(vox_op_s* op, int slot, int km, const char* use, double* v) {
@@ -691,15 +702,8 @@ static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, int km, 
     VOX_CUDA(cudaMemcpyAsync(&w.st[b], hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
     VOX_CUDA(cudaStreamSynchronize(st));
   }
-  // VOX_GRAPHS=0 enqueues each cycle's kernels directly instead of replaying
-  // the captured graph (same kernels and order; for profilers that cannot
-  // follow stream capture)
-  static const bool use_graphs = [] {
-    const char* e = std::getenv("VOX_GRAPHS");
-    return !(e && e[0] == '0');
-  }();
   cudaGraphExec_t cyc = nullptr;
-  if (use_graphs) VOX_TRY(get_cycle_graph<R>(op, pc, side, km, &cyc));
+  if (use_cycle_graphs()) VOX_TRY(get_cycle_graph<R>(op, pc, side, km, &cyc));
   auto any = [&] {
     for (int b = 0; b < km; b++)
       if (active[b]) return true;
