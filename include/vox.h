@@ -176,6 +176,28 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
  * each column-major, concatenated (chan_mvp_idx's inv_blocks). */
 vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const double* blk_im,
                                      vox_precond_t* out);
+/* Circulant preconditioner on a box of the grid (x0 <= x < x0+Ls,
+ * y0 <= y < y0+Ms, every z): level 1 is level_1_parallel_func
+ * (piecewise_constant/src_preconditioning/level_1_parallel_func.m:1-255: per
+ * x-mode the inverse of the 3MN block of A = -Mc.*G + Gram*Mr1 at the origin),
+ * level 2 is level_2_parallel_func (level_2_parallel_func.m:1-193: a second T.
+ * Chan circulant along y, per (x, y)-mode inverse 3N x 3N blocks) applied as
+ * chan_2_mvp_for_parallel_idx.m:2-22.  G: the box's Toeplitz tensor
+ * (Ls x Ms x N x 6, column-major), Mc: the box's contrast (Ls x Ms x N), mask:
+ * which box voxels it acts on (Ls*Ms*N bytes, NULL = all of the operator's
+ * unknowns in the box), scale multiplies the inverse (the resonator script
+ * negates it: -1).  Level 2 needs 3N <= 64 and M with prime factors <= 64.
+ * On its own it acts on the box's unknowns only; combine with
+ * vox_precond_create_sum. */
+vox_status vox_precond_create_box(vox_op_t op, int level, int x0, int y0, int Ls, int Ms,
+                                  const unsigned char* mask, const double* G_re,
+                                  const double* G_im, const double* Mc_re, const double* Mc_im,
+                                  double Mr1, double scale, vox_precond_t* out);
+/* prec_fun_disk_idx (prec_fun_disk_idx.m:1-23): each part applied on its own
+ * unknowns, the identity on the unknowns of no part.  The parts (handles made
+ * on op) become owned by the sum: destroy only the sum. */
+vox_status vox_precond_create_sum(vox_op_t op, const vox_precond_t* parts, int n,
+                                  vox_precond_t* out);
 void vox_precond_destroy(vox_precond_t p);
 /* A second handle on the same factors, bound to `op` (same grid and support
  * idx as the source's operator), with its own work buffers: lets solves on

@@ -313,6 +313,130 @@ def level_1_parallel_func_N(opToeplitz, L, M, N, Gram):
     return circ, circ_L
 
 
+def _level1_temp(cc, CC, C3, C4, C5, C6, il, M, N):
+    """The 3MN x 3MN block of x-mode il assembled from the x-FFT'd Chan
+    circulants (level_1_parallel_func_N.m:113-190, level_1_parallel_func.m:90-165,
+    level_2_parallel_func.m:96-166: the same toeplitz / cell2mat / triu steps)."""
+    MN = M * N
+    zblk = toeplitz(np.arange(N))
+
+    def block_toeplitz(chan):
+        res = np.zeros((MN, MN), dtype=complex)
+        for p in range(N):
+            for q in range(N):
+                res[p * M:(p + 1) * M, q * M:(q + 1) * M] = chan[zblk[p, q]]
+        return res
+
+    temp = np.zeros((3 * MN, 3 * MN), dtype=complex)
+    chan = [toeplitz(cc[il, :, i], cc[il, :, i]) for i in range(N)]
+    temp[:MN, :MN] = block_toeplitz(chan)
+    chan = [toeplitz(np.concatenate(([-CC[il, 0, i]], CC[il, 1:, i])), -CC[il, :, i])
+            for i in range(N)]
+    res = block_toeplitz(chan)
+    temp[:MN, MN:2 * MN] = res
+    temp[MN:2 * MN, :MN] = res
+    chan = [toeplitz(-C3[il, :, i], -C3[il, :, i]) for i in range(N)]
+    res = block_toeplitz(chan)
+    U = np.triu(res)
+    res = U - U.T + np.diag(np.diag(U))
+    temp[:MN, 2 * MN:] = res
+    temp[2 * MN:, :MN] = res
+    chan = [toeplitz(C4[il, :, i], C4[il, :, i]) for i in range(N)]
+    temp[MN:2 * MN, MN:2 * MN] = block_toeplitz(chan)
+    chan = [toeplitz(np.concatenate(([C5[il, 0, i]], -C5[il, 1:, i])), C5[il, :, i])
+            for i in range(N)]
+    res = block_toeplitz(chan)
+    U = np.triu(res)
+    res = U + U.T - np.diag(np.diag(U))
+    temp[MN:2 * MN, 2 * MN:] = res
+    temp[2 * MN:, MN:2 * MN] = res
+    chan = [toeplitz(C6[il, :, i], C6[il, :, i]) for i in range(N)]
+    temp[2 * MN:, 2 * MN:] = block_toeplitz(chan)
+    return temp
+
+
+def _contrast_spectra(opToeplitz, Mc, Mr, Gram):
+    """level_1_parallel_func.m:5-84 / level_2_parallel_func.m:5-84: the six
+    components of -Mc .* opToeplitz (elementwise on the grid), Gram*Mr(1) added
+    at the origin of the diagonal components, Chan circulant along x and FFT."""
+    Mc = np.asarray(Mc)
+    A = -Mc[..., None] * opToeplitz
+    mr1 = np.asarray(Mr).reshape(-1, order="F")[0]
+    for c in (0, 3, 5):
+        A[0, 0, 0, c] = Gram * mr1 + A[0, 0, 0, c]
+    signs = (+1, -1, -1, +1, +1, +1)
+    return [np.fft.fft(_chan_axis0(A[..., c], signs[c]), axis=0) for c in range(6)]
+
+
+def level_1_parallel_func(opToeplitz, Mc, Mr, L, M, N, Gram):
+    """level_1_parallel_func.m:1-255: circ_inv{i} = inv(temp_i), temp_i the
+    3MN x 3MN block of x-mode i of -Mc.*G (+ Gram*Mr(1) at the origin)."""
+    sp = _contrast_spectra(opToeplitz, Mc, Mr, Gram)
+    return [np.linalg.inv(_level1_temp(*sp, il, M, N)) for il in range(L)]
+
+
+def level_2_parallel_func(opToeplitz, Mc, Mr, L, M, N, Gram):
+    """level_2_parallel_func.m:1-193: per x-mode i, the T. Chan circulant along y
+    of every M x M sub-block of temp_i, diagonalised by FFT, collapsed to M blocks
+    of 3N x 3N (one per y-mode) and inverted: circ_2_inv[i][m]."""
+    sp = _contrast_spectra(opToeplitz, Mc, Mr, Gram)
+    out = []
+    for il in range(L):
+        temp = _level1_temp(*sp, il, M, N)
+        diag_t = np.zeros((3 * M * N, 3 * M * N), dtype=complex)
+        c = np.zeros(M, dtype=complex)
+        for k in range(3 * N):          # :170-186, 1-based j, k in the reference
+            for j in range(3 * N):
+                row_vec = temp[j * M, k * M:(k + 1) * M]
+                col_vec = temp[j * M:(j + 1) * M, k * M]
+                c[0] = col_vec[0]
+                for i in range(2, M + 1):
+                    c[i - 1] = (M + 1 - i) / M * col_vec[i - 1] + (i - 1) / M * row_vec[M - i + 1]
+                diag_t[j * M:(j + 1) * M, k * M:(k + 1) * M] = np.diag(np.fft.fft(c))
+        # :190 diag_block_collapse_temp = reshape(reshape(X.',3*M*M*N,3*N).',3*M*N,3*M*N)
+        X = diag_t.T.reshape((3 * M * M * N, 3 * N), order="F").T
+        col = X.reshape((3 * M * N, 3 * M * N), order="F")
+        out.append([np.linalg.inv(col[m * 3 * N:(m + 1) * 3 * N, m * 3 * N:(m + 1) * 3 * N])
+                    for m in range(M)])
+    return out
+
+
+def chan_2_mvp_for_parallel_idx(inv_blocks, JIn, L, M, N, idx):
+    """chan_2_mvp_for_parallel_idx.m:2-22: scatter, FFT along x, per x-mode FFT
+    along y, per (x, y) mode a 3N x 3N product, inverse FFTs, gather."""
+    Vrhs = np.zeros(3 * L * M * N, dtype=complex)
+    ii = np.asarray(idx, dtype=np.int64) - 1
+    Vrhs[ii] = JIn
+    temp = Vrhs.reshape((L, 3 * M * N), order="F")
+    temp = np.fft.fft(temp, axis=0).T
+    for i in range(L):
+        T = temp[:, i].reshape((M, 3 * N), order="F")
+        T = np.fft.fft(T, axis=0).T
+        for j in range(M):
+            T[:, j] = inv_blocks[i][j] @ T[:, j]
+        T = np.fft.ifft(T.T, axis=0)
+        temp[:, i] = T.reshape(-1, order="F")
+    temp = np.fft.ifft(temp.T, axis=0)
+    return temp.reshape(-1, order="F")[ii]
+
+
+def prec_fun_disk_idx(J, circ_WG_inv, idx_T, idx_R, L_WG, M_WG, N_WG, circ_disk_inv, L_D,
+                      M_D, N_D, L, M, N, idxS3, idx_Sq):
+    """prec_fun_disk_idx.m:1-23: the bus box by the level-1 circulant
+    (chan_mvp), the disk by the level-2 circulant on its square, identity
+    elsewhere."""
+    Jt = np.zeros(3 * L * M * N, dtype=complex)
+    s3 = np.asarray(idxS3, dtype=np.int64) - 1
+    Jt[s3] = J
+    iT = np.asarray(idx_T, dtype=np.int64) - 1
+    iR = np.asarray(idx_R, dtype=np.int64) - 1
+    JT = chan_mvp(circ_WG_inv, Jt[iT], L_WG, M_WG, N_WG)
+    JR = chan_2_mvp_for_parallel_idx(circ_disk_inv, Jt[iR], L_D, M_D, N_D, idx_Sq)
+    Jt[iT] = JT
+    Jt[iR] = JR
+    return Jt[s3]
+
+
 def face_from_Mr(Mr):
     """Bragg_MOR_script.m:64-66: face = (m-1)/m with m = real(mean_x(Mr))."""
     L = Mr.shape[0]

@@ -133,6 +133,13 @@ SIGNATURES = [
                                                ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_int, _dp, _dp,
                                                ctypes.POINTER(GmresInfo)]),
+    ("vox_precond_create_box", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_void_p, _dp, _dp, _dp, _dp,
+                                              ctypes.c_double, ctypes.c_double,
+                                              ctypes.POINTER(ctypes.c_void_p)]),
+    ("vox_precond_create_sum", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                              ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     ("vox_lane_create", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                        ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_double, ctypes.c_int,

@@ -55,7 +55,7 @@ struct OpBuffers {
   R out_scale = 1;       // multiplies the matvec output (1 or Gram for the scaled c64 copy)
 };
 
-inline int pad_stride(int n) { return (n % 2 == 0) ? n + 1 : n; }
+__host__ __device__ inline int pad_stride(int n) { return (n % 2 == 0) ? n + 1 : n; }
 
 // Members of a batched operator (independent solves of one shape, launched
 // together): member b's plane scratch and fN follow member 0's at the strides

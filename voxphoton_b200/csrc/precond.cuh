@@ -45,6 +45,36 @@ __host__ __device__ inline long long pc_work_elems(const PcGeom& g) {
   return (long long)g.L * g.n3;
 }
 
+__device__ __forceinline__ float fmaR(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaR(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// acc += a * b and acc -= a * b, complex, as four fused multiply-adds each
+template <typename C>
+__device__ __forceinline__ void cmac(C& acc, C a, C b) {
+  acc.x = fmaR(a.x, b.x, acc.x);
+  acc.x = fmaR(-a.y, b.y, acc.x);
+  acc.y = fmaR(a.x, b.y, acc.y);
+  acc.y = fmaR(a.y, b.x, acc.y);
+}
+template <typename C>
+__device__ __forceinline__ void cmsub(C& acc, C a, C b) {
+  acc.x = fmaR(-a.x, b.x, acc.x);
+  acc.x = fmaR(a.y, b.y, acc.x);
+  acc.y = fmaR(-a.x, b.y, acc.y);
+  acc.y = fmaR(-a.y, b.x, acc.y);
+}
+
+// two adjacent complex values in one access where possible (16-byte aligned)
+__device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  a = make_float2(q.x, q.y);
+  b = make_float2(q.z, q.w);
+}
+__device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b) {
+  a = p[0];
+  b = p[1];
+}
+
 // --------------------------------------------------------------- apply: x-FFT
 template <typename R>
 __global__ void __launch_bounds__(256) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
@@ -135,12 +165,52 @@ __global__ void k_chan(int L, long long V, const double2* __restrict__ G, double
   }
 }
 
-// Dense block of mode i (column-major n3 x n3) from the x-transformed Chan
-// circulants Cf [comp][z][y][x]; B = gram*I - face3 .* circ.
+// Entry (row, col) of the 3MN x 3MN block of x-mode i assembled from the
+// x-transformed Chan circulants Cf [comp][z][y][x] with the reference's
+// toeplitz / cell2mat / triu pattern (level_1_parallel_func_N.m:113-190, the
+// same in level_1_parallel_func.m and level_2_parallel_func.m); row and col
+// index (component, z, y) with y fastest.
+__device__ __forceinline__ double2 circ_entry(const double2* __restrict__ Cf, int L, int M,
+                                              int N, long long V, int i, int row, int col) {
+  const int MN = M * N;
+  const int bp = row / MN, bq = col / MN;
+  const int p = row - bp * MN, q = col - bq * MN;
+  const int yp = p % M, zp = p / M, yq = q % M, zq = q / M;
+  const int dy = yp > yq ? yp - yq : yq - yp;
+  const int dz = zp > zq ? zp - zq : zq - zp;
+  auto C = [&](int comp, int y, int z) -> double2 {
+    return Cf[comp * V + i + (long long)L * (y + (long long)M * z)];
+  };
+  const int b0 = bp < bq ? bp : bq, b1 = bp < bq ? bq : bp;
+  if (b0 == 0 && b1 == 0) return C(0, dy, dz);
+  if (b0 == 0 && b1 == 1) {
+    // toeplitz([-CC(1) CC(2:M)], -CC(1:M)): y > y' -> CC, else -CC
+    const double2 c = C(1, dy, dz);
+    return (yp > yq) ? c : make_double2(-c.x, -c.y);
+  }
+  if (b0 == 0 && b1 == 2) {
+    // -C3 symmetric, then triu antisymmetrised: p<q -> -C3, p>q -> +C3, p==q -> -C3
+    const double2 c = C(2, dy, dz);
+    return (p > q) ? c : make_double2(-c.x, -c.y);
+  }
+  if (b0 == 1 && b1 == 1) return C(3, dy, dz);
+  if (b0 == 1 && b1 == 2) {
+    // toeplitz([C5(1) -C5(2:M)], C5(1:M)) then triu symmetrised:
+    // value of the upper entry (a<=b): y_a > y_b -> -C5, else C5
+    const int a = p < q ? p : q, b = p < q ? q : p;
+    const int ya = a % M, yb = b % M;
+    const double2 c = C(4, dy, dz);
+    return (ya > yb) ? make_double2(-c.x, -c.y) : c;
+  }
+  return C(5, dy, dz);
+}
+
+// Dense block of mode i (column-major, leading dimension ld) from the
+// x-transformed Chan circulants Cf; B = gram*I - face3 .* circ.
 __global__ void k_assemble_blocks(int L, int M, int N, long long V, int i0, int nmodes, int ld,
                                   const double2* __restrict__ Cf, const double* __restrict__ face3,
                                   double gram, double2* __restrict__ B) {
-  const int MN = M * N, n3 = 3 * MN;
+  const int n3 = 3 * M * N;
   const long long per = (long long)n3 * n3;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nmodes * per;
        t += (long long)gridDim.x * blockDim.x) {
@@ -148,43 +218,260 @@ __global__ void k_assemble_blocks(int L, int M, int N, long long V, int i0, int 
     const long long e = t - im * per;
     const int col = (int)(e / n3);
     const int row = (int)(e - (long long)col * n3);
-    const int i = i0 + im;
-    const int bp = row / MN, bq = col / MN;
-    const int p = row - bp * MN, q = col - bq * MN;
-    const int yp = p % M, zp = p / M, yq = q % M, zq = q / M;
-    const int dy = yp > yq ? yp - yq : yq - yp;
-    const int dz = zp > zq ? zp - zq : zq - zp;
-    auto C = [&](int comp, int y, int z) -> double2 {
-      return Cf[comp * V + i + (long long)L * (y + (long long)M * z)];
-    };
-    double2 v;
-    const int b0 = bp < bq ? bp : bq, b1 = bp < bq ? bq : bp;
-    if (b0 == 0 && b1 == 0) {
-      v = C(0, dy, dz);
-    } else if (b0 == 0 && b1 == 1) {
-      // toeplitz([-CC(1) CC(2:M)], -CC(1:M)): y > y' -> CC, else -CC
-      const double2 c = C(1, dy, dz);
-      v = (yp > yq) ? c : make_double2(-c.x, -c.y);
-    } else if (b0 == 0 && b1 == 2) {
-      // -C3 symmetric, then triu antisymmetrised: p<q -> -C3, p>q -> +C3, p==q -> -C3
-      const double2 c = C(2, dy, dz);
-      v = (p > q) ? c : make_double2(-c.x, -c.y);
-    } else if (b0 == 1 && b1 == 1) {
-      v = C(3, dy, dz);
-    } else if (b0 == 1 && b1 == 2) {
-      // toeplitz([C5(1) -C5(2:M)], C5(1:M)) then triu symmetrised:
-      // value of the upper entry (a<=b): y_a > y_b -> -C5, else C5
-      const int a = p < q ? p : q, b = p < q ? q : p;
-      const int ya = a % M, yb = b % M;
-      const double2 c = C(4, dy, dz);
-      v = (ya > yb) ? make_double2(-c.x, -c.y) : c;
-    } else {
-      v = C(5, dy, dz);
-    }
+    const double2 v = circ_entry(Cf, L, M, N, V, i0 + im, row, col);
     const double f = face3[row];
     double2 o = make_double2(-f * v.x, -f * v.y);
     if (row == col) o.x += gram;
     B[(long long)im * ld * ld + (long long)col * ld + row] = o;
+  }
+}
+
+// --------------------------------------------------------- level-2 (build)
+// level_2_parallel_func.m:166-192: for x-mode i and the M x M sub-block (j, k)
+// of its 3MN block (j, k = component * N + z), the T. Chan circulant along y
+// of the sub-block's first column and row, c(y) = ((M-y) col(y) + y row(M-y))/M,
+// diagonalised by an FFT along y: block m of x-mode i is the 3N x 3N matrix
+// with entries fft(c_jk)(m).  One CTA per (j, k, i); output
+// B2[((i*M + m)*n2 + k)*n2 + j] (column-major 3N x 3N blocks, n2 = 3N).
+__global__ void __launch_bounds__(256) k_level2_blocks(int L, int M, int N, long long V,
+                                                       FftPlan py,
+                                                       const double2* __restrict__ tw,
+                                                       const double2* __restrict__ Cf,
+                                                       double2* __restrict__ B2) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int sy = pad_stride(M);
+  double2* a = reinterpret_cast<double2*>(smem_raw);
+  double2* b = a + sy;
+  const int n2 = 3 * N;
+  const int jk = blockIdx.x;
+  const int j = jk % n2, k = jk / n2;
+  const int i = blockIdx.y;
+  for (int y = threadIdx.x; y < M; y += blockDim.x) {
+    const double2 cv = circ_entry(Cf, L, M, N, V, i, j * M + y, k * M);
+    double2 v = cv;
+    if (y > 0) {
+      const double2 rv = circ_entry(Cf, L, M, N, V, i, j * M, k * M + (M - y));
+      const double wa = (double)(M - y) / M, wb = (double)y / M;
+      v = make_double2(wa * cv.x + wb * rv.x, wa * cv.y + wb * rv.y);
+    }
+    a[y] = v;
+  }
+  __syncthreads();
+  double2* res = block_fft(a, b, py, 1, sy, tw, -1);
+  for (int m = threadIdx.x; m < M; m += blockDim.x)
+    B2[(((long long)i * M + m) * n2 + k) * n2 + j] = res[m];
+}
+
+// In-place inverse of n x n column-major matrices (n <= 64), Gauss-Jordan with
+// partial pivoting in shared memory, one CTA per matrix; info[mat] = 1 + the
+// failing column when a pivot is zero.
+__global__ void __launch_bounds__(128) k_small_inv(int n, double2* __restrict__ A,
+                                                   int* __restrict__ info) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* a = reinterpret_cast<double2*>(smem_raw);  // n x 2n, column-major, ld n
+  __shared__ int piv_row;
+  __shared__ double2 pinv;
+  const long long base = (long long)blockIdx.x * n * n;
+  for (int t = threadIdx.x; t < 2 * n * n; t += blockDim.x) {
+    const int c = t / n, r = t - c * n;
+    a[t] = (c < n) ? A[base + t] : make_double2(c - n == r ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  for (int k = 0; k < n; k++) {
+    if (threadIdx.x == 0) {
+      int best = k;
+      double bv = -1.0;
+      for (int r = k; r < n; r++) {
+        const double2 v = a[k * n + r];
+        const double m = fabs(v.x) + fabs(v.y);
+        if (m > bv) {
+          bv = m;
+          best = r;
+        }
+      }
+      piv_row = best;
+      const double2 p = a[k * n + best];
+      const double d = p.x * p.x + p.y * p.y;
+      if (d == 0.0) {
+        if (info) info[blockIdx.x] = k + 1;
+        pinv = make_double2(0.0, 0.0);
+      } else {
+        pinv = make_double2(p.x / d, -p.y / d);
+      }
+    }
+    __syncthreads();
+    const int pr = piv_row;
+    if (pr != k)
+      for (int c = threadIdx.x; c < 2 * n; c += blockDim.x) {
+        const double2 t = a[c * n + k];
+        a[c * n + k] = a[c * n + pr];
+        a[c * n + pr] = t;
+      }
+    __syncthreads();
+    // scale the pivot row
+    for (int c = threadIdx.x; c < 2 * n; c += blockDim.x) {
+      const double2 v = a[c * n + k];
+      a[c * n + k] = make_double2(v.x * pinv.x - v.y * pinv.y, v.x * pinv.y + v.y * pinv.x);
+    }
+    __syncthreads();
+    // eliminate column k from the other rows
+    for (int t = threadIdx.x; t < 2 * n * n; t += blockDim.x) {
+      const int c = t / n, r = t - c * n;
+      if (r == k || c == k) continue;
+      const double2 f = a[k * n + r];
+      const double2 pv = a[c * n + k];
+      a[t] = make_double2(a[t].x - (f.x * pv.x - f.y * pv.y), a[t].y - (f.x * pv.y + f.y * pv.x));
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x)
+      if (r != k) a[k * n + r] = make_double2(0.0, 0.0);
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[base + t] = a[n * n + t];
+}
+
+// ---------------------------------------------------------- level-2 (apply)
+// y-FFT of the lines of the x-transformed work T [member][i][j][y] (j = 3N
+// lines of length M per x-mode), written transposed as U [member][i][m][j].
+// grid (ceil(3N / kL2Lines), L * members).
+constexpr int kL2Lines = 8;
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_l2_yfwd(PcGeom g, FftPlan py, const Cx<R>* __restrict__ tw,
+                                                 const Cx<R>* __restrict__ T, Cx<R>* __restrict__ U,
+                                                 const int* skip, int fs) {
+  using C = Cx<R>;
+  const int n2 = 3 * g.N;
+  const int mb = blockIdx.y / g.L;
+  const int i = blockIdx.y - mb * g.L;
+  if (skip && skip[(long long)mb * fs]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int sy = pad_stride(g.M);
+  C* a = reinterpret_cast<C*>(smem_raw);
+  C* b = a + kL2Lines * sy;
+  const int j0 = blockIdx.x * kL2Lines;
+  const int nl = min(kL2Lines, n2 - j0);
+  const long long plane = (long long)blockIdx.y * g.n3;
+  for (int t = threadIdx.x; t < kL2Lines * g.M; t += blockDim.x) {
+    const int l = t / g.M, y = t - l * g.M;
+    a[l * sy + y] = (l < nl) ? T[plane + (long long)(j0 + l) * g.M + y] : czero<C>();
+  }
+  __syncthreads();
+  C* res = block_fft(a, b, py, kL2Lines, sy, tw, -1);
+  for (int t = threadIdx.x; t < nl * g.M; t += blockDim.x) {
+    const int m = t / nl, l = t - m * nl;
+    U[plane + (long long)m * n2 + j0 + l] = res[l * sy + m];
+  }
+  (void)i;
+}
+
+// Inverse of k_l2_yfwd: U [member][i][m][j] -> T [member][i][j][y], times 1/M.
+template <typename R>
+__global__ void __launch_bounds__(256) k_l2_yinv(PcGeom g, FftPlan py, const Cx<R>* __restrict__ tw,
+                                                 const Cx<R>* __restrict__ U, Cx<R>* __restrict__ T,
+                                                 const int* skip, int fs) {
+  using C = Cx<R>;
+  const int n2 = 3 * g.N;
+  const int mb = blockIdx.y / g.L;
+  if (skip && skip[(long long)mb * fs]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int sy = pad_stride(g.M);
+  C* a = reinterpret_cast<C*>(smem_raw);
+  C* b = a + kL2Lines * sy;
+  const int j0 = blockIdx.x * kL2Lines;
+  const int nl = min(kL2Lines, n2 - j0);
+  const long long plane = (long long)blockIdx.y * g.n3;
+  for (int t = threadIdx.x; t < kL2Lines * g.M; t += blockDim.x) {
+    const int m = t / kL2Lines, l = t - m * kL2Lines;
+    a[l * sy + m] = (l < nl) ? U[plane + (long long)m * n2 + j0 + l] : czero<C>();
+  }
+  __syncthreads();
+  C* res = block_fft(a, b, py, kL2Lines, sy, tw, +1);
+  const R s = (R)(1.0 / g.M);
+  for (int t = threadIdx.x; t < nl * g.M; t += blockDim.x) {
+    const int l = t / g.M, y = t - l * g.M;
+    T[plane + (long long)(j0 + l) * g.M + y] = cscale(res[l * sy + y], s);
+  }
+}
+
+// Per (x-mode, y-mode) 3N x 3N products for km members (P >= km columns, the
+// unused ones zero and not written): Y[mb][i][m] = B2[i][m] X[mb][i][m].
+// One warp per (i, m); lanes take rows, each column summed in k order with
+// fused multiply-adds, so a member's result does not depend on the others.
+// grid (ceil(L*M / 8)), 256 threads, shared memory 8 * 3N * P values.
+template <typename R, int P>
+__global__ void __launch_bounds__(256) k_l2_gemv(PcGeom g, const Cx<R>* __restrict__ B2,
+                                                 const Cx<R>* __restrict__ X, Cx<R>* __restrict__ Y,
+                                                 const int* skip, int fs, int km) {
+  using C = Cx<R>;
+  if (skip) {
+    bool all = true;
+    for (int b = 0; b < km; b++) all = all && skip[(long long)b * fs] != 0;
+    if (all) return;
+  }
+  const int n2 = 3 * g.N;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long im = (long long)blockIdx.x * 8 + warp;  // i * M + m
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* xw = reinterpret_cast<C*>(smem_raw) + (size_t)warp * n2 * P;  // this warp's columns
+  if (im >= (long long)g.L * g.M) return;
+  const long long ws = (long long)g.L * g.n3;  // member stride of the work
+  for (int t = lane; t < n2 * P; t += 32) {
+    const int k = t / P, q = t - k * P;
+    xw[k * P + q] = (q < km) ? X[q * ws + im * n2 + k] : czero<C>();
+  }
+  __syncwarp();
+  const C* Bb = B2 + im * n2 * n2;
+  for (int r0 = 0; r0 < n2; r0 += 32) {
+    const int r = r0 + lane;
+    C acc[P];
+#pragma unroll
+    for (int q = 0; q < P; q++) acc[q] = czero<C>();
+    if (r < n2) {
+      for (int k = 0; k < n2; k++) {
+        const C bv = Bb[(long long)k * n2 + r];
+#pragma unroll
+        for (int q = 0; q < P; q++) cmac(acc[q], bv, xw[k * P + q]);
+      }
+#pragma unroll
+      for (int q = 0; q < P; q++)
+        if (q < km) Y[q * ws + im * n2 + r] = acc[q];
+    }
+  }
+}
+
+// out = in for km members (the identity part of a sum of preconditioners)
+template <typename R>
+__global__ void k_copy_members(long long n, const Cx<R>* __restrict__ in, Cx<R>* __restrict__ out,
+                               const int* skip, long long vs, int fs) {
+  const int mb = blockIdx.y;
+  if (skip && skip[(long long)mb * fs]) return;
+  in += mb * vs;
+  out += mb * vs;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
+// Index map of a box of the grid (all z): sub[c][z][y][x] = the operator's slot
+// of voxel (x0+x, y0+y, z) when mask (Ls*Ms*N, or all) selects it, else -1.
+__global__ void k_vmap_box(int L, int M, int N, int x0, int y0, int Ls, int Ms,
+                           const int* __restrict__ vmap, const unsigned char* __restrict__ mask,
+                           int* __restrict__ sub) {
+  const long long Vs = (long long)Ls * Ms * N;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 3 * Vs;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / Vs);
+    const long long e = t - c * Vs;
+    const int x = (int)(e % Ls);
+    const int y = (int)((e / Ls) % Ms);
+    const int z = (int)(e / ((long long)Ls * Ms));
+    int v = -1;
+    if (!mask || mask[e]) {
+      const long long cell = (long long)(x0 + x) + (long long)L * ((y0 + y) + (long long)M * z);
+      v = vmap[(long long)c * L * M * N + cell];
+    }
+    sub[t] = v;
   }
 }
 
@@ -561,36 +848,6 @@ __device__ __forceinline__ void cp_async_wait_n(int n) {
     case 6: cp_async_wait<6>(); break;
     default: cp_async_wait<7>(); break;
   }
-}
-
-__device__ __forceinline__ float fmaR(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ double fmaR(double a, double b, double c) { return __fma_rn(a, b, c); }
-
-// acc += a * b and acc -= a * b, complex, as four fused multiply-adds each
-template <typename C>
-__device__ __forceinline__ void cmac(C& acc, C a, C b) {
-  acc.x = fmaR(a.x, b.x, acc.x);
-  acc.x = fmaR(-a.y, b.y, acc.x);
-  acc.y = fmaR(a.x, b.y, acc.y);
-  acc.y = fmaR(a.y, b.x, acc.y);
-}
-template <typename C>
-__device__ __forceinline__ void cmsub(C& acc, C a, C b) {
-  acc.x = fmaR(-a.x, b.x, acc.x);
-  acc.x = fmaR(a.y, b.y, acc.x);
-  acc.y = fmaR(-a.x, b.y, acc.y);
-  acc.y = fmaR(-a.y, b.x, acc.y);
-}
-
-// two adjacent complex values in one access where possible (16-byte aligned)
-__device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
-  const float4 q = *reinterpret_cast<const float4*>(p);
-  a = make_float2(q.x, q.y);
-  b = make_float2(q.z, q.w);
-}
-__device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b) {
-  a = p[0];
-  b = p[1];
 }
 
 // t (npad x P, interleaved) <- U^{-1} L^{-1} t for the mode whose tile stream

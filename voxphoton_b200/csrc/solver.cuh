@@ -8,8 +8,14 @@ struct PcFactors;
 
 struct vox_precond_s {
   vox_op_s* op = nullptr;
-  PcGeom g{};
+  int kind = 0;                // 0 per-x-mode blocks (level 1), 1 level 2, 2 sum of parts
+  PcGeom g{};                  // the grid it acts on (the operator's, or a box of it)
+  const int* vmap = nullptr;   // that grid's index map into the operator's vector
   FftPlan pl{};
+  FftPlan ply{};               // level 2: FFT along y
+  double2* twyd = nullptr;     // level 2: y twiddles
+  float2* twyf = nullptr;
+  std::vector<vox_precond_s*> parts;  // sum: the parts (owned)
   double2* Ad = nullptr;       // c128 inverse blocks, Lf blocks of ld x ld (column-major)
   float2* Af = nullptr;        // c64 copy (Gram * inverse, for the A/Gram operator)
   int ld = 0;                  // leading dimension of the blocks (3MN rounded up to 32)
@@ -103,6 +109,45 @@ static vox_status inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStr
   return VOX_OK;
 }
 
+template <typename R> Cx<R>* pc_twy(vox_precond_s* p);
+template <> double2* pc_twy<double>(vox_precond_s* p) { return p->twyd; }
+template <> float2* pc_twy<float>(vox_precond_s* p) { return p->twyf; }
+
+static int l2_cols(int km) {
+  int c = 1;
+  while (c < km) c *= 2;
+  return c;
+}
+
+template <typename R, int P>
+static void launch_l2_gemv(vox_precond_s* p, const Cx<R>* X, Cx<R>* Y, cudaStream_t st,
+                           const int* skip, int fs, int km) {
+  const PcGeom& g = p->g;
+  const long long nb = ((long long)g.L * g.M + 7) / 8;
+  k_l2_gemv<R, P><<<(unsigned)nb, 256, (size_t)8 * 3 * g.N * P * sizeof(Cx<R>), st>>>(
+      g, pc_A<R>(p), X, Y, skip, fs, km);
+}
+
+// Level-2 per-(x, y)-mode products on the x-transformed work T of km members
+// (T is overwritten; the result lands in T2).
+template <typename R>
+static vox_status l2_apply(vox_precond_s* p, Cx<R>* T, Cx<R>* T2, cudaStream_t st,
+                           const int* skip, int fs, int km) {
+  const PcGeom& g = p->g;
+  const size_t ys = (size_t)2 * kL2Lines * pad_stride(g.M) * sizeof(Cx<R>);
+  const dim3 gy((3 * g.N + kL2Lines - 1) / kL2Lines, g.L * km);
+  k_l2_yfwd<R><<<gy, 256, ys, st>>>(g, p->ply, pc_twy<R>(p), T, T2, skip, fs);
+  switch (l2_cols(km)) {
+    case 1: launch_l2_gemv<R, 1>(p, T2, T, st, skip, fs, km); break;
+    case 2: launch_l2_gemv<R, 2>(p, T2, T, st, skip, fs, km); break;
+    case 4: launch_l2_gemv<R, 4>(p, T2, T, st, skip, fs, km); break;
+    default: launch_l2_gemv<R, 8>(p, T2, T, st, skip, fs, km); break;
+  }
+  k_l2_yinv<R><<<gy, 256, ys, st>>>(g, p->ply, pc_twy<R>(p), T, T2, skip, fs);
+  VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
 // out = M^{-1} in (c128) or f_scale * M^{-1} in (c64 copy), for the members
 // of mm (vectors mm.vs apart, skip flags mm.fs apart); mm.m0 selects the
 // first member's work in this handle.
@@ -120,10 +165,22 @@ static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaSt
   const dim3 gx(nb, mm.km);
   Cx<R>* T = pc_T<R>(p, 0) + mm.m0 * pc_work_elems(g);
   Cx<R>* T2 = pc_T<R>(p, 1) + mm.m0 * pc_work_elems(g);
-  k_pc_xfwd<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->op->vmap, T, skip,
+  if (p->kind == 2) {
+    // sum: identity, then each part on its own box of the grid
+    k_copy_members<R><<<dim3(nblk(p->op->g.n), mm.km), 256, 0, st>>>(p->op->g.n, in, out, skip,
+                                                                     mm.vs, mm.fs);
+    for (vox_precond_s* q : p->parts) VOX_TRY(pc_apply<R>(q, in, out, st, skip, mm));
+    VOX_CUDA(cudaGetLastError());
+    return VOX_OK;
+  }
+  k_pc_xfwd<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->vmap, T, skip,
                                                   mm.vs, mm.fs);
-  VOX_TRY(inv_apply<R>(p, T, T2, st, skip, mm.fs, mm.km));
-  k_pc_xinv<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T2, p->op->vmap,
+  if (p->kind == 1) {
+    VOX_TRY(l2_apply<R>(p, T, T2, st, skip, mm.fs, mm.km));
+  } else {
+    VOX_TRY(inv_apply<R>(p, T, T2, st, skip, mm.fs, mm.km));
+  }
+  k_pc_xinv<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T2, p->vmap,
                                                   (R)(1.0 / g.L), out, skip, mm.vs, mm.fs);
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
@@ -136,6 +193,12 @@ static vox_status pc_attrs() {
   VOX_TRY(smem_cap(k_pc_inv_apply<R, 2>));
   VOX_TRY(smem_cap(k_pc_inv_apply<R, 4>));
   VOX_TRY(smem_cap(k_pc_inv_apply<R, 8>));
+  VOX_TRY(smem_cap(k_l2_yfwd<R>));
+  VOX_TRY(smem_cap(k_l2_yinv<R>));
+  VOX_TRY(smem_cap(k_l2_gemv<R, 1>));
+  VOX_TRY(smem_cap(k_l2_gemv<R, 2>));
+  VOX_TRY(smem_cap(k_l2_gemv<R, 4>));
+  VOX_TRY(smem_cap(k_l2_gemv<R, 8>));
   VOX_TRY(smem_cap(k_lu_batched<R>));
   return VOX_OK;
 }
@@ -157,7 +220,13 @@ struct PcFactors {
   double2 *Ad = nullptr, *Dld = nullptr, *Dud = nullptr, *tiles_d = nullptr, *twd = nullptr;
   float2 *Af = nullptr, *Dlf = nullptr, *Duf = nullptr, *tiles_f = nullptr, *twf = nullptr;
   int *piv = nullptr, *perm = nullptr;
+  double2* twyd = nullptr;
+  float2* twyf = nullptr;
+  int* vmap = nullptr;  // a box's own index map
   ~PcFactors() {
+    cudaFree(twyd);
+    cudaFree(twyf);
+    cudaFree(vmap);
     cudaFree(Ad);
     cudaFree(Af);
     cudaFree(piv);
@@ -188,11 +257,16 @@ static void pc_seal(vox_precond_s* p) {
   f->twf = p->twf;
   f->piv = p->piv;
   f->perm = p->perm;
+  f->twyd = p->twyd;
+  f->twyf = p->twyf;
+  if (p->op && p->vmap != p->op->vmap) f->vmap = const_cast<int*>(p->vmap);
   p->factors = std::move(f);
 }
 
 static void pc_free(vox_precond_s* p) {
   if (!p) return;
+  for (vox_precond_s* q : p->parts) pc_free(q);  // a sum owns its parts
+  p->parts.clear();
   if (p->factors) {
     p->factors.reset();  // frees the arrays only if no view still holds them
   } else {  // construction did not complete: the arrays are still this handle's
@@ -209,6 +283,9 @@ static void pc_free(vox_precond_s* p) {
     own.twf = p->twf;
     own.piv = p->piv;
     own.perm = p->perm;
+    own.twyd = p->twyd;
+    own.twyf = p->twyf;
+    if (p->op && p->vmap && p->vmap != p->op->vmap) own.vmap = const_cast<int*>(p->vmap);
   }
   cudaFree(p->Td);
   cudaFree(p->Td2);
@@ -217,14 +294,18 @@ static void pc_free(vox_precond_s* p) {
   delete p;
 }
 
-static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
+// Grid, x-FFT plan, twiddles and work of a preconditioner acting on an
+// L x M x N grid (the operator's, or a box of it with its own index map set
+// by the caller); `lu` adds the checks of the per-x-mode LU build.
+static vox_status pc_common(vox_op_s* op, vox_precond_s* p, int L, int M, int N, bool lu) {
   p->op = op;
+  if (!p->vmap) p->vmap = op->vmap;
   PcGeom& g = p->g;
-  g.L = op->g.L;
-  g.M = op->g.M;
-  g.N = op->g.N;
+  g.L = L;
+  g.M = M;
+  g.N = N;
   g.n3 = 3 * g.M * g.N;
-  g.V = op->g.V;
+  g.V = (long long)L * M * N;
   if (!make_fft_plan(g.L, &p->pl)) {
     set_error("preconditioner: FFT length L has a prime factor above 64");
     return VOX_ERR_UNSUPPORTED;
@@ -238,9 +319,9 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   }
   // the LU panel bound (n3 <= 1760) also keeps the streamed solve's
   // ring + right-hand sides (64 KiB + 32 B * n3) under the cap
-  if ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
-      lu_stream2_smem<double>(lu_npad(g.n3), kInvBuildCols) > (size_t)kSmemCap ||
-      inv_apply_smem<double>(g.n3, 2) > (size_t)kSmemCap) {
+  if (lu && ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
+             lu_stream2_smem<double>(lu_npad(g.n3), kInvBuildCols) > (size_t)kSmemCap ||
+             inv_apply_smem<double>(g.n3, 2) > (size_t)kSmemCap)) {
     set_error("preconditioner: 3*M*N too large for the batched LU panel");
     return VOX_ERR_UNSUPPORTED;
   }
@@ -259,26 +340,19 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p) {
   return VOX_OK;
 }
 
-}  // namespace vox
-
-extern "C" {
-
-vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const double* G_im,
-                                     const double* face3, vox_precond_t* out) {
-  if (!op || !G_re || !face3 || !out) {
-    set_error("vox_precond_create_level1: NULL argument");
-    return VOX_ERR_BAD_ARG;
-  }
-  *out = nullptr;
-  DeviceGuard dg(op->device);
-  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
-  VOX_TRY(pc_common(op, p.get()));
+// Level-1 inverse blocks of the grid of p (pc_common done): per x-mode
+// inv(gram_block*I - face3 .* circ_i(G)) times `scale`, G the L x M x N x 6
+// Toeplitz-like tensor of that grid (level_1_parallel_func_N.m:1-281 +
+// Bragg_MOR_script.m:61-72; with gram_block = 0, face3 = -1 and G = -Mc.*G +
+// Gram*Mr(1) at the origin it is level_1_parallel_func.m:1-255).  Modes L-i
+// reuse block i when the tensor allows it.
+static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector<double2>& G,
+                               const std::vector<double>& face3, double gram_block,
+                               double scale) {
   const PcGeom& g = p->g;
   cudaStream_t st = op->stream;
   const long long V = g.V;
   // Toeplitz -> Chan circulants -> FFT along x
-  std::vector<double2> G(6 * V);
-  for (long long i = 0; i < 6 * V; i++) G[i] = make_double2(G_re[i], G_im ? G_im[i] : 0.0);
   double2 *dG, *dC;
   VOX_TRY(dalloc(&dG, 6 * V));
   std::unique_ptr<double2, decltype(&cudaFree)> gG(dG, cudaFree);
@@ -291,7 +365,7 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   double* dface;
   VOX_TRY(dalloc(&dface, g.n3));
   std::unique_ptr<double, decltype(&cudaFree)> gF(dface, cudaFree);
-  VOX_CUDA(cudaMemcpy(dface, face3, g.n3 * sizeof(double), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpy(dface, face3.data(), g.n3 * sizeof(double), cudaMemcpyHostToDevice));
   // Pairing: the Chan circulants satisfy c[L-j] = s*c[j] (s = -1 for xy, xz),
   // so B_{L-i} = D B_i D exactly when G_xy and G_xz vanish on the x = 0 plane
   // (true of the physical tensor); then only modes 0..L/2 are factored.
@@ -321,7 +395,7 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   VOX_TRY(dalloc(&p->Dld, dsz));
   VOX_TRY(dalloc(&p->Dud, dsz));
   k_assemble_blocks<<<nblk(Lf * per), 256, 0, st>>>(g.L, g.M, g.N, V, 0, Lf, ld, dC, dface,
-                                                     op->gram, p->Ad);
+                                                     gram_block, p->Ad);
   VOX_CUDA(cudaGetLastError());
   int* dinfo;
   VOX_TRY(dalloc(&dinfo, Lf));
@@ -335,7 +409,7 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   VOX_CUDA(cudaStreamSynchronize(st));
   for (int i = 0; i < Lf; i++)
     if (info[i]) {
-      set_error("vox_precond_create_level1: block " + std::to_string(i) + " is singular");
+      set_error("level-1 preconditioner: block " + std::to_string(i) + " is singular");
       return VOX_ERR_BAD_ARG;
     }
   k_lu_perm<<<Lf, 32, 0, st>>>(g.n3, p->piv, p->perm);
@@ -354,6 +428,8 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
       <<<dim3((g.n3 + kInvBuildCols - 1) / kInvBuildCols, Lf), 32 * kRoundTiles,
          lu_stream2_smem<double>(ld, kInvBuildCols), st>>>(g, p->tiles_d, p->perm, ld, p->Ad);
   VOX_CUDA(cudaGetLastError());
+  if (scale != 1.0) k_cast_scale<double><<<nblk(Lf * perp), 256, 0, st>>>(Lf * perp, p->Ad, scale,
+                                                                         p->Ad);
   // c64 copy of Gram * inverse: it preconditions the c64 operator A/Gram
   p->f_scale = op->gram;
   if (op->has_f) {
@@ -368,9 +444,196 @@ vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const doub
   p->tiles_d = nullptr;
   p->Dld = p->Dud = nullptr;
   (void)dsz;
+  p->kind = 0;
+  p->ld = ld;
+  return VOX_OK;
+}
+
+// Level-2 inverse blocks of the grid of p (pc_common done), from
+// A = -Mc.*G + Gram*Mr(1) at the origin (level_2_parallel_func.m:1-193): per
+// x-mode i and y-mode m the 3N x 3N block, inverted, times `scale`.
+static vox_status build_level2(vox_op_s* op, vox_precond_s* p, const std::vector<double2>& A,
+                               double scale) {
+  const PcGeom& g = p->g;
+  cudaStream_t st = op->stream;
+  const long long V = g.V;
+  const int n2 = 3 * g.N;
+  if (n2 > 64) {
+    set_error("level-2 preconditioner: 3N above 64");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  if (!make_fft_plan(g.M, &p->ply)) {
+    set_error("level-2 preconditioner: FFT length M has a prime factor above 64");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  if ((size_t)2 * kL2Lines * pad_stride(g.M) * sizeof(double2) > (size_t)kSmemCap) {
+    set_error("level-2 preconditioner: M too long for the shared-memory FFT");
+    return VOX_ERR_UNSUPPORTED;
+  }
+  std::vector<double2> tw = twiddles(g.M);
+  std::vector<float2> twf(g.M);
+  for (int i = 0; i < g.M; i++) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+  VOX_TRY(dalloc(&p->twyd, g.M));
+  VOX_TRY(dalloc(&p->twyf, g.M));
+  VOX_CUDA(cudaMemcpy(p->twyd, tw.data(), g.M * sizeof(double2), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpy(p->twyf, twf.data(), g.M * sizeof(float2), cudaMemcpyHostToDevice));
+  double2 *dA, *dC;
+  VOX_TRY(dalloc(&dA, 6 * V));
+  std::unique_ptr<double2, decltype(&cudaFree)> gA(dA, cudaFree);
+  VOX_TRY(dalloc(&dC, 6 * V));
+  std::unique_ptr<double2, decltype(&cudaFree)> gC(dC, cudaFree);
+  VOX_CUDA(cudaMemcpy(dA, A.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice));
+  k_chan<<<nblk(6 * V), 256, 0, st>>>(g.L, V, dA, dC);
+  VOX_CUDA(cudaGetLastError());
+  VOX_TRY(fft_axis_d(dC, g.L, g.M, g.N, 1, g.L, (long long)g.L * g.M, V, 6, 0, -1, st));
+  const long long nblocks = (long long)g.L * g.M;
+  const long long tot = nblocks * n2 * n2;
+  VOX_TRY(dalloc(&p->Ad, tot));
+  VOX_TRY(smem_cap(k_level2_blocks));
+  VOX_TRY(smem_cap(k_small_inv));
+  k_level2_blocks<<<dim3(n2 * n2, g.L), 256, (size_t)2 * pad_stride(g.M) * sizeof(double2), st>>>(
+      g.L, g.M, g.N, V, p->ply, p->twyd, dC, p->Ad);
+  VOX_CUDA(cudaGetLastError());
+  int* dinfo;
+  VOX_TRY(dalloc(&dinfo, nblocks));
+  std::unique_ptr<int, decltype(&cudaFree)> gI(dinfo, cudaFree);
+  VOX_CUDA(cudaMemsetAsync(dinfo, 0, nblocks * sizeof(int), st));
+  k_small_inv<<<(unsigned)nblocks, 128, (size_t)2 * n2 * n2 * sizeof(double2), st>>>(n2, p->Ad,
+                                                                                     dinfo);
+  VOX_CUDA(cudaGetLastError());
+  std::vector<int> info(nblocks);
+  VOX_CUDA(cudaMemcpyAsync(info.data(), dinfo, nblocks * sizeof(int), cudaMemcpyDeviceToHost, st));
+  VOX_CUDA(cudaStreamSynchronize(st));
+  for (long long i = 0; i < nblocks; i++)
+    if (info[i]) {
+      set_error("level-2 preconditioner: block " + std::to_string(i) + " is singular");
+      return VOX_ERR_BAD_ARG;
+    }
+  if (scale != 1.0) k_cast_scale<double><<<nblk(tot), 256, 0, st>>>(tot, p->Ad, scale, p->Ad);
+  p->f_scale = op->gram;
+  if (op->has_f) {
+    VOX_TRY(dalloc(&p->Af, tot));
+    k_cast_scale<float><<<nblk(tot), 256, 0, st>>>(tot, p->Ad, op->gram, p->Af);
+  }
+  VOX_CUDA(cudaGetLastError());
+  VOX_CUDA(cudaStreamSynchronize(st));
+  p->kind = 1;
+  p->Lf = g.L;
+  p->paired = 0;
+  p->ld = n2;
+  return VOX_OK;
+}
+
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_precond_create_level1(vox_op_t op, const double* G_re, const double* G_im,
+                                     const double* face3, vox_precond_t* out) {
+  if (!op || !G_re || !face3 || !out) {
+    set_error("vox_precond_create_level1: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  DeviceGuard dg(op->device);
+  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
+  VOX_TRY(pc_common(op, p.get(), op->g.L, op->g.M, op->g.N, true));
+  const long long V = p->g.V;
+  std::vector<double2> G(6 * V);
+  for (long long i = 0; i < 6 * V; i++) G[i] = make_double2(G_re[i], G_im ? G_im[i] : 0.0);
+  std::vector<double> f3(face3, face3 + p->g.n3);
+  VOX_TRY(build_level1(op, p.get(), G, f3, op->gram, 1.0));
   pc_seal(p.get());
   op->pcs.push_back(p.get());
   *out = p.release();
+  return VOX_OK;
+}
+
+vox_status vox_precond_create_box(vox_op_t op, int level, int x0, int y0, int Ls, int Ms,
+                                  const unsigned char* mask, const double* G_re,
+                                  const double* G_im, const double* Mc_re, const double* Mc_im,
+                                  double Mr1, double scale, vox_precond_t* out) {
+  if (!op || !G_re || !Mc_re || !out) {
+    set_error("vox_precond_create_box: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  if (level != 1 && level != 2) {
+    set_error("vox_precond_create_box: level must be 1 or 2");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (Ls < 1 || Ms < 1 || x0 < 0 || y0 < 0 || x0 + Ls > op->g.L || y0 + Ms > op->g.M) {
+    set_error("vox_precond_create_box: the box leaves the operator's grid");
+    return VOX_ERR_BAD_ARG;
+  }
+  DeviceGuard dg(op->device);
+  const int Ns = op->g.N;
+  const long long Vs = (long long)Ls * Ms * Ns;
+  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
+  // the box's own index map into the operator's vector
+  int* vm;
+  VOX_TRY(dalloc(&vm, 3 * Vs));
+  p->vmap = vm;
+  p->op = op;
+  {
+    unsigned char* dmask = nullptr;
+    if (mask) {
+      VOX_TRY(dalloc(&dmask, Vs));
+      VOX_CUDA(cudaMemcpy(dmask, mask, Vs, cudaMemcpyHostToDevice));
+    }
+    k_vmap_box<<<nblk(3 * Vs), 256, 0, op->stream>>>(op->g.L, op->g.M, Ns, x0, y0, Ls, Ms,
+                                                     op->vmap, dmask, vm);
+    VOX_CUDA(cudaGetLastError());
+    VOX_CUDA(cudaStreamSynchronize(op->stream));
+    cudaFree(dmask);
+  }
+  VOX_TRY(pc_common(op, p.get(), Ls, Ms, Ns, level == 1));
+  // A = -Mc .* G, Gram * Mr(1) added at the origin of the diagonal components
+  std::vector<double2> A(6 * Vs);
+  for (int c = 0; c < 6; c++)
+    for (long long e = 0; e < Vs; e++) {
+      const double gr = G_re[c * Vs + e], gi = G_im ? G_im[c * Vs + e] : 0.0;
+      const double mr = Mc_re[e], mi = Mc_im ? Mc_im[e] : 0.0;
+      A[c * Vs + e] = make_double2(-(mr * gr - mi * gi), -(mr * gi + mi * gr));
+    }
+  for (int c : {0, 3, 5}) A[c * Vs].x += op->gram * Mr1;
+  if (level == 1) {
+    std::vector<double> f3(p->g.n3, -1.0);
+    VOX_TRY(build_level1(op, p.get(), A, f3, 0.0, scale));
+  } else {
+    VOX_TRY(build_level2(op, p.get(), A, scale));
+  }
+  pc_seal(p.get());
+  op->pcs.push_back(p.get());
+  *out = p.release();
+  return VOX_OK;
+}
+
+vox_status vox_precond_create_sum(vox_op_t op, const vox_precond_t* parts, int n,
+                                  vox_precond_t* out) {
+  if (!op || !parts || n < 1 || !out) {
+    set_error("vox_precond_create_sum: bad argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  for (int i = 0; i < n; i++)
+    if (!parts[i] || parts[i]->op != op || parts[i]->kind == 2 ||
+        std::find(op->pcs.begin(), op->pcs.end(), parts[i]) == op->pcs.end()) {
+      set_error("vox_precond_create_sum: every part must be a box or level-1 handle of op");
+      return VOX_ERR_BAD_ARG;
+    }
+  vox_precond_s* p = new vox_precond_s();
+  p->op = op;
+  p->kind = 2;
+  p->K = op->K;
+  p->f_scale = op->gram;
+  p->g = parts[0]->g;
+  for (int i = 0; i < n; i++) {
+    p->parts.push_back(parts[i]);
+    op->pcs.erase(std::remove(op->pcs.begin(), op->pcs.end(), parts[i]), op->pcs.end());
+  }
+  op->pcs.push_back(p);
+  *out = p;
   return VOX_OK;
 }
 
@@ -383,7 +646,7 @@ vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const do
   *out = nullptr;
   DeviceGuard dg(op->device);
   std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
-  VOX_TRY(pc_common(op, p.get()));
+  VOX_TRY(pc_common(op, p.get(), op->g.L, op->g.M, op->g.N, true));
   const PcGeom& g = p->g;
   // every mode's block, stored at the padded leading dimension (zeros beyond n3)
   const int ld = p->ld;
@@ -1124,7 +1387,10 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
                                               b.gram, scale, b.out_scale, MV_AN, w.w, nullptr,
                                               w.vs, 0);
   });
-  if (pc) {
+  if (pc && pc->kind != 0) {
+    // level 2 or a sum: the whole apply as one stage
+    out[4] = timeit([&] { pc_apply<R>(pc, w.V, w.t, st, nullptr, wmembers(w, km)); });
+  } else if (pc) {
     const PcGeom& pg = pc->g;
     const int nb = (pg.n3 + pg.ybx - 1) / pg.ybx;
     Cx<R>* T = pc_T<R>(pc, 0);
@@ -1207,6 +1473,39 @@ vox_status vox_op_set_stream(vox_op_t op, void* stream) {
   return VOX_OK;
 }
 
+}  // extern "C"
+
+namespace vox {
+
+// A second handle on src's factors bound to op, with its own work (a sum's
+// parts are shared the same way).
+static vox_status pc_share(vox_precond_s* src, vox_op_s* op, vox_precond_s** out) {
+  *out = nullptr;
+  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
+  *p = *src;  // geometry, plans and factor pointers (shared owner copied)
+  p->op = op;
+  if (src->vmap == src->op->vmap) p->vmap = op->vmap;
+  p->parts.clear();
+  p->Td = p->Td2 = nullptr;
+  p->Tf = p->Tf2 = nullptr;
+  if (src->kind == 2) {
+    p->K = op->K;
+    for (vox_precond_s* q : src->parts) {
+      vox_precond_s* qs;
+      VOX_TRY(pc_share(q, op, &qs));
+      p->parts.push_back(qs);
+    }
+  } else {
+    VOX_TRY(pc_alloc_work(p.get(), op->K));
+  }
+  *out = p.release();
+  return VOX_OK;
+}
+
+}  // namespace vox
+
+extern "C" {
+
 vox_status vox_precond_share(vox_precond_t src, vox_op_t op, vox_precond_t* out) {
   if (!src || !op || !out) {
     set_error("vox_precond_share: NULL argument");
@@ -1220,14 +1519,10 @@ vox_status vox_precond_share(vox_precond_t src, vox_op_t op, vox_precond_t* out)
     return VOX_ERR_BAD_ARG;
   }
   DeviceGuard dg(op->device);
-  std::unique_ptr<vox_precond_s, void (*)(vox_precond_s*)> p(new vox_precond_s(), pc_free);
-  *p = *src;  // geometry, plans and factor pointers (shared owner copied)
-  p->op = op;
-  p->Td = p->Td2 = nullptr;
-  p->Tf = p->Tf2 = nullptr;
-  VOX_TRY(pc_alloc_work(p.get(), op->K));
-  op->pcs.push_back(p.get());
-  *out = p.release();
+  vox_precond_s* p;
+  VOX_TRY(pc_share(src, op, &p));
+  op->pcs.push_back(p);
+  *out = p;
   return VOX_OK;
 }
 
@@ -1235,6 +1530,20 @@ vox_status vox_precond_info(vox_precond_t p, int* n_blocks, int* ld, int* paired
   if (!p) {
     set_error("vox_precond_info: NULL preconditioner");
     return VOX_ERR_BAD_ARG;
+  }
+  if (p->kind == 1) {
+    if (n_blocks) *n_blocks = p->g.L * p->g.M;
+    if (ld) *ld = p->ld;
+    if (paired) *paired = 0;
+    return VOX_OK;
+  }
+  if (p->kind == 2) {
+    int nb = 0;
+    for (vox_precond_s* q : p->parts) nb += q->kind == 1 ? q->g.L * q->g.M : q->Lf;
+    if (n_blocks) *n_blocks = nb;
+    if (ld) *ld = 0;
+    if (paired) *paired = 0;
+    return VOX_OK;
   }
   if (n_blocks) *n_blocks = p->Lf;
   if (ld) *ld = p->ld;

@@ -143,7 +143,55 @@ def microdisk(radius=5e-6, gap=200e-9, bus_width=500e-9, height=220e-9, len_abs=
     ramp = np.where(X >= xr - len_abs, ((X - (xr - len_abs)) / len_abs) ** 2, ramp)
     e2d = np.where(bus, e2d - 1j * abs_im * ramp, e2d)
     e_r = np.repeat(e2d[:, :, None], z.size, axis=2)
-    return Problem("microdisk", res, e_r, (x, y, z), lam0)
+    return Problem("microdisk", res, e_r, (x, y, z), lam0,
+                   {"radius": radius, "gap": gap, "bus_width": bus_width, "ybus": ybus,
+                    "disk_c": disk_c, "len_abs": len_abs})
+
+
+def microdisk_regions(p: Problem):
+    """The preconditioner's sub-domains of the resonator (resonator_MOR_scripts.m:
+    45-56 bus box, 115-124 disk square, 170-186 disk voxels), as 1-based
+    column-major positions in the whole grid (single component; x3 for the
+    three components as the reference's idx_*3):
+
+    * bus: every voxel of the rows (y) of the bus waveguide, L x M_WG x N;
+    * square: the x range |x - x_disk| <= radius and the rows above the bus and
+      the gap, L_D x M_D x N (the level-2 grid);
+    * disk: the disk's voxels in the whole grid, and in the square's grid.
+    """
+    x, y, z = p.centres
+    L, M, N = p.shape
+    mt = p.meta
+    yb = np.flatnonzero(np.abs(y - mt["ybus"]) <= mt["bus_width"] / 2)
+    xs = np.flatnonzero(np.abs(x) <= mt["radius"])
+    ys = np.flatnonzero(y >= mt["ybus"] + mt["bus_width"] / 2 + mt["gap"])
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    disk2 = (X ** 2 + (Y - mt["disk_c"]) ** 2) <= mt["radius"] ** 2
+
+    def positions(xi, yi, mask2=None):
+        g = np.zeros((L, M, N), dtype=bool)
+        sub = np.zeros((L, M), dtype=bool)
+        sub[np.ix_(xi, yi)] = True
+        if mask2 is not None:
+            sub &= mask2
+        g[:, :, :] = sub[:, :, None]
+        return np.flatnonzero(g.reshape(-1, order="F")) + 1
+
+    idx_bus = positions(np.arange(L), yb)
+    idx_square = positions(xs, ys)
+    idx_disk = positions(xs, ys, disk2)
+    sq_mask = disk2[np.ix_(xs, ys)]
+    sq3 = np.repeat(sq_mask[:, :, None], N, axis=2)
+    idx_disk_in_sq = np.flatnonzero(sq3.reshape(-1, order="F")) + 1
+    return {"bus": (int(yb[0]), int(yb.size)), "idx_bus": idx_bus,
+            "square": (int(xs[0]), int(xs.size), int(ys[0]), int(ys.size)),
+            "idx_square": idx_square, "idx_disk": idx_disk, "idx_disk_in_sq": idx_disk_in_sq}
+
+
+def ext3(idx, V):
+    """[idx; V + idx; 2V + idx] (the three Cartesian components)."""
+    idx = np.asarray(idx)
+    return np.concatenate([idx, V + idx, 2 * V + idx])
 
 
 def plane_wave(p: Problem, k_dir=(1.0, 0.0, 0.0), Eo=(0.0, 1.0, 0.0)):

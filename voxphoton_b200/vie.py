@@ -254,6 +254,63 @@ class Preconditioner:
         check(lib().vox_precond_create_blocks(op.handle, dptr(re), dptr(im), ctypes.byref(h)))
         return cls(op, h)
 
+    @classmethod
+    def box(cls, op: Operator, level, x0, y0, Ls, Ms, G_box, Mc_box, Mr1=1.0, mask=None,
+            scale=-1.0):
+        """Level-1 (level_1_parallel_func) or level-2 (level_2_parallel_func)
+        circulant preconditioner on the box x0:x0+Ls, y0:y0+Ms (all z) of op's
+        grid: G_box its Toeplitz tensor, Mc_box its contrast, mask the box
+        voxels it acts on (default: all of op's unknowns in the box); scale -1
+        is the resonator script's negation."""
+        re, im = split(fortran_flat(np.asarray(G_box)))
+        mre, mim = split(fortran_flat(np.asarray(Mc_box)))
+        mk = None
+        if mask is not None:
+            mk = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(-1, order="F"))
+        h = ctypes.c_void_p()
+        check(lib().vox_precond_create_box(
+            op.handle, int(level), int(x0), int(y0), int(Ls), int(Ms),
+            mk.ctypes.data_as(ctypes.c_void_p) if mk is not None else None,
+            dptr(re), dptr(im), dptr(mre), dptr(mim), float(Mr1), float(scale), ctypes.byref(h)))
+        return cls(op, h)
+
+    @classmethod
+    def sum(cls, op: Operator, parts):
+        """prec_fun_disk_idx: each part on its unknowns, identity elsewhere (the
+        parts are owned by the sum from now on)."""
+        arr = (ctypes.c_void_p * len(parts))(*[q.handle for q in parts])
+        h = ctypes.c_void_p()
+        check(lib().vox_precond_create_sum(op.handle, arr, len(parts), ctypes.byref(h)))
+        for q in parts:
+            op._pcs.discard(q)
+            q._h = None
+        return cls(op, h)
+
+    @classmethod
+    def disk(cls, op: Operator, G, p, regions=None):
+        """resonator_MOR_scripts.m:94-198: level 1 on the bus box with the
+        contrast at its centre (Mc_WG(round(L_WG/2),1,1)), level 2 on the disk
+        square with the disk material's contrast ((e_r-1)/e_r, e_r the scalar
+        Si permittivity of the script) acting on the disk's voxels, both
+        inverses negated, identity elsewhere (prec_fun_disk_idx)."""
+        from . import geometry as geo
+        r = regions or geo.microdisk_regions(p)
+        G = np.asarray(G)
+        Mc = p.Mop()
+        L, M, N = p.shape
+        yb0, Mw = r["bus"]
+        Mc_c = Mc[int(np.floor(L / 2 + 0.5)) - 1, yb0, 0]
+        bus = cls.box(op, 1, 0, yb0, L, Mw, G[:L, :Mw, :N, :], np.full((L, Mw, N), Mc_c),
+                      1.0, None, -1.0)
+        x0, Ls, y0, Ms = r["square"]
+        sq = np.zeros(Ls * Ms * N, dtype=bool)
+        sq[r["idx_disk_in_sq"] - 1] = True
+        mask = sq.reshape((Ls, Ms, N), order="F")
+        e_si = geo.EPS_SI / geo.EPS_SIO2
+        disk = cls.box(op, 2, x0, y0, Ls, Ms, G[:Ls, :Ms, :N, :],
+                       np.full((Ls, Ms, N), (e_si - 1) / e_si), 1.0, mask, -1.0)
+        return cls.sum(op, [bus, disk])
+
     @property
     def handle(self):
         return self._h
