@@ -145,3 +145,30 @@ def test_bad_arguments_raise():
         vb.Operator(Mc, 1.0, [1, 1], G=G)       # duplicate position
     with pytest.raises(vb.vie._lib.VoxError):
         vb.Operator(Mc, 1.0, [3 * L * M * N + 1], G=G)
+
+
+def test_matvec_split_planes_for_tall_grids():
+    # 8 x 430 x 11: a padded plane of 3N = 33 rows x Py (864) values exceeds
+    # shared memory in both precisions, so kernel 2 runs in its split form
+    from voxphoton_b200 import geometry as geo
+    rng = np.random.default_rng(11)
+    L, M, N = 8, 430, 11
+    res = 20e-9
+    ko = 2 * np.pi * geo.N_EXT / 1550e-9
+    G = vb.assemble_toeplitz((L, M, N), ko, res)
+    Mc = 0.3 + 0.1j + 0.05 * rng.standard_normal((L, M, N))
+    Mr = 1.0 + 0.1 * rng.standard_normal((L, M, N))
+    keep = rng.random(L * M * N) < 0.7
+    s = np.flatnonzero(keep) + 1
+    V = L * M * N
+    idx = np.concatenate([s, V + s, 2 * V + s])
+    op = vb.Operator(Mc, res ** 3, idx, G=G, Mr=Mr)
+    fN = ov.fN_from_toeplitz(G)
+    for t in ("notransp", "transp"):
+        x = rng.standard_normal(idx.size) + 1j * rng.standard_normal(idx.size)
+        ref = ov.mv_AN_const(x, fN, Mr, Mc, res ** 3, t, idx)
+        y = op.mv_AN(x, t, prec="c128")
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 1e-12
+        y32 = op.mv_AN(x, t, prec="c64")
+        assert np.linalg.norm(y32 - ref) / np.linalg.norm(ref) < 1e-5
+    op.close()

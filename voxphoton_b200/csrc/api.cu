@@ -252,8 +252,19 @@ static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cu
   const Cx<R>* fN = b.fN + mm.m0 * fN_elems(g);
   k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1, skip,
                                             mm.vs, mm.fs);
-  k_plane<R><<<gp, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1, fN, T2, skip,
-                                             mm.fs);
+  if (g.split) {
+    Cx<R>* TY = b.TY + mm.m0 * planey_elems(g);
+    const int rows = 3 * g.N;
+    const dim3 gy(g.Px, (rows + g.ry - 1) / g.ry, mm.km);
+    const dim3 gz(g.Px, (g.Py + g.kcs - 1) / g.kcs, mm.km);
+    const size_t ysm = 2ull * g.ry * g.sy * cs, zsm = 2ull * 3 * g.kcs * g.sz * cs;
+    k_ysplit_fwd<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, T1, TY, skip, mm.fs);
+    k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, fN, TY, skip, mm.fs);
+    k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, TY, T2, skip, mm.fs);
+  } else {
+    k_plane<R><<<gp, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1, fN, T2, skip,
+                                               mm.fs);
+  }
   k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
                                             b.gram, scale, b.out_scale, mode, out, skip, mm.vs,
                                             mm.fs);
@@ -279,6 +290,9 @@ static vox_status set_smem_attrs() {
   VOX_TRY(smem_cap(k_xfwd<R>));
   VOX_TRY(smem_cap(k_xinv<R>));
   VOX_TRY(smem_cap(k_plane<R>));
+  VOX_TRY(smem_cap(k_ysplit_fwd<R>));
+  VOX_TRY(smem_cap(k_zsplit<R>));
+  VOX_TRY(smem_cap(k_ysplit_inv<R>));
   return VOX_OK;
 }
 
@@ -309,7 +323,15 @@ static bool pick_shapes(OpGeom& g, size_t csz) {
     else
       g.kc = (g.kc + 1) / 2;
   }
-  return fits(kSmemCap);
+  g.split = 0;
+  if (fits(kSmemCap)) return true;
+  // the 3N y-transformed rows of a plane do not fit: split kernel 2 in three
+  g.split = 1;
+  const size_t rowb = 2ull * g.sy * csz, colb = 2ull * 3 * g.sz * csz;
+  if (rowb > (size_t)kSmemCap || colb > (size_t)kSmemCap) return false;
+  g.ry = (int)std::max<size_t>(1, std::min<size_t>(rows, kSmemBudget / rowb));
+  g.kcs = (int)std::max<size_t>(1, std::min<size_t>(g.Py, kSmemBudget / colb));
+  return true;
 }
 
 // In-place batched FFT of a 3-D array along one axis (setup path).
@@ -421,6 +443,7 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
   const long long tsz = plane_elems(g);
   VOX_TRY(dalloc(&b.T1, tsz * op->K));
   VOX_TRY(dalloc(&b.T2, tsz * op->K));
+  if (g.split) VOX_TRY(dalloc(&b.TY, planey_elems(g) * op->K));
   VOX_TRY(set_smem_attrs<R>());
   return VOX_OK;
 }
@@ -435,6 +458,7 @@ static void free_bufs(OpBuffers<R>& b) {
   cudaFree(b.twZ);
   cudaFree(b.T1);
   cudaFree(b.T2);
+  cudaFree(b.TY);
   b = OpBuffers<R>();
 }
 
@@ -860,7 +884,7 @@ extern "C" vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, 
   const OpGeom& g = prec == VOX_C128 ? op->d.geo : op->f.geo;
   const size_t cs = prec == VOX_C128 ? sizeof(double2) : sizeof(float2);
   const size_t half = ((size_t)g.Px * 3 * g.N * g.M * cs + 255) / 256 * 256;
-  if (2 * half > kNoAllocScratchBytes) {
+  if (2 * half > kNoAllocScratchBytes || g.split) {
     set_error("vox_mv_AN_noalloc: this operator needs " + std::to_string(2 * half) +
               " bytes of scratch; the fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
               " bytes (use vox_mv_AN_device)");

@@ -36,6 +36,9 @@ struct OpGeom {
   int sy, sz;     // smem strides of y rows / z columns in kernel 2
   int rc, kc;     // rows per chunk / ky columns per chunk in kernel 2
   int sym;        // fN stored as one octant (exact per-axis parity), else full
+  int split;      // kernel 2 split in three (a plane does not fit in shared memory)
+  int ry;         // split: rows per CTA of the y-FFT kernels
+  int kcs;        // split: ky columns per CTA of the z kernel
 };
 
 enum MvMode { MV_AN = 0, MV_AN_T = 1, MV_L = 2 };
@@ -50,6 +53,7 @@ struct OpBuffers {
   Cx<R>* twZ = nullptr;  // Pz
   Cx<R>* T1 = nullptr;
   Cx<R>* T2 = nullptr;
+  Cx<R>* TY = nullptr;   // split kernel 2: [Px][3N][Py] y-transformed planes
   OpGeom geo{};          // sizes and launch shapes for this precision
   R gram = 0;            // Gram in this precision's units
   R out_scale = 1;       // multiplies the matvec output (1 or Gram for the scaled c64 copy)
@@ -63,6 +67,9 @@ __host__ __device__ inline int pad_stride(int n) { return (n % 2 == 0) ? n + 1 :
 // ints apart.  A single-member launch has b = 0 throughout.
 __host__ __device__ inline long long plane_elems(const OpGeom& g) {
   return (long long)g.Px * 3 * g.N * g.M;
+}
+__host__ __device__ inline long long planey_elems(const OpGeom& g) {
+  return (long long)g.Px * 3 * g.N * g.Py;
 }
 __host__ __device__ inline long long fN_elems(const OpGeom& g) {
   if (g.sym) return 6LL * (g.Px / 2 + 1) * (g.Py / 2 + 1) * (g.Pz / 2 + 1);
@@ -237,6 +244,144 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
       tout[(long long)(r0 + r) * g.M + y] = res[(size_t)r * g.sy + y];
     }
     __syncthreads();
+  }
+}
+
+// ------------------------------------------------- kernel 2, split form
+// For planes of 3N rows x Py that do not fit in shared memory, kernel 2's
+// three phases run as three kernels through TY [kx][row][ky] (per member):
+// forward y-FFT of row chunks; per ky chunk the z-FFT, tensor product and
+// inverse z-FFT (in place in TY); inverse y-FFT of row chunks cropped to M.
+template <typename R>
+__global__ void __launch_bounds__(256) k_ysplit_fwd(OpGeom g, FftPlan py,
+                                                    const Cx<R>* __restrict__ twY,
+                                                    const Cx<R>* __restrict__ T1,
+                                                    Cx<R>* __restrict__ TY, const int* skip,
+                                                    int fs) {
+  using C = Cx<R>;
+  const int mb = blockIdx.z;
+  if (skip && skip[(long long)mb * fs]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* wA = reinterpret_cast<C*>(smem_raw);
+  C* wB = wA + (size_t)g.ry * g.sy;
+  const int rows = 3 * g.N;
+  const int kx = blockIdx.x;
+  const int r0 = blockIdx.y * g.ry;
+  const int nr = min(g.ry, rows - r0);
+  const C* tin = T1 + mb * plane_elems(g) + (long long)kx * rows * g.M;
+  C* ty = TY + mb * planey_elems(g) + (long long)kx * rows * g.Py;
+  for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
+    const int r = t / g.Py;
+    const int y = t - r * g.Py;
+    wA[(size_t)r * g.sy + y] = (y < g.M) ? tin[(long long)(r0 + r) * g.M + y] : czero<C>();
+  }
+  __syncthreads();
+  C* res = block_fft(wA, wB, py, nr, g.sy, twY, -1);
+  for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
+    const int r = t / g.Py;
+    const int y = t - r * g.Py;
+    ty[(long long)(r0 + r) * g.Py + y] = res[(size_t)r * g.sy + y];
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_zsplit(OpGeom g, FftPlan pz,
+                                                const Cx<R>* __restrict__ twZ,
+                                                const Cx<R>* __restrict__ fN,
+                                                Cx<R>* __restrict__ TY, const int* skip, int fs) {
+  using C = Cx<R>;
+  const int mb = blockIdx.z;
+  if (skip && skip[(long long)mb * fs]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* wA = reinterpret_cast<C*>(smem_raw);
+  C* wB = wA + (size_t)3 * g.kcs * g.sz;
+  const int kx = blockIdx.x;
+  const int k0 = blockIdx.y * g.kcs;
+  const int nk = min(g.kcs, g.Py - k0);
+  C* ty = TY + mb * planey_elems(g) + (long long)kx * 3 * g.N * g.Py;
+  fN += mb * fN_elems(g);
+  for (int t = threadIdx.x; t < 3 * nk * g.Pz; t += blockDim.x) {
+    const int s = t / g.Pz;
+    const int zz = t - s * g.Pz;
+    const int c = s / nk;
+    const int j = s - c * nk;
+    wA[(size_t)s * g.sz + zz] =
+        (zz < g.N) ? ty[(long long)(c * g.N + zz) * g.Py + k0 + j] : czero<C>();
+  }
+  __syncthreads();
+  C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, twZ, -1);
+  // tensor product (octant storage: see k_plane)
+  const int fx = g.sym && (2 * kx > g.Px);
+  const int hy = g.sym ? g.Py / 2 + 1 : g.Py, hz = g.sym ? g.Pz / 2 + 1 : g.Pz;
+  const C* fplane = fN + (long long)(fx ? g.Px - kx : kx) * hy * hz * 6;
+  for (int t = threadIdx.x; t < nk * g.Pz; t += blockDim.x) {
+    const int j = t / g.Pz;
+    const int kz = t - j * g.Pz;
+    const int ky = k0 + j;
+    const int fy = g.sym && (2 * ky > g.Py);
+    const int fz = g.sym && (2 * kz > g.Pz);
+    const C* f = fplane + ((long long)(fy ? g.Py - ky : ky) * hz + (fz ? g.Pz - kz : kz)) * 6;
+    C f1 = f[1], f2 = f[2], f4 = f[4];
+    const C f0 = f[0], f3 = f[3], f5 = f[5];
+    if (fx ^ fy) f1 = cscale(f1, (R)-1);
+    if (fx ^ fz) f2 = cscale(f2, (R)-1);
+    if (fy ^ fz) f4 = cscale(f4, (R)-1);
+    C* p0 = res + (size_t)(0 * nk + j) * g.sz + kz;
+    C* p1 = res + (size_t)(1 * nk + j) * g.sz + kz;
+    C* p2 = res + (size_t)(2 * nk + j) * g.sz + kz;
+    const C a = *p0, b = *p1, cc = *p2;
+    C o0 = cmul(f0, a), o1 = cmul(f1, a), o2 = cmul(f2, a);
+    cfma(o0, f1, b);
+    cfma(o1, f3, b);
+    cfma(o2, f4, b);
+    cfma(o0, f2, cc);
+    cfma(o1, f4, cc);
+    cfma(o2, f5, cc);
+    *p0 = o0;
+    *p1 = o1;
+    *p2 = o2;
+  }
+  __syncthreads();
+  C* other = (res == wA) ? wB : wA;
+  C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, twZ, +1);
+  for (int t = threadIdx.x; t < 3 * nk * g.N; t += blockDim.x) {
+    const int s = t / g.N;
+    const int zz = t - s * g.N;
+    const int c = s / nk;
+    const int j = s - c * nk;
+    ty[(long long)(c * g.N + zz) * g.Py + k0 + j] = res2[(size_t)s * g.sz + zz];
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_ysplit_inv(OpGeom g, FftPlan py,
+                                                    const Cx<R>* __restrict__ twY,
+                                                    const Cx<R>* __restrict__ TY,
+                                                    Cx<R>* __restrict__ T2, const int* skip,
+                                                    int fs) {
+  using C = Cx<R>;
+  const int mb = blockIdx.z;
+  if (skip && skip[(long long)mb * fs]) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* wA = reinterpret_cast<C*>(smem_raw);
+  C* wB = wA + (size_t)g.ry * g.sy;
+  const int rows = 3 * g.N;
+  const int kx = blockIdx.x;
+  const int r0 = blockIdx.y * g.ry;
+  const int nr = min(g.ry, rows - r0);
+  const C* ty = TY + mb * planey_elems(g) + (long long)kx * rows * g.Py;
+  C* tout = T2 + mb * plane_elems(g) + (long long)kx * rows * g.M;
+  for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
+    const int r = t / g.Py;
+    const int y = t - r * g.Py;
+    wA[(size_t)r * g.sy + y] = ty[(long long)(r0 + r) * g.Py + y];
+  }
+  __syncthreads();
+  C* res = block_fft(wA, wB, py, nr, g.sy, twY, +1);
+  for (int t = threadIdx.x; t < nr * g.M; t += blockDim.x) {
+    const int r = t / g.M;
+    const int y = t - r * g.M;
+    tout[(long long)(r0 + r) * g.M + y] = res[(size_t)r * g.sy + y];
   }
 }
 

@@ -1379,8 +1379,18 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
                                               nullptr, w.vs, 0);
   });
   out[1] = timeit([&] {
-    k_plane<R><<<dim3(g.Px, km), 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, b.T1,
-                                                           b.fN, b.T2, nullptr, 0);
+    if (g.split) {
+      const int rows = 3 * g.N;
+      const dim3 gy(g.Px, (rows + g.ry - 1) / g.ry, km);
+      const dim3 gz(g.Px, (g.Py + g.kcs - 1) / g.kcs, km);
+      const size_t ysm = 2ull * g.ry * g.sy * cs, zsm = 2ull * 3 * g.kcs * g.sz * cs;
+      k_ysplit_fwd<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, b.T1, b.TY, nullptr, 0);
+      k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, b.fN, b.TY, nullptr, 0);
+      k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, b.TY, b.T2, nullptr, 0);
+    } else {
+      k_plane<R><<<dim3(g.Px, km), 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ,
+                                                             b.T1, b.fN, b.T2, nullptr, 0);
+    }
   });
   out[2] = timeit([&] {
     k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, w.V, b.Mr, b.Mc,

@@ -138,7 +138,9 @@ class Family:
 
     def __init__(self, key, problem: geo.Problem, band, nG=5, precond=True, device=0, members=1,
                  G_nodes=None):
-        """G_nodes: the Toeplitz tensors at the nG nodes, if already assembled."""
+        """G_nodes: the Toeplitz tensors at the nG nodes, if already assembled;
+        precond: "level1" (or True) for the level-1 circulant preconditioner,
+        "disk" for the resonator's bus + disk composite, None for none."""
         self.key = key
         self.members = int(members)
         self.p = problem
@@ -157,7 +159,9 @@ class Family:
         self.assembly_s = time.time() - t0
         t0 = time.time()
         self.pc = None
-        if precond:
+        if precond == "disk":
+            self.pc = Preconditioner.disk(self.node_ops[nG // 2], Gc, problem)
+        elif precond:
             self.pc = Preconditioner.level1(self.node_ops[nG // 2], Gc, problem.e_r)
         self.precond_s = time.time() - t0
         self.rhs = _RhsBuilder(problem, self.idx)
