@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vox", choices=["vox", "reference"])
     ap.add_argument("--workload", default="sweep",
-                    help="sweep (default) | bragg20 | bragg20-p<N> | strip | bragg10")
+                    help="sweep (default) | microdisk | mor | bragg20 | bragg20-p<N> | strip | bragg10")
     ap.add_argument("--precond", default="level1", choices=["none", "level1"])
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--restart", type=int, default=50)
@@ -64,6 +64,18 @@ def parse():
                     help="member slots refilled as solves finish, or whole batches")
     ap.add_argument("--sweep-fp64", type=int, default=50,
                     help="requests solved one at a time in plain complex128 for the baseline")
+    ap.add_argument("--disk-restart", type=int, default=128,
+                    help="GMRES restart length of the microdisk workload (the resonator "
+                         "stagnates under GMRES(50))")
+    ap.add_argument("--disk-fp64", type=int, default=3,
+                    help="microdisk wavelengths solved by the plain FP64 drop-in")
+    ap.add_argument("--mor-config", default="bragg20",
+                    help="grating of the reduced-order sweep (bragg20 = 1160 x 30 x 11)")
+    ap.add_argument("--mor-order", type=int, default=5)
+    ap.add_argument("--mor-tol", type=float, default=1e-4,
+                    help="tolerance of the model's solves (the script's 1e-4)")
+    ap.add_argument("--mor-check", type=int, default=5,
+                    help="wavelengths compared against full solves")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not spawn the nvidia-smi clock sampler (profiler runs)")
@@ -562,14 +574,19 @@ def run_microdisk(args, world, rank, local):
     fam.add_slot(torch.cuda.Stream())
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
-    lane_bytes = max(free0 - free1, 1)
+    # the lane's Krylov arenas are allocated at its first solve: count them here
+    # (complex64 basis of restart + 6 columns, complex128 refinement vectors)
+    arena = args.sweep_members * fam.idx.size * ((args.disk_restart + 6) * 8 + 8 * 16)
+    lane_bytes = max(free0 - free1, 1) + arena
     io_bytes = 2 * 16 * steps * fam.idx.size
     nslots = int(max(1, min(args.sweep_slots, 0.6 * (free1 - io_bytes) // lane_bytes)))
     while len(fam.slots) < nslots:
         fam.add_slot(torch.cuda.Stream())
     reqs = [sv.Request(i, "disk", float(l), 0.0) for i, l in enumerate(lams)]
-    srv = sv.SweepServer([fam], sv.ServeConfig(tol=args.tol, side=args.sweep_side,
-                                               maxit_inner=80))
+    R = args.disk_restart
+    maxit = max(2, 1600 // R)
+    srv = sv.SweepServer([fam], sv.ServeConfig(tol=args.tol, side=args.sweep_side, restart=R,
+                                               maxit_inner=maxit))
     srv.prepare_device()
     srv.warm()
     _progress("warm")
@@ -600,7 +617,7 @@ def run_microdisk(args, world, rank, local):
     _progress(f"host-buffer: {wall_h:.2f} s")
     # matvec stages of one lane (all members) against their bytes
     op_m, pc_m = fam.slots[0]
-    stage = op_m.profile_stages(pc_m, prec="c64", restart=50, kgs=20, reps=5)
+    stage = op_m.profile_stages(pc_m, prec="c64", restart=R, kgs=R // 2, reps=3)
     info = op_m.info()
     L, M, N = p.shape
     K = args.sweep_members
@@ -623,9 +640,9 @@ def run_microdisk(args, world, rank, local):
     torch.cuda.empty_cache()
     op1 = vb.Operator(fam.mop, p.Gram, fam.idx, G=fam._Gc, device=local)
     fam.slots = [(op1, fam.pc.share(op1))]
-    srv64 = sv.SweepServer([fam], sv.ServeConfig(tol=args.tol, mode="fp64", maxit_fp64=80))
-    srv64.solve_one(fam, sv.Request(-1, "disk", 1550e-9, 0.0))
-    sub = reqs[::max(1, len(reqs) // max(1, args.sweep_fp64))][:max(1, args.sweep_fp64)]
+    srv64 = sv.SweepServer([fam], sv.ServeConfig(tol=args.tol, mode="fp64", restart=R,
+                                                 maxit_fp64=maxit))
+    sub = reqs[::max(1, len(reqs) // max(1, args.disk_fp64))][:max(1, args.disk_fp64)]
     t64 = time.perf_counter()
     res64 = [srv64.solve_one(fam, r) for r in sub]
     wall64 = time.perf_counter() - t64
@@ -640,7 +657,7 @@ def run_microdisk(args, world, rank, local):
                 "config": {"workload": f"microdisk: Si disk r = 5 um + bus waveguide, "
                                        f"{L}x{M}x{N} at 20 nm, {steps} wavelengths over "
                                        f"1540-1560 nm submitted together",
-                           "n_unknowns": int(n), "tol": args.tol, "restart": 50,
+                           "n_unknowns": int(n), "tol": args.tol, "restart": R,
                            "precond": "bus level 1 + disk level 2 (prec_fun_disk_idx), "
                                       "at band centre",
                            "lanes": nslots, "members_per_lane": K,
@@ -667,9 +684,128 @@ def run_microdisk(args, world, rank, local):
     fam.close()
 
 
+def run_mor(args, world, rank, local):
+    """Reduced-order wavelength sweep of one Bragg grating (Bragg_MOR_script.m:
+    84-142 and example_Bragg_1500nm_to_1600nm.m:85-100): 5 Legendre nodes x
+    order 5 solves at the script's 1e-4, then the reduced solve at every
+    wavelength of the sweep (0.1 nm steps over 1500-1600 nm, as the script's
+    free_wavelength).  One step = one wavelength.  Timed: the whole model
+    build (solves, Arnoldi, basis, projections) plus the projection of every
+    right-hand side, the reduced solves and the lift of every solution, with
+    the right-hand sides resident in HBM."""
+    import torch
+    import voxphoton_b200 as vb
+    from voxphoton_b200 import geometry as geo
+    from voxphoton_b200 import mor
+    from voxphoton_b200 import serving as sv
+    torch.cuda.set_device(local)
+    band = (1500e-9, 1600e-9)
+    steps = args.steps if args.steps else 1001
+    lams = np.linspace(band[0], band[1], steps)
+    p = geo.bragg_config(args.mor_config)
+    t = time.time()
+    fam = sv.Family("mor", p, band, nG=5, precond="level1", device=local)
+    setup_s = time.time() - t
+    _progress(f"setup {setup_s:.1f} s")
+    n = fam.idx.size
+    dev = torch.device("cuda", local)
+    VRHS = torch.empty((5, n), dtype=torch.complex128, device=dev)
+    fam.rhs.fill_device([geo.C0 / l * geo.N_EXT for l in fam.nodes], VRHS)
+    B = torch.empty((steps, n), dtype=torch.complex128, device=dev)
+    fam.rhs.fill_device([geo.C0 / l * geo.N_EXT for l in lams], B)
+    kw = dict(order=args.mor_order, tol=args.mor_tol, restart=args.restart, maxit_inner=40)
+
+    def build():
+        return mor.ReducedModel(fam.node_ops, fam.nodes, fam.mop, p.Gram, fam.idx, fam._Gc,
+                                VRHS, pc=fam.pc, **kw)
+
+    def online(rm):
+        X = torch.empty_like(B)
+        for c0 in range(0, steps, 128):
+            c1 = min(steps, c0 + 128)
+            Xc, _ = rm.solve(lams[c0:c1], B[c0:c1])
+            X[c0:c1].copy_(Xc)
+        return X
+
+    rm = build()                                  # warm-up: graphs, arenas, allocator
+    online(rm)
+    rm.close()
+    torch.cuda.synchronize()
+    clocks = None if args.no_clocks else Clocks(local)
+    if clocks:
+        clocks.start()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    e0.record()
+    rm = build()
+    e1.record()
+    X = online(rm)
+    e2.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    clk = clocks.stop() if clocks else {"sm_mhz": None, "sm_max_mhz": None,
+                                        "reasons": ["not sampled (--no-clocks)"]}
+    build_s = e0.elapsed_time(e1) / 1e3
+    online_s = e1.elapsed_time(e2) / 1e3
+    _progress(f"model of rank {rm.rank} in {build_s:.2f} s, {steps} wavelengths in "
+              f"{online_s * 1e3:.1f} ms")
+    # accuracy: the reduced solutions against full solves at sampled wavelengths
+    op1 = vb.Operator(fam.mop, p.Gram, fam.idx, G=fam._Gc, device=local)
+    pc1 = fam.pc.share(op1)
+    errs, rres = [], []
+    for c in np.linspace(0, steps - 1, args.mor_check).astype(int):
+        op1.interp(fam.node_ops, sv.lagrange_weights(lams[c], fam.nodes))
+        b = B[c].cpu().numpy()
+        xd, info = vb.solve_refined(op1, b, tol=1e-9, L1=pc1, maxit_inner=40)
+        xm = X[c].cpu().numpy()
+        errs.append(float(np.linalg.norm(xm - xd) / np.linalg.norm(xd)))
+        rres.append(float(np.linalg.norm(op1.mv_AN(xm) - b) / np.linalg.norm(b)))
+    pc1.close()
+    op1.close()
+    iters = [i.total_iters for info in rm.infos for i in info]
+    # online HBM bytes: P read twice per 128-wavelength chunk, B read, X written
+    r = rm.rank
+    chunks = (steps + 127) // 128
+    online_bytes = 2 * chunks * r * n * 16 + 2 * steps * n * 16
+    hbm, src = peaks()
+    ach = online_bytes / online_s / 1e9
+    if rank == 0:
+        line = {"metric": "reduced-order sweep: wavelengths/s including the model build",
+                "value": steps / (build_s + online_s), "unit": "wavelengths/s",
+                "n_gpus": world, "steps": steps, "warmup": 1,
+                "ms_per_step": 1e3 * (build_s + online_s) / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128",
+                "data": "synthetic",
+                "config": {"workload": f"MOR sweep of {p.name} {p.shape[0]}x{p.shape[1]}x"
+                                       f"{p.shape[2]} ({args.mor_config}), {steps} wavelengths "
+                                       f"over 1500-1600 nm",
+                           "nG": 5, "order": args.mor_order, "rank": r, "tol": args.mor_tol,
+                           "n_unknowns": int(n), "setup_s": round(setup_s, 1),
+                           "precond": "level1 at band centre, shared by the nodes",
+                           "l2": "inputs larger than L2 (right-hand sides "
+                                 f"{steps * n * 16 / 1e9:.1f} GB)"},
+                "build_s": build_s, "online_ms": online_s * 1e3,
+                "node_solves": len(iters), "mean_iters": float(np.mean(iters)),
+                "accuracy": {"sampled": len(errs), "max_rel_err_vs_full_solve": max(errs),
+                             "max_true_relres": max(rres)},
+                "e2e": {"value": steps / wall, "unit": "wavelengths/s",
+                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                        "note": "host wall clock of the same timed region"},
+                "roofline": {"bound": "hbm", "kernel": "online phase (k_block_dot_partial + "
+                                                       "k_block_update)",
+                             "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                             "traffic": None, "peak_source": src,
+                             "bytes": online_bytes},
+                "cpu_baseline": None, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    rm.close()
+    fam.close()
+
+
 def main():
     args = parse()
-    if args.steps is None and args.workload not in ("sweep", "microdisk"):
+    if args.steps is None and args.workload not in ("sweep", "microdisk", "mor"):
         args.steps = 10
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -679,6 +815,9 @@ def main():
         return
     if args.workload == "microdisk":
         run_microdisk(args, world, rank, local)
+        return
+    if args.workload == "mor":
+        run_mor(args, world, rank, local)
         return
     if args.workload == "sweep":
         if world > 1:

@@ -166,6 +166,28 @@ vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* 
  * so nothing carries over from the previous call. */
 vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, const void* in, void* out,
                              void* stream);
+/* count products of a batched operator in one launch: member m multiplies
+ * in + m*n_idx into out + m*n_idx with its own fN (the reduced-order model's
+ * MVP_A{iG} / MVP_E{iG} at all nodes at once, Bragg_MOR_script.m:39-41,
+ * 78-80, 137-140).  1 <= count <= members. */
+vox_status vox_mv_AN_batch_device(vox_op_t op, int transp, vox_prec prec, int count,
+                                  const void* in, void* out, void* stream);
+
+/* Tall-skinny products of the reduced-order model on interleaved complex128
+ * device blocks, column-major: X is n x a (column stride ldx), Y n x b (ldy),
+ * 1 <= a, b <= 32.
+ *   vox_block_dot:    C = X^H Y (a x b device array, leading dimension a);
+ *                     Vtemp(:,j)'*v, P'*Qtemp{iG}, P'*Vrhs (Bragg_MOR_script.m:
+ *                     114-116, 137-142; example_Bragg_1500nm_to_1600nm.m:97).
+ *                     FP64 sums in a fixed order: repeated calls agree bitwise.
+ *   vox_block_update: Y = beta*Y + X*W, W a x b (device, leading dimension a);
+ *                     v - h*Vtemp(:,j), P*x_temp (example_…:100). Y must not
+ *                     overlap X; beta == 0 does not read Y.
+ * stream is a cudaStream_t (NULL = the default stream). */
+vox_status vox_block_dot(long long n, int a, int b, const void* X, long long ldx, const void* Y,
+                         long long ldy, void* C, void* stream);
+vox_status vox_block_update(long long n, int a, int b, const void* X, long long ldx,
+                            const void* W, double beta, void* Y, long long ldy, void* stream);
 
 /* Level-1 circulant preconditioner (T. Chan circulant along x, per-mode dense
  * blocks inv(Gram*I - diag(face3)*circ_i)); face3 = (m-1)/m with m the x-mean of
@@ -212,6 +234,10 @@ vox_status vox_precond_info(vox_precond_t p, int* n_blocks, int* ld, int* paired
 /* mvp = chan_mvp_idx(inv_blocks, JIn, L, M, N, idx), host buffers of length n_idx. */
 vox_status vox_precond_apply(vox_precond_t p, vox_prec prec, const double* in_re,
                              const double* in_im, double* out_re, double* out_im);
+/* Device variant in complex128: in/out interleaved double2 device vectors of
+ * n_idx; stream is a cudaStream_t (NULL = the operator's).  The building block
+ * of the solvers whose outer loop runs on the host (pgmresDR, bicgstab). */
+vox_status vox_precond_apply_device(vox_precond_t p, const void* in, void* out, void* stream);
 
 /* pgmres(A, b, restart, tol, maxit, L1) / (..., [], [], R1): one precision end to end. */
 vox_status vox_pgmres(vox_op_t op, vox_precond_t pc, int side, vox_prec prec, const double* b_re,

@@ -571,6 +571,207 @@ def pgmres(A, b, restart=None, tol=None, maxit=None, L1=None, L2=None, R1=None, 
 
 
 # --------------------------------------------------------------------------
+# GMRES with deflated restarting (recycled harmonic Ritz subspace)
+# --------------------------------------------------------------------------
+
+def _precond_chain(A, L1, L2, R1, R2):
+    """The operator of one Arnoldi step: L2 L1 A R1 R2 (pgmresDR_iter.m:60-96)."""
+    def op(v):
+        w = _apply(R2, v)
+        w = _apply(R1, w)
+        w = _apply(A, w)
+        w = _apply(L1, w)
+        return _apply(L2, w)
+    return op
+
+
+def pgmresDR_iter(A, r, m, L1, L2, R1, R2, C, tol):
+    """pgmresDR_iter.m:22-142: one cycle of Arnoldi on (I - C C') L A R with
+    one-pass classical Gram-Schmidt (:101-106).  Returns (V, H, B, k, resvec)."""
+    op = _precond_chain(A, L1, L2, R1, R2)
+    n = r.shape[0]
+    V = np.zeros((n, m + 1), dtype=complex)
+    V[:, 0] = r / np.linalg.norm(r)
+    kc = 0 if C is None else C.shape[1]
+    B = np.zeros((kc, m), dtype=complex)
+    H = np.zeros((m + 1, m), dtype=complex)
+    resvec = np.zeros(m)
+    for k in range(1, m + 1):
+        w = op(V[:, k - 1])
+        if kc:
+            B[:, k - 1] = C.conj().T @ w
+            w = w - C @ B[:, k - 1]
+        H[:k, k - 1] = V[:, :k].conj().T @ w
+        w = w - V[:, :k] @ H[:k, k - 1]
+        H[k, k - 1] = np.linalg.norm(w)
+        V[:, k] = w / H[k, k - 1]
+        rhs = np.zeros(k + 1, dtype=complex)
+        rhs[0] = np.linalg.norm(r)
+        y = np.linalg.lstsq(H[:k + 1, :k], rhs, rcond=None)[0]
+        res = rhs - H[:k + 1, :k] @ y
+        resvec[k - 1] = np.linalg.norm(res)
+        if resvec[k - 1] < tol:
+            return V[:, :k + 1], H[:k + 1, :k], B[:, :k], k, resvec[:k]
+    return V, H, B, m, resvec
+
+
+def _sort_eig(vals, vecs):
+    """sortrows([abs(vals) vecs']): ascending magnitude (stable for ties)."""
+    order = np.argsort(np.abs(vals), kind="stable")
+    return vecs[:, order]
+
+
+def getHarmVecs1(m, k, H):
+    """getHarmVecs1.m: the k harmonic Ritz vectors of smallest harmonic Ritz
+    value of the (m+1) x m Hessenberg H."""
+    Hm = H[:m, :]
+    T = np.linalg.solve(Hm.conj().T, np.eye(m))
+    T[:m, :m - 1] = 0
+    T = Hm + H[m, m - 1] ** 2 * T
+    vals, vecs = np.linalg.eig(T)
+    return _sort_eig(vals, vecs)[:, :k]
+
+
+def getHarmVecs2(m, k, H2, V, U, C):
+    """getHarmVecs2.m: harmonic Ritz vectors of the augmented cycle from the
+    generalized problem (H2' W) z = theta (H2' H2) z; the k of largest
+    |theta| (the script's last k after an ascending sort)."""
+    import scipy.linalg
+    Bm = H2.conj().T @ H2
+    W = np.zeros((m + 1, m), dtype=complex)
+    W[:k, :k] = C.conj().T @ U
+    W[k:m + 1, :k] = V.conj().T @ U
+    W[k:m, k:m] = np.eye(m - k)
+    Am = H2.conj().T @ W
+    vals, vecs = scipy.linalg.eig(Am, Bm)
+    return _sort_eig(vals, vecs)[:, m - k:m]
+
+
+def pgmresDR(A, b, restart=None, tol=None, maxit=None, ritz=None, L1=None, L2=None, R1=None,
+             R2=None, x0=None):
+    """pgmresDR.m:73-282.  Returns (x, flag, relres, iter=[p, outit], resvec)."""
+    restart = 50 if restart is None else restart
+    tol = 1e-3 if tol is None else tol
+    maxit = 10 if maxit is None else maxit
+    ritz = min(10, round(restart / 2)) if ritz is None else min(ritz, restart - 1)
+    b = np.asarray(b, dtype=complex)
+    x0 = np.zeros_like(b) if x0 is None else np.asarray(x0, dtype=complex)
+    r = b - _apply(A, x0)
+    bp = b
+    if L1 is not None:
+        r = _apply(L1, r)
+        bp = _apply(L1, bp)
+    if L2 is not None:
+        r = _apply(L2, r)
+        bp = _apply(L2, bp)
+    bnorm = np.linalg.norm(bp)
+    resvec = np.zeros(restart * (maxit + 1) + 1)
+    it = 0
+    outit = 0
+    resvec[it] = np.linalg.norm(r) / bnorm
+    V, H, _, p, rv = pgmresDR_iter(A, r, restart, L1, L2, R1, R2, None, tol * bnorm)
+    resvec[it + 1:it + 1 + p] = rv / bnorm
+    it += p
+    y = np.linalg.lstsq(H, V.conj().T @ r, rcond=None)[0]
+    x = V[:, :p] @ y
+    r = r - V @ (H @ y)
+    U = C = None
+    if resvec[it] > tol:
+        P = getHarmVecs1(p, p - 1 if ritz > p - 1 else ritz, H)
+        U = V[:, :p] @ P
+        Cq, R = np.linalg.qr(H @ P)
+        C = V @ Cq
+        U = np.linalg.solve(R.T, U.T).T                         # U / R
+    while resvec[it] > tol and outit < maxit:
+        outit += 1
+        V, H, B, p, rv = pgmresDR_iter(A, r, restart, L1, L2, R1, R2, C, tol * bnorm)
+        resvec[it + 1:it + 1 + p] = rv / bnorm
+        it += p
+        k = U.shape[1]
+        d = np.linalg.norm(U, axis=0)
+        D = np.diag(1.0 / d)
+        U = U @ D
+        H2 = np.zeros((k + H.shape[0], k + H.shape[1]), dtype=complex)
+        H2[:k, :k] = D
+        H2[:k, k:] = B
+        H2[k:, k:] = H
+        CV = np.concatenate([C, V], axis=1)
+        y = np.linalg.lstsq(H2, CV.conj().T @ r, rcond=None)[0]
+        x = x + np.concatenate([U, V[:, :p]], axis=1) @ y
+        r = r - CV @ (H2 @ y)
+        if resvec[it] > tol:
+            P = getHarmVecs2(p + k, k, H2, V, U, C)
+            U = np.concatenate([U, V[:, :p]], axis=1) @ P
+            Q, R = np.linalg.qr(H2 @ P)
+            C = CV @ Q
+            U = np.linalg.solve(R.T, U.T).T
+    x = _apply(R2, x)
+    x = _apply(R1, x)
+    x = x0 + x
+    resvec = resvec[:it + 1]
+    relres = np.linalg.norm(b - _apply(A, x)) / np.linalg.norm(b)
+    flag = 0 if relres <= tol else 1
+    return x, flag, relres, [p, outit], resvec
+
+
+# --------------------------------------------------------------------------
+# BiCGStab (JVIE_Solver_const.m:470-504 calls MATLAB's built-in bicgstab)
+# --------------------------------------------------------------------------
+
+def bicgstab(A, b, tol=1e-6, maxit=20, M=None, x0=None):
+    """Preconditioned BiCGStab (van der Vorst 1992; the right-preconditioned
+    form of Barrett et al., Templates, 1994, with M applied as M \\ v),
+    the published algorithm behind MATLAB's bicgstab(A, b, tol, maxit, M):
+    the residual is tested after each half step, so iter may end in .5.
+    Returns (x, flag, relres, iter, resvec) with resvec the ||r|| history
+    (one entry per half step).  flag 0 converged, 1 maxit reached, 4 a scalar
+    of the recurrence vanished (breakdown)."""
+    b = np.asarray(b, dtype=complex)
+    x = np.zeros_like(b) if x0 is None else np.asarray(x0, dtype=complex).copy()
+    nb = np.linalg.norm(b)
+    r = b - _apply(A, x) if x0 is not None else b.copy()
+    rt = r.copy()
+    resvec = [np.linalg.norm(r)]
+    if resvec[0] <= tol * nb:
+        return x, 0, resvec[0] / nb, 0.0, np.array(resvec)
+    rho_prev = alpha = omega = 1.0
+    p = v = np.zeros_like(b)
+    for i in range(1, maxit + 1):
+        rho = np.vdot(rt, r)
+        if rho == 0:
+            return x, 4, np.linalg.norm(b - _apply(A, x)) / nb, i - 1.0, np.array(resvec)
+        if i == 1:
+            p = r.copy()
+        else:
+            beta = (rho / rho_prev) * (alpha / omega)
+            p = r + beta * (p - omega * v)
+        ph = _apply(M, p)
+        v = _apply(A, ph)
+        alpha = rho / np.vdot(rt, v)
+        s = r - alpha * v
+        x = x + alpha * ph
+        resvec.append(np.linalg.norm(s))
+        if resvec[-1] <= tol * nb:
+            return x, 0, np.linalg.norm(b - _apply(A, x)) / nb, i - 0.5, np.array(resvec)
+        sh = _apply(M, s)
+        t = _apply(A, sh)
+        tt = np.vdot(t, t)
+        if tt == 0:
+            return x, 4, np.linalg.norm(b - _apply(A, x)) / nb, i - 0.5, np.array(resvec)
+        omega = np.vdot(t, s) / tt
+        x = x + omega * sh
+        r = s - omega * t
+        resvec.append(np.linalg.norm(r))
+        if resvec[-1] <= tol * nb:
+            return x, 0, np.linalg.norm(b - _apply(A, x)) / nb, float(i), np.array(resvec)
+        if omega == 0:
+            return x, 4, np.linalg.norm(b - _apply(A, x)) / nb, float(i), np.array(resvec)
+        rho_prev = rho
+    relres = np.linalg.norm(b - _apply(A, x)) / nb
+    return x, 0 if relres <= tol else 1, relres, float(maxit), np.array(resvec)
+
+
+# --------------------------------------------------------------------------
 # JVIE-II right-hand side (JVIE_Solver_const.m:133-157, 243-251)
 # --------------------------------------------------------------------------
 

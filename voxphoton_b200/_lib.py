@@ -82,6 +82,18 @@ SIGNATURES = [
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     ("vox_mv_AN_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("vox_precond_apply_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p]),
+    ("vox_mv_AN_batch_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p]),
+    ("vox_block_dot", ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
+                                     ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p]),
+    ("vox_block_update", ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
+                                        ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong,
+                                        ctypes.c_void_p]),
     ("vox_precond_create_level1", ctypes.c_int, [ctypes.c_void_p, _dp, _dp, _dp,
                                                  ctypes.POINTER(ctypes.c_void_p)]),
     ("vox_precond_create_blocks", ctypes.c_int, [ctypes.c_void_p, _dp, _dp,

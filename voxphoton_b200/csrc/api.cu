@@ -22,6 +22,7 @@
 #include "krylov.cuh"
 #include "mvp.cuh"
 #include "precond.cuh"
+#include "block.cuh"
 
 namespace vox {
 
@@ -223,9 +224,17 @@ template <> GmresWork<double>& work<double>(vox_op_s* op) { return op->wd; }
 template <> GmresWork<float>& work<float>(vox_op_s* op) { return op->wf; }
 
 static size_t xsmem(const OpGeom& g, size_t csz) { return 2ull * g.ybx * g.sx * csz; }
+// k_plane: the plane's y-transformed rows, two work buffers, the y and z twiddles
 static size_t psmem(const OpGeom& g, size_t csz) {
   const size_t wsize = std::max((size_t)g.rc * g.sy, (size_t)3 * g.kc * g.sz);
-  return ((size_t)3 * g.N * g.sy + 2 * wsize) * csz;
+  return ((size_t)3 * g.N * g.sy + 2 * wsize + g.Py + g.Pz) * csz;
+}
+// split form: ry rows (k_ysplit_*) or 3 kcs columns (k_zsplit), ping-pong, twiddles
+static size_t ysmem(const OpGeom& g, size_t csz) {
+  return (2ull * g.ry * g.sy + g.Py) * csz;
+}
+static size_t zsmem(const OpGeom& g, size_t csz) {
+  return (2ull * 3 * g.kcs * g.sz + g.Pz) * csz;
 }
 
 // Members taking part in one launch: km members starting at m0 (their fN
@@ -257,7 +266,7 @@ static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cu
     const int rows = 3 * g.N;
     const dim3 gy(g.Px, (rows + g.ry - 1) / g.ry, mm.km);
     const dim3 gz(g.Px, (g.Py + g.kcs - 1) / g.kcs, mm.km);
-    const size_t ysm = 2ull * g.ry * g.sy * cs, zsm = 2ull * 3 * g.kcs * g.sz * cs;
+    const size_t ysm = ysmem(g, cs), zsm = zsmem(g, cs);
     k_ysplit_fwd<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, T1, TY, skip, mm.fs);
     k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, fN, TY, skip, mm.fs);
     k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, TY, T2, skip, mm.fs);
@@ -328,9 +337,12 @@ static bool pick_shapes(OpGeom& g, size_t csz) {
   // the 3N y-transformed rows of a plane do not fit: split kernel 2 in three
   g.split = 1;
   const size_t rowb = 2ull * g.sy * csz, colb = 2ull * 3 * g.sz * csz;
-  if (rowb > (size_t)kSmemCap || colb > (size_t)kSmemCap) return false;
-  g.ry = (int)std::max<size_t>(1, std::min<size_t>(rows, kSmemBudget / rowb));
-  g.kcs = (int)std::max<size_t>(1, std::min<size_t>(g.Py, kSmemBudget / colb));
+  const size_t twy = (size_t)g.Py * csz, twz = (size_t)g.Pz * csz;
+  if (rowb + twy > (size_t)kSmemCap || colb + twz > (size_t)kSmemCap) return false;
+  g.ry = (int)std::max<size_t>(
+      1, std::min<size_t>(rows, (kSmemBudget - std::min(kSmemBudget, twy)) / rowb));
+  g.kcs = (int)std::max<size_t>(
+      1, std::min<size_t>(g.Py, (kSmemBudget - std::min(kSmemBudget, twz)) / colb));
   return true;
 }
 
@@ -800,6 +812,64 @@ vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* 
   if (prec == VOX_C128)
     return matvec<double>(op, mode, (const double2*)in, (double2*)out, st, nullptr);
   return matvec<float>(op, mode, (const float2*)in, (float2*)out, st, nullptr);
+}
+
+vox_status vox_mv_AN_batch_device(vox_op_t op, int transp, vox_prec prec, int count,
+                                  const void* in, void* out, void* stream) {
+  if (!op || !in || !out) {
+    set_error("NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (count < 1 || count > op->K) {
+    set_error("count must be 1..members of the operator");
+    return VOX_ERR_BAD_ARG;
+  }
+  VOX_TRY(check_prec(op, prec));
+  DeviceGuard dg(op->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : op->stream;
+  const int mode = transp ? MV_AN_T : MV_AN;
+  Members mm;
+  mm.km = count;
+  mm.vs = op->g.n;
+  if (prec == VOX_C128)
+    return matvec<double>(op, mode, (const double2*)in, (double2*)out, st, nullptr, mm);
+  return matvec<float>(op, mode, (const float2*)in, (float2*)out, st, nullptr, mm);
+}
+
+vox_status vox_block_dot(long long n, int a, int b, const void* X, long long ldx, const void* Y,
+                         long long ldy, void* C, void* stream) {
+  if (!X || !Y || !C || n < 0 || a < 1 || b < 1 || a > kBlkCols || b > kBlkCols ||
+      ldx < n || ldy < n) {
+    set_error("vox_block_dot: bad sizes or NULL block");
+    return VOX_ERR_BAD_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long tiles = (n + kBlkRows - 1) / kBlkRows;
+  const int ctas = (int)std::max<long long>(1, std::min<long long>(kBlkCtas, tiles));
+  double2* partial = nullptr;
+  VOX_TRY(smem_cap(k_block_dot_partial));
+  VOX_CUDA(cudaMallocAsync((void**)&partial, (size_t)ctas * a * b * sizeof(double2), st));
+  k_block_dot_partial<<<ctas, kBlkThreads, block_dot_smem(a, b), st>>>(
+      n, a, b, (const double2*)X, ldx, (const double2*)Y, ldy, partial);
+  k_block_dot_reduce<<<(a * b + 255) / 256, 256, 0, st>>>(a, b, ctas, partial, (double2*)C);
+  const cudaError_t e = cudaGetLastError();
+  VOX_CUDA(cudaFreeAsync(partial, st));
+  VOX_CUDA(e);
+  return VOX_OK;
+}
+
+vox_status vox_block_update(long long n, int a, int b, const void* X, long long ldx,
+                            const void* W, double beta, void* Y, long long ldy, void* stream) {
+  if (!X || !W || !Y || n < 0 || a < 1 || b < 1 || a > kBlkCols || b > kBlkCols ||
+      ldx < n || ldy < n) {
+    set_error("vox_block_update: bad sizes or NULL block");
+    return VOX_ERR_BAD_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  k_block_update<<<nblk(n, kBlkThreads), kBlkThreads, 0, st>>>(
+      n, a, b, (const double2*)X, ldx, (const double2*)W, beta, (double2*)Y, ldy);
+  VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
 }
 
 }  // extern "C"

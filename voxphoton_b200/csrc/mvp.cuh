@@ -146,6 +146,11 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
   C* wA = ybuf + (size_t)rows * g.sy;
   const int wsize = max(g.rc * g.sy, 3 * g.kc * g.sz);
   C* wB = wA + wsize;
+  // the y and z twiddle tables, read by every butterfly, from shared memory
+  C* tys = wB + wsize;
+  C* tzs = tys + g.Py;
+  for (int t = threadIdx.x; t < g.Py; t += blockDim.x) tys[t] = twY[t];
+  for (int t = threadIdx.x; t < g.Pz; t += blockDim.x) tzs[t] = twZ[t];
   const int kx = blockIdx.x;
   const C* tin = T1 + (long long)kx * rows * g.M;
   C* tout = T2 + (long long)kx * rows * g.M;
@@ -159,7 +164,7 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
       wA[(size_t)r * g.sy + y] = (y < g.M) ? tin[(long long)(r0 + r) * g.M + y] : czero<C>();
     }
     __syncthreads();
-    C* res = block_fft(wA, wB, py, nr, g.sy, twY, -1);
+    C* res = block_fft(wA, wB, py, nr, g.sy, tys, -1);
     for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
       const int r = t / g.Py;
       const int y = t - r * g.Py;
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
           (zz < g.N) ? ybuf[(size_t)(c * g.N + zz) * g.sy + k0 + j] : czero<C>();
     }
     __syncthreads();
-    C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, twZ, -1);
+    C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, tzs, -1);
     // tensor product (in place in res)
     for (int t = threadIdx.x; t < nk * g.Pz; t += blockDim.x) {
       const int j = t / g.Pz;
@@ -217,7 +222,7 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
     }
     __syncthreads();
     C* other = (res == wA) ? wB : wA;
-    C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, twZ, +1);
+    C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, tzs, +1);
     for (int t = threadIdx.x; t < 3 * nk * g.N; t += blockDim.x) {
       const int s = t / g.N;
       const int zz = t - s * g.N;
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
       wA[(size_t)r * g.sy + y] = ybuf[(size_t)(r0 + r) * g.sy + y];
     }
     __syncthreads();
-    C* res = block_fft(wA, wB, py, nr, g.sy, twY, +1);
+    C* res = block_fft(wA, wB, py, nr, g.sy, tys, +1);
     for (int t = threadIdx.x; t < nr * g.M; t += blockDim.x) {
       const int r = t / g.M;
       const int y = t - r * g.M;
@@ -264,6 +269,8 @@ __global__ void __launch_bounds__(256) k_ysplit_fwd(OpGeom g, FftPlan py,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* wA = reinterpret_cast<C*>(smem_raw);
   C* wB = wA + (size_t)g.ry * g.sy;
+  C* tys = wB + (size_t)g.ry * g.sy;
+  for (int t = threadIdx.x; t < g.Py; t += blockDim.x) tys[t] = twY[t];
   const int rows = 3 * g.N;
   const int kx = blockIdx.x;
   const int r0 = blockIdx.y * g.ry;
@@ -276,7 +283,7 @@ __global__ void __launch_bounds__(256) k_ysplit_fwd(OpGeom g, FftPlan py,
     wA[(size_t)r * g.sy + y] = (y < g.M) ? tin[(long long)(r0 + r) * g.M + y] : czero<C>();
   }
   __syncthreads();
-  C* res = block_fft(wA, wB, py, nr, g.sy, twY, -1);
+  C* res = block_fft(wA, wB, py, nr, g.sy, tys, -1);
   for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
     const int r = t / g.Py;
     const int y = t - r * g.Py;
@@ -295,6 +302,8 @@ __global__ void __launch_bounds__(256) k_zsplit(OpGeom g, FftPlan pz,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* wA = reinterpret_cast<C*>(smem_raw);
   C* wB = wA + (size_t)3 * g.kcs * g.sz;
+  C* tzs = wB + (size_t)3 * g.kcs * g.sz;
+  for (int t = threadIdx.x; t < g.Pz; t += blockDim.x) tzs[t] = twZ[t];
   const int kx = blockIdx.x;
   const int k0 = blockIdx.y * g.kcs;
   const int nk = min(g.kcs, g.Py - k0);
@@ -309,7 +318,7 @@ __global__ void __launch_bounds__(256) k_zsplit(OpGeom g, FftPlan pz,
         (zz < g.N) ? ty[(long long)(c * g.N + zz) * g.Py + k0 + j] : czero<C>();
   }
   __syncthreads();
-  C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, twZ, -1);
+  C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, tzs, -1);
   // tensor product (octant storage: see k_plane)
   const int fx = g.sym && (2 * kx > g.Px);
   const int hy = g.sym ? g.Py / 2 + 1 : g.Py, hz = g.sym ? g.Pz / 2 + 1 : g.Pz;
@@ -343,7 +352,7 @@ __global__ void __launch_bounds__(256) k_zsplit(OpGeom g, FftPlan pz,
   }
   __syncthreads();
   C* other = (res == wA) ? wB : wA;
-  C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, twZ, +1);
+  C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, tzs, +1);
   for (int t = threadIdx.x; t < 3 * nk * g.N; t += blockDim.x) {
     const int s = t / g.N;
     const int zz = t - s * g.N;
@@ -365,6 +374,8 @@ __global__ void __launch_bounds__(256) k_ysplit_inv(OpGeom g, FftPlan py,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* wA = reinterpret_cast<C*>(smem_raw);
   C* wB = wA + (size_t)g.ry * g.sy;
+  C* tys = wB + (size_t)g.ry * g.sy;
+  for (int t = threadIdx.x; t < g.Py; t += blockDim.x) tys[t] = twY[t];
   const int rows = 3 * g.N;
   const int kx = blockIdx.x;
   const int r0 = blockIdx.y * g.ry;
@@ -377,7 +388,7 @@ __global__ void __launch_bounds__(256) k_ysplit_inv(OpGeom g, FftPlan py,
     wA[(size_t)r * g.sy + y] = ty[(long long)(r0 + r) * g.Py + y];
   }
   __syncthreads();
-  C* res = block_fft(wA, wB, py, nr, g.sy, twY, +1);
+  C* res = block_fft(wA, wB, py, nr, g.sy, tys, +1);
   for (int t = threadIdx.x; t < nr * g.M; t += blockDim.x) {
     const int r = t / g.M;
     const int y = t - r * g.M;

@@ -742,6 +742,18 @@ vox_status vox_precond_apply(vox_precond_t p, vox_prec prec, const double* in_re
   return VOX_OK;
 }
 
+vox_status vox_precond_apply_device(vox_precond_t p, const void* in, void* out, void* stream) {
+  if (!p || !in || !out) {
+    set_error("vox_precond_apply_device: NULL argument");
+    return VOX_ERR_BAD_ARG;
+  }
+  vox_op_s* op = p->op;
+  VOX_TRY(check_prec(op, VOX_C128));
+  DeviceGuard dg(op->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : op->stream;
+  return pc_apply<double>(p, (const double2*)in, (double2*)out, st, nullptr);
+}
+
 }  // extern "C"
 
 namespace vox {
@@ -1383,7 +1395,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
       const int rows = 3 * g.N;
       const dim3 gy(g.Px, (rows + g.ry - 1) / g.ry, km);
       const dim3 gz(g.Px, (g.Py + g.kcs - 1) / g.kcs, km);
-      const size_t ysm = 2ull * g.ry * g.sy * cs, zsm = 2ull * 3 * g.kcs * g.sz * cs;
+      const size_t ysm = ysmem(g, cs), zsm = zsmem(g, cs);
       k_ysplit_fwd<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, b.T1, b.TY, nullptr, 0);
       k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, b.fN, b.TY, nullptr, 0);
       k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, b.TY, b.T2, nullptr, 0);

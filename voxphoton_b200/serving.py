@@ -132,6 +132,24 @@ class _RhsBuilder:
         omega = 2 * np.pi * freq
         return 1j * omega * geo.EPS0 * self.coef * fx[self.xi]
 
+    def fill_device(self, freqs, out):
+        """The right-hand sides at every frequency of freqs into the rows of
+        out, a (len(freqs), n) complex128 CUDA tensor (synthetic input built
+        in place, without host copies of n-vectors)."""
+        import torch
+        dev = out.device
+        if getattr(self, "_dev", None) is None or self._dev[0] != dev:
+            self._dev = (dev, torch.from_numpy(self.xi).to(dev),
+                         torch.from_numpy(self.coef.astype(np.complex128)).to(dev))
+        _, xi, coef = self._dev
+        for r, freq in enumerate(freqs):
+            k = 2 * np.pi * freq / geo.C0
+            fx = np.exp(-1j * k * self.x) * (np.exp(-1j * k * self.dx / 2)
+                                             - np.exp(1j * k * self.dx / 2)) / (-1j * k)
+            fx = fx * (1j * 2 * np.pi * freq * geo.EPS0)
+            out[r].copy_(coef * torch.from_numpy(fx).to(dev)[xi])
+        return out
+
 
 class Family:
     """Resident state of one device length."""

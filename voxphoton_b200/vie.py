@@ -81,6 +81,7 @@ class Operator:
         self._keep.append(ia)
         d.precisions = (1 if "c128" in precisions else 0) | (2 if "c64" in precisions else 0)
         d.device = device
+        self.device = int(device)
         h = ctypes.c_void_p()
         if members == 1:
             check(lib().vox_op_create(ctypes.byref(d), ctypes.byref(h)))
