@@ -322,6 +322,13 @@ vox_status vox_jvie_rhs(int L, int M, int N, const double* er_re, const double* 
  * assembly_nop_const(r, ko, dx, 'DEMCEM').  nthreads <= 0 uses all cores. */
 vox_status vox_assemble_toeplitz(int L, int M, int N, double ko, double dx, int nthreads,
                                  double* G_re, double* G_im);
+/* The same tensor with the regular face-pair cubature on the GPU `device`
+ * (one warp per cell and face pair, the host's Gauss rules; the eight near
+ * cells' singular corrections on the host): the device half of
+ * assembly_nop_const.m:44-92 / cubature_nop_const.cpp:8-125.  Agrees with
+ * vox_assemble_toeplitz to rounding; output in the same host arrays. */
+vox_status vox_assemble_toeplitz_device(int L, int M, int N, double ko, double dx, int device,
+                                        double* G_re, double* G_im);
 /* The five singular face-pair integrals (self, edge coplanar/orthogonal,
  * vertex coplanar/orthogonal) of exp(-j ko R)/R over dx-squares: out[10] as
  * re/im pairs in the order ST, EAc, EAo, VAc, VAo. */

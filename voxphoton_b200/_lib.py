@@ -121,6 +121,9 @@ SIGNATURES = [
     ("vox_assemble_toeplitz", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              _dp, _dp]),
+    ("vox_assemble_toeplitz_device", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_double, ctypes.c_double,
+                                                    ctypes.c_int, _dp, _dp]),
     ("vox_singular_integrals", ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                               _dp]),
     ("vox_op_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),

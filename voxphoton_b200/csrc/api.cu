@@ -23,6 +23,7 @@
 #include "mvp.cuh"
 #include "precond.cuh"
 #include "block.cuh"
+#include "cubature.cuh"
 
 namespace vox {
 
@@ -855,6 +856,111 @@ vox_status vox_block_dot(long long n, int a, int b, const void* X, long long ldx
   const cudaError_t e = cudaGetLastError();
   VOX_CUDA(cudaFreeAsync(partial, st));
   VOX_CUDA(e);
+  return VOX_OK;
+}
+
+}  // extern "C"
+
+namespace vox {
+// host parts of the assembly (assembly.cpp)
+void asm_rule(int np, std::vector<double>& w, std::vector<double>& u, std::vector<double>& v);
+void asm_tables(double dx, double p1[6][3], double a[6][3], double b[6][3], double P[6][6][6],
+                int obs[21], int src[21], int fill[15][4]);
+void asm_near_cell(int mx, int my, int mz, const double Ipair[21][2], double ko, double dx,
+                   double G[6][2]);
+}  // namespace vox
+
+extern "C" {
+
+vox_status vox_assemble_toeplitz_device(int L, int M, int N, double ko, double dx, int device,
+                                        double* G_re, double* G_im) {
+  if (L < 2 || M < 2 || N < 2 || !G_re || !G_im || dx <= 0) {
+    set_error("vox_assemble_toeplitz_device: needs L, M, N >= 2 and output buffers");
+    return VOX_ERR_BAD_ARG;
+  }
+  DeviceGuard dg(device);
+  const long long V = (long long)L * M * N;
+  CubGeom g;
+  asm_tables(dx, g.p1, g.a, g.b, g.P, g.obs, g.src, g.fill);
+  // rules: far 4 x 4, medium 10 x 10, near 20 x 20 points per face
+  const int nps[3] = {4, 10, 20};
+  std::vector<double> host;
+  size_t off[3][3];
+  for (int r = 0; r < 3; r++) {
+    std::vector<double> w, u, v;
+    asm_rule(nps[r], w, u, v);
+    off[r][0] = host.size();
+    host.insert(host.end(), w.begin(), w.end());
+    off[r][1] = host.size();
+    host.insert(host.end(), u.begin(), u.end());
+    off[r][2] = host.size();
+    host.insert(host.end(), v.begin(), v.end());
+  }
+  cudaStream_t st;
+  VOX_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct Cleanup {
+    cudaStream_t st;
+    double* rules = nullptr;
+    double2* Ipair = nullptr;
+    double2* G = nullptr;
+    ~Cleanup() {
+      cudaFree(rules);
+      cudaFree(Ipair);
+      cudaFree(G);
+      cudaStreamDestroy(st);
+    }
+  } c{st};
+  VOX_TRY(dalloc(&c.rules, host.size()));
+  VOX_TRY(dalloc(&c.Ipair, (size_t)V * 21));
+  VOX_TRY(dalloc(&c.G, (size_t)V * 6));
+  VOX_CUDA(cudaMemcpyAsync(c.rules, host.data(), host.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, st));
+  CubRules rr;
+  for (int r = 0; r < 3; r++) {
+    rr.w[r] = c.rules + off[r][0];
+    rr.u[r] = c.rules + off[r][1];
+    rr.v[r] = c.rules + off[r][2];
+    rr.np[r] = nps[r] * nps[r];
+  }
+  const long long warps = V * 21;
+  const long long blocks = (warps * 32 + 255) / 256;
+  k_cubature_pairs<<<(unsigned)blocks, 256, 0, st>>>(L, M, N, std::min(5, L), std::min(5, M),
+                                                     std::min(5, N), ko, dx, g, rr, c.Ipair);
+  k_cubature_project<<<nblk(V), 256, 0, st>>>(L, M, N, g, c.Ipair, c.G);
+  VOX_CUDA(cudaGetLastError());
+  std::vector<double2> Gh((size_t)V * 6);
+  VOX_CUDA(cudaMemcpyAsync(Gh.data(), c.G, Gh.size() * sizeof(double2), cudaMemcpyDeviceToHost,
+                           st));
+  // the near cells' pair integrals, for the singular corrections on the host
+  double2 In[8][21];
+  for (int m = 0; m < 8; m++) {
+    const int mx = m & 1, my = (m >> 1) & 1, mz = m >> 2;
+    const long long cell = mx + (long long)L * (my + (long long)M * mz);
+    VOX_CUDA(cudaMemcpyAsync(In[m], c.Ipair + cell * 21, 21 * sizeof(double2),
+                             cudaMemcpyDeviceToHost, st));
+  }
+  VOX_CUDA(cudaStreamSynchronize(st));
+  for (long long i = 0; i < V * 6; i++) {
+    const long long cell = i % V;
+    const int mx = (int)(cell % L), my = (int)((cell / L) % M), mz = (int)(cell / ((long long)L * M));
+    if (mx < 2 && my < 2 && mz < 2) continue;
+    G_re[i] = Gh[i].x;
+    G_im[i] = Gh[i].y;
+  }
+  for (int m = 0; m < 8; m++) {
+    const int mx = m & 1, my = (m >> 1) & 1, mz = m >> 2;
+    const long long cell = mx + (long long)L * (my + (long long)M * mz);
+    double Ip[21][2], Gc[6][2];
+    for (int t = 0; t < 21; t++) {
+      Ip[t][0] = In[m][t].x;
+      Ip[t][1] = In[m][t].y;
+    }
+    asm_near_cell(mx, my, mz, Ip, ko, dx, Gc);
+    for (int k = 0; k < 6; k++) {
+      G_re[cell + V * k] = Gc[k][0];
+      G_im[cell + V * k] = Gc[k][1];
+    }
+  }
   return VOX_OK;
 }
 

@@ -372,6 +372,72 @@ void projection(double P[6][6][6]) {
 
 }  // namespace
 
+// Host parts shared with the device cubature (vox_assemble_toeplitz_device):
+// the quadrature rules, the face geometry and projections, and the near-cell
+// correction, all exactly as the host assembly below uses them.
+namespace vox {
+
+// 2-D rule of np x np points on [0,1]^2 (gauss_2d.m ordering): w, u, v.
+void asm_rule(int np, std::vector<double>& w, std::vector<double>& u, std::vector<double>& v) {
+  const Rule2D r = rule2d(np);
+  w = r.w;
+  u = r.u;
+  v = r.v;
+}
+
+// Face origins and edge vectors of the voxel [0,dx]^3, and P(ii, jj, comp).
+void asm_tables(double dx, double p1[6][3], double a[6][3], double b[6][3], double P[6][6][6],
+                int obs[21], int src[21], int fill[15][4]) {
+  Face F[6];
+  cube_faces(dx, F);
+  for (int k = 0; k < 6; k++)
+    for (int j = 0; j < 3; j++) {
+      p1[k][j] = F[k].p1[j];
+      a[k][j] = F[k].a[j];
+      b[k][j] = F[k].b[j];
+    }
+  projection(P);
+  for (int t = 0; t < 21; t++) {
+    obs[t] = kObs[t];
+    src[t] = kSrc[t];
+  }
+  std::memcpy(fill, kFill, sizeof(kFill));
+}
+
+// G(m) of a near cell (mx, my, mz < 2) from its 21 regular pair integrals
+// (20 x 20 rule, already scaled by dx^4): fill by symmetry, replace the
+// singular entries (nearby_correct.m), project.  G[k] = re/im of component k.
+void asm_near_cell(int mx, int my, int mz, const double Ipair[21][2], double ko, double dx,
+                   double G[6][2]) {
+  const Singular sg = singular_terms(ko, dx, 32);
+  const cd sv[6] = {0.0, sg.ST, sg.EAc, sg.EAo, sg.VAc, sg.VAo};
+  cd I[6][6];
+  for (int t = 0; t < 21; t++) I[kObs[t]][kSrc[t]] = cd(Ipair[t][0], Ipair[t][1]);
+  for (const auto& f : kFill) I[f[0]][f[1]] = I[f[2]][f[3]];
+  int ti = -1;
+  for (int t = 0; t < 8; t++)
+    if (kNear[t].m[0] == mx + 1 && kNear[t].m[1] == my + 1 && kNear[t].m[2] == mz + 1) ti = t;
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++)
+      if (kNearPzero[ti][i][j]) {
+        const int c = kNear[ti].code[i][j];
+        I[i][j] = (c == KEEP || c == ZERO) ? cd(0.0) : sv[c];
+      }
+  double P[6][6][6];
+  projection(P);
+  const double inv4pi = 1.0 / (4.0 * M_PI);
+  for (int k = 0; k < 6; k++) {
+    cd g = 0.0;
+    for (int j = 0; j < 6; j++)
+      for (int i = 0; i < 6; i++) g += I[i][j] * P[i][j][k];
+    g *= inv4pi;
+    G[k][0] = g.real();
+    G[k][1] = g.imag();
+  }
+}
+
+}  // namespace vox
+
 extern "C" {
 
 vox_status vox_singular_integrals(double ko, double dx, int order, double* out) {

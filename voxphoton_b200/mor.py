@@ -29,6 +29,7 @@ below `rank_tol` times the largest (numerically absent from the span).
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
 
 import numpy as np
@@ -82,6 +83,31 @@ def _ptr(t):
 def _stream(t):
     torch = _torch()
     return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+@contextlib.contextmanager
+def device_stream(dev, ops=()):
+    """Run the enclosed torch work and libvox calls in order on one CUDA
+    stream: torch's current stream when it is a created stream, else a new
+    side stream ordered after it (libvox's operators run on non-blocking
+    streams, which the legacy default stream does not order against).  The
+    operators in `ops` are pointed at that stream for the duration."""
+    torch = _torch()
+    cur = torch.cuda.current_stream(dev)
+    s = cur if cur.cuda_stream != 0 else torch.cuda.Stream(device=dev)
+    if s is not cur:
+        s.wait_stream(cur)
+    prev = [getattr(op, "stream_ptr", 0) for op in ops]
+    try:
+        with torch.cuda.stream(s):
+            for op in ops:
+                op.set_stream(s.cuda_stream)
+            yield s
+    finally:
+        for op, p in zip(ops, prev):
+            op.set_stream(p)
+        if s is not cur:
+            cur.wait_stream(s)
 
 
 def _block(t):
@@ -178,6 +204,13 @@ class ReducedModel:
             self.opE.interp(node_ops, lagrange_deriv_weights(self.nodes[i], self.nodes),
                             member=i)                                     # fN_deriv{i}
         self.pc = pc.share(self.opA) if pc is not None else None
+        with device_stream(dev, (self.opA, self.opE)):
+            self._build(VRHS, dev, side, tol, restart, maxit_inner, inner_tol, rank_tol)
+
+    def _build(self, VRHS, dev, side, tol, restart, maxit_inner, inner_tol, rank_tol):
+        torch = _torch()
+        nG = self.nG
+        pc = self.pc
         n = self.opA.n
         self.n = n
         kw = dict(pc=self.pc, side=side if pc is not None else None, tol=tol, restart=restart,
@@ -244,13 +277,8 @@ class ReducedModel:
         return self.opE.handle
 
     def _solve(self, B, X, kw):
-        """The batched refined solve runs on the operator's own stream: order
-        it after (and before) the work queued on torch's stream."""
-        torch = _torch()
-        torch.cuda.synchronize(B.device)
-        info = self.opA.solve_refined_batch_device(B.data_ptr(), X.data_ptr(), self.nG, **kw)
-        torch.cuda.synchronize(B.device)
-        return info
+        """The batched refined solve (on the operators' stream, the build's)."""
+        return self.opA.solve_refined_batch_device(B.data_ptr(), X.data_ptr(), self.nG, **kw)
 
     @staticmethod
     def _orthonormalise(P, rank_tol):
@@ -276,12 +304,13 @@ class ReducedModel:
         lams: Vrhs is (count, n) on the device (or host); returns the lifted
         solutions P x (count, n) on the device and the reduced coefficients."""
         torch = _torch()
-        Vrhs = torch.as_tensor(Vrhs, dtype=torch.complex128).to(self.P.device).contiguous()
-        R = block_dot(self.P, Vrhs).cpu().numpy()          # RHS = P' Vrhs, (r, count)
-        Xt = np.empty_like(R)
-        for c, S in enumerate(np.asarray(lams, dtype=float)):
-            Xt[:, c] = np.linalg.solve(self.reduced_matrix(S), R[:, c])
-        return block_update(self.P, Xt), Xt
+        with device_stream(self.P.device):
+            Vrhs = torch.as_tensor(Vrhs, dtype=torch.complex128).to(self.P.device).contiguous()
+            R = block_dot(self.P, Vrhs).cpu().numpy()          # RHS = P' Vrhs, (r, count)
+            Xt = np.empty_like(R)
+            for c, S in enumerate(np.asarray(lams, dtype=float)):
+                Xt[:, c] = np.linalg.solve(self.reduced_matrix(S), R[:, c])
+            return block_update(self.P, Xt), Xt
 
     def close(self):
         if self.pc is not None:

@@ -19,7 +19,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, lib
-from .mor import _block, _ptr, _stream, block_dot, block_update
+from .mor import _ptr, _stream, block_dot, block_update, device_stream
 
 
 def _torch():
@@ -166,6 +166,12 @@ def pgmresDR(A, b, restart=None, tol=None, maxit=None, ritz=None, L1=None, L2=No
     b and x0 may be host arrays or (n,) complex128 CUDA tensors; x is
     returned as a host array."""
     torch = _torch()
+    with device_stream(torch.device("cuda", A.device), (A,)):
+        return _pgmresDR(A, b, restart, tol, maxit, ritz, L1, L2, R1, R2, x0)
+
+
+def _pgmresDR(A, b, restart, tol, maxit, ritz, L1, L2, R1, R2, x0):
+    torch = _torch()
     restart = 50 if restart is None else int(restart)
     tol = 1e-3 if tol is None else float(tol)
     maxit = 10 if maxit is None else int(maxit)
@@ -248,6 +254,12 @@ def bicgstab(A, b, tol=1e-6, maxit=20, M=None, x0=None):
     Preconditioner handle).  The residual is tested after each half step;
     resvec holds ||r|| per half step; flag 0 converged, 1 maxit reached,
     4 breakdown."""
+    torch = _torch()
+    with device_stream(torch.device("cuda", A.device), (A,)):
+        return _bicgstab(A, b, tol, maxit, M, x0)
+
+
+def _bicgstab(A, b, tol, maxit, M, x0):
     torch = _torch()
     ops = _DeviceOps(A)
     n = ops.n

@@ -150,6 +150,7 @@ class Operator:
     def set_stream(self, stream_ptr):
         """Run on the caller's cudaStream_t (an int handle; 0 restores the op's)."""
         check(lib().vox_op_set_stream(self._h, ctypes.c_void_p(stream_ptr or None)))
+        self.stream_ptr = stream_ptr or 0
 
     def launches(self):
         v = ctypes.c_longlong()
@@ -553,14 +554,20 @@ def jvie_rhs(e_r, Einc, Gram, freq, idx):
     return ore + 1j * oim
 
 
-def assemble_toeplitz(shape3, ko, dx, nthreads=0):
-    """assembly_nop_const(r, ko, dx, 'DEMCEM') on the host (C++): G (L x M x N x 6)."""
+def assemble_toeplitz(shape3, ko, dx, nthreads=0, device=None):
+    """assembly_nop_const(r, ko, dx, 'DEMCEM'): G (L x M x N x 6).  On the host
+    (C++, nthreads) by default; with device=<ordinal> the regular face-pair
+    cubature runs on that GPU (vox_assemble_toeplitz_device)."""
     L, M, N = shape3
     V = L * M * N
     re = np.empty(6 * V)
     im = np.empty(6 * V)
-    check(lib().vox_assemble_toeplitz(L, M, N, float(ko), float(dx), int(nthreads), dptr(re),
-                                      dptr(im)))
+    if device is None:
+        check(lib().vox_assemble_toeplitz(L, M, N, float(ko), float(dx), int(nthreads),
+                                          dptr(re), dptr(im)))
+    else:
+        check(lib().vox_assemble_toeplitz_device(L, M, N, float(ko), float(dx), int(device),
+                                                 dptr(re), dptr(im)))
     return (re + 1j * im).reshape((L, M, N, 6), order="F")
 
 
