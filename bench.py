@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--sweep-slots", type=int, default=4, help="lanes per device length")
     ap.add_argument("--sweep-members", type=int, default=4,
                     help="solves per lane advanced in lockstep (batched operator members)")
-    ap.add_argument("--sweep-side", default="left", choices=["left", "right"],
+    ap.add_argument("--sweep-side", default="right", choices=["left", "right"],
                     help="preconditioning side of the mixed-precision inner solves")
     ap.add_argument("--sweep-batching", default="continuous", choices=["continuous", "lockstep"],
                     help="member slots refilled as solves finish, or whole batches")
@@ -294,34 +294,19 @@ def _progress(msg, _t0=[time.time()]):
     print(f"[bench {time.time() - _t0[0]:7.1f} s] {msg}", file=sys.stderr, flush=True)
 
 
-def _assemble_family_nodes(periods, band, world, rank):
-    """Toeplitz tensors of every (device length, Legendre node) pair.  With
-    several ranks on one box the pairs are split across the ranks (host cores
-    divided between them) and exchanged through a temporary directory, so
-    setup does not grow with the number of ranks."""
+def _assemble_family_nodes(periods, band, device):
+    """Toeplitz tensors of every (device length, Legendre node) pair, the
+    regular cubature on this rank's GPU (vox_assemble_toeplitz_device)."""
     import voxphoton_b200 as vb
     from voxphoton_b200 import geometry as geo
     from voxphoton_b200 import serving as sv
     nodes = sv.legendre_nodes(band[0], band[1], 5)
-    jobs = [(pr, j) for pr in periods for j in range(len(nodes))]
-    ncores = os.cpu_count() or 1
-    if world == 1:
-        out = {}
-        for pr, j in jobs:
+    out = {}
+    for pr in periods:
+        for j in range(len(nodes)):
             q = geo.bragg(periods=pr, M=30).with_wavelength(nodes[j])
-            out[(pr, j)] = vb.assemble_toeplitz(q.shape, q.ko, q.res)
-        return out
-    import torch.distributed as dist
-    holder = [tempfile.mkdtemp(prefix="vox_G_") if rank == 0 else None]
-    dist.broadcast_object_list(holder, src=0)
-    d = holder[0]
-    for i, (pr, j) in enumerate(jobs):
-        if i % world == rank:
-            q = geo.bragg(periods=pr, M=30).with_wavelength(nodes[j])
-            G = vb.assemble_toeplitz(q.shape, q.ko, q.res, nthreads=max(1, ncores // world))
-            np.save(os.path.join(d, f"G_{pr}_{j}.npy"), G)
-    dist.barrier()
-    return {(pr, j): np.load(os.path.join(d, f"G_{pr}_{j}.npy")) for pr, j in jobs}
+            out[(pr, j)] = vb.assemble_toeplitz(q.shape, q.ko, q.res, device=device)
+    return out
 
 
 def run_sweep(args, world, rank, local):
@@ -345,7 +330,7 @@ def run_sweep(args, world, rank, local):
     steps = args.steps if args.steps else 201
     lams = np.linspace(band[0], band[1], steps)
     t = time.time()
-    Gs = _assemble_family_nodes(periods, band, world, rank)
+    Gs = _assemble_family_nodes(periods, band, local)
     fams = [sv.Family(pr, geo.bragg(periods=pr, M=30), band, nG=5, device=local,
                       members=args.sweep_members, G_nodes=[Gs[(pr, j)] for j in range(5)])
             for pr in periods]
@@ -373,7 +358,8 @@ def run_sweep(args, world, rank, local):
             op.set_stream(op.torch_stream.cuda_stream)
     items = [(pr, lam) for lam in lams for pr in periods]
     reqs = sv.poisson_stream(items, rate=args.sweep_rate, seed=args.seed + rank)
-    cfg = sv.ServeConfig(tol=args.tol, side=args.sweep_side, batching=args.sweep_batching)
+    cfg = sv.ServeConfig(tol=args.tol, side=args.sweep_side, batching=args.sweep_batching,
+                         inner_tol=args.inner_tol)
     srv = sv.SweepServer(fams, cfg)
     srv.prepare_device()
     # warm-up: a full batch on every lane (captures the cycle graphs), then W
@@ -586,7 +572,7 @@ def run_microdisk(args, world, rank, local):
     R = args.disk_restart
     maxit = max(2, 1600 // R)
     srv = sv.SweepServer([fam], sv.ServeConfig(tol=args.tol, side=args.sweep_side, restart=R,
-                                               maxit_inner=maxit))
+                                               maxit_inner=maxit, inner_tol=args.inner_tol))
     srv.prepare_device()
     srv.warm()
     _progress("warm")

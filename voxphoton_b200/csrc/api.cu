@@ -307,6 +307,9 @@ static vox_status set_smem_attrs() {
 }
 
 static const size_t kSmemBudget = 110 * 1024;  // two CTAs per SM
+// k_plane in complex64: three CTAs per SM (at most 80 registers a thread, its
+// launch bounds), which measured faster than two CTAs of 110 KB
+static const size_t kPlaneBudget = 72 * 1024;
 
 // Pick launch shapes for precision of size csz; returns false if a plane
 // cannot be staged in shared memory.
@@ -325,7 +328,8 @@ static bool pick_shapes(OpGeom& g, size_t csz) {
   g.rc = rows;
   g.kc = g.Py;
   auto fits = [&](size_t budget) { return psmem(g, csz) <= budget; };
-  while (!fits(kSmemBudget) && (g.kc > 1 || g.rc > 1)) {
+  const size_t pbudget = csz == sizeof(float2) ? kPlaneBudget : kSmemBudget;
+  while (!fits(pbudget) && (g.kc > 1 || g.rc > 1)) {
     if ((size_t)3 * g.kc * g.sz >= (size_t)g.rc * g.sy && g.kc > 1)
       g.kc = (g.kc + 1) / 2;
     else if (g.rc > 1)
@@ -447,7 +451,8 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
     std::vector<Cx<R>> wc(n);
     for (int i = 0; i < n; i++) wc[i] = from_d2<Cx<R>>(w[i]);
     VOX_TRY(dalloc(dst, n));
-    VOX_CUDA(cudaMemcpy(*dst, wc.data(), n * sizeof(Cx<R>), cudaMemcpyHostToDevice));
+    VOX_CUDA(cudaMemcpyAsync(*dst, wc.data(), n * sizeof(Cx<R>), cudaMemcpyHostToDevice,
+                             st));
     return VOX_OK;
   };
   VOX_TRY(up_tw(g.Px, &b.twX));
@@ -601,7 +606,8 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
       vmap[p] = (int)i;
     }
     VOX_TRY(dalloc(&op->vmap, 3 * V));
-    VOX_CUDA(cudaMemcpy(op->vmap, vmap.data(), 3 * V * sizeof(int), cudaMemcpyHostToDevice));
+    VOX_CUDA(cudaMemcpyAsync(op->vmap, vmap.data(), 3 * V * sizeof(int), cudaMemcpyHostToDevice,
+                             st));
   }
   // material arrays
   std::vector<double2> Mr, Mc(V);
@@ -624,7 +630,8 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
       G[i] = make_double2(desc->G_re[i], desc->G_im ? desc->G_im[i] : 0.0);
     double2* dG;
     VOX_TRY(dalloc(&dG, 6 * V));
-    VOX_CUDA(cudaMemcpy(dG, G.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice));
+    VOX_CUDA(cudaMemcpyAsync(dG, G.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice,
+                             st));
     k_embed_from_toeplitz<<<nblk(6 * P), 256, 0, st>>>(g, dG, emb);
     VOX_CUDA(cudaGetLastError());
     VOX_CUDA(cudaStreamSynchronize(st));
@@ -638,7 +645,8 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
     double2* dF;
     VOX_TRY(dalloc(&dF, 6 * Q));
     std::unique_ptr<double2, decltype(&cudaFree)> dF_guard(dF, cudaFree);
-    VOX_CUDA(cudaMemcpy(dF, F.data(), 6 * Q * sizeof(double2), cudaMemcpyHostToDevice));
+    VOX_CUDA(cudaMemcpyAsync(dF, F.data(), 6 * Q * sizeof(double2), cudaMemcpyHostToDevice,
+                             st));
     // inverse 3-D FFT (unscaled) of each component: x stride 1, y 2L, z 4LM
     for (int ax = 0; ax < 3; ax++)
       VOX_TRY(fft_axis_d(dF, L2, M2, N2, 1, L2, (long long)L2 * M2, Q, 6, ax, +1, st));

@@ -113,6 +113,125 @@ __device__ __forceinline__ void reduce_partials(const double2* partial, int nj, 
 // Per-CTA dot products of nj basis vectors with w over the CTA's grid-stride
 // elements, kDotBatch basis vectors per sweep (FP64 accumulation).
 constexpr int kDotBatch = 8;
+
+// acc += conj(v) * w in FP64
+__device__ __forceinline__ void acc_cdot(double2& acc, double vx, double vy, double wx,
+                                         double wy) {
+  acc.x += vx * wx + vy * wy;
+  acc.y += vx * wy - vy * wx;
+}
+
+// The rows of one batch: one row per thread and step (complex128: 16-byte loads).
+template <typename R>
+__device__ __forceinline__ void dots_rows(const Cx<R>* __restrict__ V, long long ldv, int j0,
+                                          int nb, const Cx<R>* __restrict__ w, long long n,
+                                          double2 (&acc)[kDotBatch]) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 wi = to_d2(w[i]);
+#pragma unroll
+    for (int q = 0; q < kDotBatch; q++) {
+      if (q < nb) {
+        const double2 v = to_d2(V[(j0 + q) * ldv + i]);
+        acc_cdot(acc[q], v.x, v.y, wi.x, wi.y);
+      }
+    }
+  }
+}
+
+// complex64: two rows per thread and step, 16-byte loads (the basis columns
+// and w start on 256-byte boundaries of the Krylov arena); an odd last row
+// goes to thread 0 of CTA 0.
+template <>
+__device__ __forceinline__ void dots_rows<float>(const float2* __restrict__ V, long long ldv,
+                                                 int j0, int nb, const float2* __restrict__ w,
+                                                 long long n, double2 (&acc)[kDotBatch]) {
+  const long long n2 = n >> 1;
+  const float4* __restrict__ w4 = reinterpret_cast<const float4*>(w);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float4 wv = w4[i];
+#pragma unroll
+    for (int q = 0; q < kDotBatch; q++) {
+      if (q < nb) {
+        const float4 v = reinterpret_cast<const float4*>(V + (j0 + q) * ldv)[i];
+        acc_cdot(acc[q], v.x, v.y, wv.x, wv.y);
+        acc_cdot(acc[q], v.z, v.w, wv.z, wv.w);
+      }
+    }
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const float2 wi = w[n - 1];
+#pragma unroll
+    for (int q = 0; q < kDotBatch; q++) {
+      if (q < nb) {
+        const float2 v = V[(j0 + q) * ldv + n - 1];
+        acc_cdot(acc[q], v.x, v.y, wi.x, wi.y);
+      }
+    }
+  }
+}
+
+// w <- w - V h over this thread's rows (the rows dots_rows<R> gives it, so a
+// kernel may update and then take dots without a grid-wide barrier); returns
+// the sum of |w_i|^2 over those rows in FP64.
+template <typename R>
+__device__ __forceinline__ double update_rows(const Cx<R>* __restrict__ V, long long ldv, int nj,
+                                              const Cx<R>* hs, Cx<R>* w, long long n) {
+  double nrm = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    Cx<R> wi = w[i];
+#pragma unroll 4
+    for (int j = 0; j < nj; j++) {
+      const Cx<R> v = V[j * ldv + i];
+      const Cx<R> h = hs[j];
+      wi.x -= v.x * h.x - v.y * h.y;
+      wi.y -= v.x * h.y + v.y * h.x;
+    }
+    w[i] = wi;
+    nrm += (double)wi.x * wi.x + (double)wi.y * wi.y;
+  }
+  return nrm;
+}
+
+template <>
+__device__ __forceinline__ double update_rows<float>(const float2* __restrict__ V, long long ldv,
+                                                     int nj, const float2* hs, float2* w,
+                                                     long long n) {
+  double nrm = 0.0;
+  const long long n2 = n >> 1;
+  float4* w4 = reinterpret_cast<float4*>(w);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2;
+       i += (long long)gridDim.x * blockDim.x) {
+    float4 wv = w4[i];
+#pragma unroll 4
+    for (int j = 0; j < nj; j++) {
+      const float4 v = reinterpret_cast<const float4*>(V + j * ldv)[i];
+      const float2 h = hs[j];
+      wv.x -= v.x * h.x - v.y * h.y;
+      wv.y -= v.x * h.y + v.y * h.x;
+      wv.z -= v.z * h.x - v.w * h.y;
+      wv.w -= v.z * h.y + v.w * h.x;
+    }
+    w4[i] = wv;
+    nrm += (double)wv.x * wv.x + (double)wv.y * wv.y;
+    nrm += (double)wv.z * wv.z + (double)wv.w * wv.w;
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    float2 wi = w[n - 1];
+    for (int j = 0; j < nj; j++) {
+      const float2 v = V[j * ldv + n - 1];
+      const float2 h = hs[j];
+      wi.x -= v.x * h.x - v.y * h.y;
+      wi.y -= v.x * h.y + v.y * h.x;
+    }
+    w[n - 1] = wi;
+    nrm += (double)wi.x * wi.x + (double)wi.y * wi.y;
+  }
+  return nrm;
+}
+
 template <typename R>
 __device__ __forceinline__ void cta_dots(const Cx<R>* __restrict__ V, long long ldv, int nj,
                                          const Cx<R>* __restrict__ w, long long n,
@@ -125,18 +244,7 @@ __device__ __forceinline__ void cta_dots(const Cx<R>* __restrict__ V, long long 
 #pragma unroll
     for (int q = 0; q < kDotBatch; q++) acc[q] = make_double2(0.0, 0.0);
     const int nb = min(kDotBatch, nj - j0);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-      const double2 wi = to_d2(w[i]);
-#pragma unroll
-      for (int q = 0; q < kDotBatch; q++) {
-        if (q < nb) {
-          const double2 v = to_d2(V[(j0 + q) * ldv + i]);
-          acc[q].x += v.x * wi.x + v.y * wi.y;  // conj(v) * w
-          acc[q].y += v.x * wi.y - v.y * wi.x;
-        }
-      }
-    }
+    dots_rows<R>(V, ldv, j0, nb, w, n, acc);
 #pragma unroll
     for (int q = 0; q < kDotBatch; q++) {
       const double2 s = warp_sum(acc[q]);
@@ -188,18 +296,7 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_update_dots(GmresDev* st, in
   const int nj = k + 1;
   for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<Cx<R>>(st->h1[j]);
   __syncthreads();
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    Cx<R> wi = w[i];
-#pragma unroll 4
-    for (int j = 0; j < nj; j++) {
-      const Cx<R> v = V[j * ldv + i];
-      const Cx<R> h = hs[j];
-      wi.x -= v.x * h.x - v.y * h.y;
-      wi.y -= v.x * h.y + v.y * h.x;
-    }
-    w[i] = wi;
-  }
+  update_rows<R>(V, ldv, nj, hs, w, n);
   __syncthreads();
   cta_dots<R>(V, ldv, nj, w, n, st->partial, sh);
   if (last_block(&st->ticket)) {
@@ -247,20 +344,7 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, in
   const int nj = k + 1;
   for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<Cx<R>>(st->h2[j]);
   __syncthreads();
-  double2 acc = make_double2(0.0, 0.0);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    Cx<R> wi = w[i];
-#pragma unroll 4
-    for (int j = 0; j < nj; j++) {
-      const Cx<R> v = V[j * ldv + i];
-      const Cx<R> h = hs[j];
-      wi.x -= v.x * h.x - v.y * h.y;
-      wi.y -= v.x * h.y + v.y * h.x;
-    }
-    w[i] = wi;
-    acc.x += (double)wi.x * wi.x + (double)wi.y * wi.y;
-  }
+  const double2 acc = make_double2(update_rows<R>(V, ldv, nj, hs, w, n), 0.0);
   const double2 s = block_sum(acc, sh);
   if (threadIdx.x == 0) st->partial[blockIdx.x] = s;
   if (last_block(&st->ticket)) {

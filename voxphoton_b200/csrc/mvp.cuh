@@ -127,13 +127,12 @@ __global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>*
 }
 
 // ---------------------------------------------------------------- kernel 2
+// complex64: three CTAs per SM (80 registers); complex128: its own register need
 template <typename R>
-__global__ void __launch_bounds__(256) k_plane(OpGeom g, FftPlan py, FftPlan pz,
-                                               const Cx<R>* __restrict__ twY,
-                                               const Cx<R>* __restrict__ twZ,
-                                               const Cx<R>* __restrict__ T1,
-                                               const Cx<R>* __restrict__ fN,
-                                               Cx<R>* __restrict__ T2, const int* skip, int fs) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
+    k_plane(OpGeom g, FftPlan py, FftPlan pz, const Cx<R>* __restrict__ twY,
+            const Cx<R>* __restrict__ twZ, const Cx<R>* __restrict__ T1,
+            const Cx<R>* __restrict__ fN, Cx<R>* __restrict__ T2, const int* skip, int fs) {
   using C = Cx<R>;
   const int mb = blockIdx.y;
   if (skip && skip[(long long)mb * fs]) return;

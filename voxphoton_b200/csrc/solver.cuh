@@ -330,8 +330,10 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p, int L, int M, int N,
   for (int i = 0; i < g.L; i++) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
   VOX_TRY(dalloc(&p->twd, g.L));
   VOX_TRY(dalloc(&p->twf, g.L));
-  VOX_CUDA(cudaMemcpy(p->twd, tw.data(), g.L * sizeof(double2), cudaMemcpyHostToDevice));
-  VOX_CUDA(cudaMemcpy(p->twf, twf.data(), g.L * sizeof(float2), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpyAsync(p->twd, tw.data(), g.L * sizeof(double2), cudaMemcpyHostToDevice,
+                           op->stream));
+  VOX_CUDA(cudaMemcpyAsync(p->twf, twf.data(), g.L * sizeof(float2), cudaMemcpyHostToDevice,
+                           op->stream));
   VOX_TRY(pc_alloc_work(p, op->K));
   VOX_TRY(pc_attrs<double>());
   VOX_TRY(pc_attrs<float>());
@@ -358,14 +360,16 @@ static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector
   std::unique_ptr<double2, decltype(&cudaFree)> gG(dG, cudaFree);
   VOX_TRY(dalloc(&dC, 6 * V));
   std::unique_ptr<double2, decltype(&cudaFree)> gC(dC, cudaFree);
-  VOX_CUDA(cudaMemcpy(dG, G.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpyAsync(dG, G.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice,
+                           st));
   k_chan<<<nblk(6 * V), 256, 0, st>>>(g.L, V, dG, dC);
   VOX_CUDA(cudaGetLastError());
   VOX_TRY(fft_axis_d(dC, g.L, g.M, g.N, 1, g.L, (long long)g.L * g.M, V, 6, 0, -1, st));
   double* dface;
   VOX_TRY(dalloc(&dface, g.n3));
   std::unique_ptr<double, decltype(&cudaFree)> gF(dface, cudaFree);
-  VOX_CUDA(cudaMemcpy(dface, face3.data(), g.n3 * sizeof(double), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpyAsync(dface, face3.data(), g.n3 * sizeof(double), cudaMemcpyHostToDevice,
+                           st));
   // Pairing: the Chan circulants satisfy c[L-j] = s*c[j] (s = -1 for xy, xz),
   // so B_{L-i} = D B_i D exactly when G_xy and G_xz vanish on the x = 0 plane
   // (true of the physical tensor); then only modes 0..L/2 are factored.
@@ -475,14 +479,17 @@ static vox_status build_level2(vox_op_s* op, vox_precond_s* p, const std::vector
   for (int i = 0; i < g.M; i++) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
   VOX_TRY(dalloc(&p->twyd, g.M));
   VOX_TRY(dalloc(&p->twyf, g.M));
-  VOX_CUDA(cudaMemcpy(p->twyd, tw.data(), g.M * sizeof(double2), cudaMemcpyHostToDevice));
-  VOX_CUDA(cudaMemcpy(p->twyf, twf.data(), g.M * sizeof(float2), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpyAsync(p->twyd, tw.data(), g.M * sizeof(double2), cudaMemcpyHostToDevice,
+                           st));
+  VOX_CUDA(cudaMemcpyAsync(p->twyf, twf.data(), g.M * sizeof(float2), cudaMemcpyHostToDevice,
+                           st));
   double2 *dA, *dC;
   VOX_TRY(dalloc(&dA, 6 * V));
   std::unique_ptr<double2, decltype(&cudaFree)> gA(dA, cudaFree);
   VOX_TRY(dalloc(&dC, 6 * V));
   std::unique_ptr<double2, decltype(&cudaFree)> gC(dC, cudaFree);
-  VOX_CUDA(cudaMemcpy(dA, A.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpyAsync(dA, A.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice,
+                           st));
   k_chan<<<nblk(6 * V), 256, 0, st>>>(g.L, V, dA, dC);
   VOX_CUDA(cudaGetLastError());
   VOX_TRY(fft_axis_d(dC, g.L, g.M, g.N, 1, g.L, (long long)g.L * g.M, V, 6, 0, -1, st));
@@ -579,7 +586,8 @@ vox_status vox_precond_create_box(vox_op_t op, int level, int x0, int y0, int Ls
     unsigned char* dmask = nullptr;
     if (mask) {
       VOX_TRY(dalloc(&dmask, Vs));
-      VOX_CUDA(cudaMemcpy(dmask, mask, Vs, cudaMemcpyHostToDevice));
+      VOX_CUDA(cudaMemcpyAsync(dmask, mask, Vs, cudaMemcpyHostToDevice,
+                               op->stream));
     }
     k_vmap_box<<<nblk(3 * Vs), 256, 0, op->stream>>>(op->g.L, op->g.M, Ns, x0, y0, Ls, Ms,
                                                      op->vmap, dmask, vm);
@@ -660,7 +668,8 @@ vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const do
         B[i * per + c * ld + r] = make_double2(blk_re[s], blk_im ? blk_im[s] : 0.0);
       }
   VOX_TRY(dalloc(&p->Ad, tot));
-  VOX_CUDA(cudaMemcpy(p->Ad, B.data(), tot * sizeof(double2), cudaMemcpyHostToDevice));
+  VOX_CUDA(cudaMemcpyAsync(p->Ad, B.data(), tot * sizeof(double2), cudaMemcpyHostToDevice,
+                           op->stream));
   p->Lf = g.L;
   p->paired = 0;
   p->f_scale = op->gram;
@@ -778,7 +787,7 @@ static vox_status ensure_work(vox_op_s* op, int m) {
   w.x = w.r + w.ldv;
   w.b = w.x + w.ldv;
   VOX_TRY(dalloc(&w.st, K));
-  VOX_CUDA(cudaMemset(w.st, 0, K * sizeof(GmresDev)));
+  VOX_CUDA(cudaMemsetAsync(w.st, 0, K * sizeof(GmresDev), op->stream));
   VOX_CUDA(cudaMallocHost((void**)&w.hst, K * kGmresHdr));
   VOX_CUDA(cudaMallocHost((void**)&w.hflag, K * sizeof(int)));
   VOX_CUDA(cudaMallocHost((void**)&w.hscal, K * sizeof(double)));
@@ -1090,6 +1099,13 @@ __global__ void k_axpy_d2_from(long long n, const float2* __restrict__ d, double
   }
 }
 
+// Fraction of the remaining relative target that an automatic inner solve aims
+// at: its residual is the true one with a right preconditioner or none, the
+// preconditioned one with a left preconditioner.
+static double inner_target_factor(const vox_precond_s* pc, int side) {
+  return (pc && side == VOX_PREC_LEFT) ? 0.3 : 0.9;
+}
+
 // complex64 GMRES inside FP64 iterative refinement, for `count` right-hand
 // sides at once (members 0..count-1; b_dev and x_dev hold count vectors of n).
 // Each member's result equals what the single-member solve gives for it.
@@ -1110,10 +1126,12 @@ static vox_status refined_run(vox_op_s* op, vox_precond_s* pc, int side, int cou
               " (the operator's members)");
     return VOX_ERR_BAD_ARG;
   }
-  // inner_tol <= 0: aim each inner solve at the remaining target directly
-  // (0.3 * tol * ||b|| / ||r||, the factor leaving room for the gap between the
-  // preconditioned residual GMRES minimises and the true residual)
+  // inner_tol <= 0: aim each inner solve at the remaining target directly,
+  // f * tol * ||b|| / ||r||: f = 0.3 with a left preconditioner (room for the gap
+  // between the preconditioned residual GMRES minimises and the true one),
+  // f = 0.9 otherwise (GMRES minimises the true residual of the complex64 system)
   const bool auto_tol = inner_tol <= 0;
+  const double fac = inner_target_factor(pc, side);
   if (max_refine < 1) max_refine = 10;
   VOX_TRY(ensure_work<float>(op, restart));
   if (!op->wd.arena) VOX_TRY(ensure_work<double>(op, 1));
@@ -1168,7 +1186,7 @@ static vox_status refined_run(vox_op_s* op, vox_precond_s* pc, int side, int cou
       // inner right-hand side: r / ||r|| in complex64 (operator copy is A/Gram)
       k_cast_scale<float><<<nb, 256, 0, st>>>(n, wd.mem(wd.r, b), 1.0 / rn[b], wf.mem(wf.b, b));
       // tolerance relative to ||r||; never ask for less than what reaches tol
-      itol[b] = auto_tol ? std::min(0.5, 0.3 * tol * bn[b] / rn[b])
+      itol[b] = auto_tol ? std::min(0.5, fac * tol * bn[b] / rn[b])
                          : std::min(0.5, std::max(inner_tol, 0.5 * tol * bn[b] / rn[b]));
       op->launches += 1;
     }

@@ -170,7 +170,8 @@ class Family:
         Gc = None
         for j, lam in enumerate(self.nodes):
             pj = problem.with_wavelength(lam)
-            G = G_nodes[j] if G_nodes is not None else assemble_toeplitz(pj.shape, pj.ko, pj.res)
+            G = G_nodes[j] if G_nodes is not None else assemble_toeplitz(pj.shape, pj.ko, pj.res,
+                                                                         device=device)
             self.node_ops.append(Operator(self.mop, pj.Gram, self.idx, G=G, device=device))
             if j == nG // 2:
                 Gc = G
@@ -224,6 +225,8 @@ class ServeConfig:
     batching: str = "continuous"  # "continuous" (a member slot is refilled as soon as
                                   # its solve ends) or "lockstep" (a lane's batch
                                   # starts and ends together)
+    inner_tol: float = 0.0       # relative target of each complex64 inner solve; 0 aims
+                                 # each one at the remaining FP64 target directly
 
 
 class SweepServer:
@@ -259,7 +262,7 @@ class SweepServer:
         side = (1 if c.side == "left" else 2) if pc is not None else 0
         _lib.check(lib.vox_solve_refined_batch(op.handle, pc.handle if pc is not None else None,
                                                side, count, _lib.dptr(bre), _lib.dptr(bim),
-                                               c.tol, c.restart, c.maxit_inner, 0.0, 10,
+                                               c.tol, c.restart, c.maxit_inner, c.inner_tol, 10,
                                                _lib.dptr(xre), _lib.dptr(xim), infos))
         return [(infos[i], (xre[i] + 1j * xim[i]) if c.keep_x else None) for i in range(count)]
 
@@ -281,7 +284,7 @@ class SweepServer:
         pch = pc.handle if pc is not None else None
         if c.mode == "mixed":
             _lib.check(lib.vox_solve_refined(op.handle, pch, side, _lib.dptr(bre), _lib.dptr(bim),
-                                             c.tol, c.restart, c.maxit_inner, 0.0, 10,
+                                             c.tol, c.restart, c.maxit_inner, c.inner_tol, 10,
                                              _lib.dptr(xre), _lib.dptr(xim), ctypes.byref(info)))
         else:
             _lib.check(lib.vox_pgmres(op.handle, pch, side, _lib.VOX_C128, _lib.dptr(bre),
@@ -319,7 +322,7 @@ class SweepServer:
                 bbuf[i * n:(i + 1) * n].copy_(dev_b[req.rid])
             infos = op.solve_refined_batch_device(
                 bbuf.data_ptr(), xbuf.data_ptr(), len(reqs), pc=pc, side=c.side,
-                tol=c.tol, restart=c.restart, maxit_inner=c.maxit_inner, inner_tol=0.0,
+                tol=c.tol, restart=c.restart, maxit_inner=c.maxit_inner, inner_tol=c.inner_tol,
                 max_refine=10)
             for i, req in enumerate(reqs):
                 dev_x[req.rid].copy_(xbuf[i * n:(i + 1) * n])
@@ -349,7 +352,8 @@ class SweepServer:
         if key not in self._lanes:
             c = self.cfg
             self._lanes[key] = Lane(op, pc, side=c.side, tol=c.tol, restart=c.restart,
-                                    maxit_inner=c.maxit_inner, inner_tol=0.0, max_refine=10)
+                                    maxit_inner=c.maxit_inner, inner_tol=c.inner_tol,
+                                    max_refine=10)
         return self._lanes[key]
 
     def close(self):
