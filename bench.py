@@ -247,7 +247,7 @@ def run_reference(args, world, rank):
     Mc = p.Mop()
     ncores = os.cpu_count() or 1
     try:
-        import scipy.fft as sfft
+        import scipy.fft  # noqa: F401  (threaded FFTs for the oracle)
 
         def A(v):
             return ov.mv_AN_const(v, fN, ones, Mc, p.Gram, "notransp", idx)

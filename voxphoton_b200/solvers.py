@@ -13,8 +13,6 @@ is FP64 numpy/scipy on the host, of the size the reference hands to MATLAB.
 """
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 
 from . import _lib
