@@ -1,17 +1,22 @@
 """Benchmark: GMRES solves/s of the JVIE-II frequency solve on B200.
 
-Workload (default): Bragg grating, 60 periods + 2 um quadratic absorbers,
-20 nm voxels -> 1160 x 30 x 11 grid, lambda = 1550 nm, y-polarised plane wave
-along the grating.  One step = one complete solve to 1e-5 relative residual
-||b - A x|| / ||b|| (FP64), by complex64 GMRES(50) inside FP64 iterative
-refinement.  Synthetic, seeded geometry; operator assembled on the host by
-libvox; everything in the timed region runs in libvox's sm_100a kernels.
+Workload (default, `--workload sweep`): the mixed-length Bragg sweep - gratings
+of 20, 40, 60, 80 and 100 periods (520-1800 x 30 x 11 at 20 nm), 201
+wavelengths over 1500-1600 nm each = 1005 solves arriving as a seeded Poisson
+stream, complex64 GMRES(50) + FP64 refinement to 1e-5 relative residual
+||b - A x|| / ||b|| on continuously batched lanes, against the plain complex128
+drop-in solved one request at a time.  Synthetic, seeded geometry; operators
+assembled by libvox; everything in the timed region runs in libvox's sm_100a
+kernels.  Other workloads: microdisk, mor, bragg20, bragg20-p<N>, strip,
+bragg10 (single solves).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vox|reference]
-                    [--precond none|level1] [--workload bragg20|strip|bragg10]
+                    [--workload sweep|microdisk|mor|bragg20|strip|bragg10]
 
-N > 1 (torchrun): independent replicas, one per GPU (the solve does not
-shard); value = total solves / max-over-ranks device time.
+--impl reference: the reference's CPU path (the numpy oracle; MATLAB is
+absent) on the host cores, whole solves.  N > 1 (torchrun): independent
+replicas, one per GPU (the solve does not shard); value = total solves /
+max-over-ranks device time.
 """
 from __future__ import annotations
 
@@ -35,8 +40,8 @@ def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (default: 201 wavelengths for the sweep, 10 solves "
-                         "otherwise)")
+                    help="timed steps (sweep: the whole 1005-solve stream divided into K "
+                         "steps, default 20; other workloads: K solves, default 10)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vox", choices=["vox", "reference"])
     ap.add_argument("--workload", default="sweep",
@@ -47,7 +52,6 @@ def parse():
     ap.add_argument("--inner-tol", type=float, default=0.0,
                     help="complex64 inner GMRES tolerance (0: aim at the target directly)")
     ap.add_argument("--fp64-steps", type=int, default=3)
-    ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
     ap.add_argument("--no-stages", action="store_true", help="skip per-kernel timing")
@@ -206,88 +210,187 @@ def kernel_bytes(op_info, shape, n, pc_info, k):
     return b
 
 
-def cpu_baseline(p, G, idx, b, iters_per_solve, sample_iters, restart):
-    """The oracle (numpy complex128 restatement of mv_AN_const + pgmres_iter)
-    timed on a bounded sample: `sample_iters` Arnoldi steps, scaled to one
-    solve of `iters_per_solve` steps."""
-    from oracle import vie as ov
-    try:
-        from threadpoolctl import threadpool_limits
-        ctx = threadpool_limits(limits=1)
-    except Exception:
-        ctx = None
-    fN = ov.fN_from_toeplitz(G)
-    ones = np.ones(p.shape)
-    Mc = p.Mop()
-    A = lambda v: ov.mv_AN_const(v, fN, ones, Mc, p.Gram, "notransp", idx)
-    t = time.perf_counter()
-    ov.pgmres_iter(A, np.zeros_like(b), b, sample_iters, None, None, None, None, 0.0)
-    dt = time.perf_counter() - t
-    if ctx is not None:
-        ctx.unregister() if hasattr(ctx, "unregister") else None
-    per_iter = dt / sample_iters
-    solve_s = per_iter * max(1, iters_per_solve)
-    return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": 1, "kind": "port",
-            "sample": f"{sample_iters} Arnoldi steps of the numpy complex128 oracle "
-                      f"(mv_AN_const + classical Gram-Schmidt, 1 thread) = {dt:.2f} s, "
-                      f"scaled to {iters_per_solve} steps per solve"}
+def _cpu_geometry():
+    """voxphoton_b200/geometry.py (numpy only) loaded from its file: importing
+    the package would load libvox, which the CPU reference path never touches."""
+    import importlib.util
+    name = "_vox_geometry_cpu"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            name, os.path.join(ROOT, "voxphoton_b200", "geometry.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+class OracleGrating:
+    """The reference CPU path for one Bragg grating of the sweep, on the oracle
+    (numpy complex128 restatement of the reference; libvox is never loaded):
+
+    * Toeplitz tensors at the nG Legendre wavelengths of the band
+      (assembly_nop_const.m with the reference's own compiled cubature cores,
+      oracle/_ref) and their circulants fN (circulant_nop_const.m,
+      fft_operator.m);
+    * the level-1 preconditioner at the band centre (level_1_parallel_func_N.m
+      + Bragg_MOR_script.m:61-72: one dense inverse per x-mode, all L of them);
+    * per request: fN interpolated to its wavelength (lagrange_int.m), the
+      plane-wave JVIE-II right-hand side, then
+      pgmres(A, b, restart, tol, maxit, L1 = chan_mvp_idx) (pgmres.m:70-181).
+
+    FFTs run on `threads` scipy.fft workers, the dense products on numpy's
+    BLAS threads.  Only the pgmres call is timed."""
+
+    def __init__(self, periods, band, threads, nG=5):
+        from oracle import assembly as oa
+        from oracle import vie as ov
+        self.ov = ov
+        self.geo = _cpu_geometry()
+        ov.set_fft_workers(threads)
+        self.threads = threads
+        self.p = self.geo.bragg(periods=periods, M=30)
+        self.nodes = ov.legendre_wavelengths(band[0], band[1], nG)
+        t = time.perf_counter()
+        Gc = None
+        self.fN = []
+        for j, lam in enumerate(self.nodes):
+            q = self.p.with_wavelength(lam)
+            G = oa.assembly_nop_const(q.shape, q.ko, q.res)
+            self.fN.append(ov.fN_from_toeplitz(G))
+            if j == nG // 2:
+                Gc = G
+        L, M, N = self.p.shape
+        circ, _ = ov.level_1_parallel_func_N(Gc, L, M, N, self.p.Gram)
+        self.inv = ov.level1_inverse_blocks(circ, ov.face_from_Mr(self.p.e_r.astype(complex)),
+                                            self.p.Gram)
+        self.setup_s = time.perf_counter() - t
+
+    def solve(self, lam, tol, restart, maxit):
+        """One request; returns (seconds in pgmres, iterations, relres, flag)."""
+        ov = self.ov
+        q = self.p.with_wavelength(lam)
+        _, Mc, idx, b = ov.jvie2_system(self.geo.plane_wave(q), q.e_r, q.Gram, q.freq)
+        fN = ov.lagrange_int(self.fN, lam, self.nodes)
+        L, M, N = q.shape
+        ones = np.ones(q.shape)
+
+        def A(v):
+            return ov.mv_AN_const(v, fN, ones, Mc, q.Gram, "notransp", idx)
+
+        def P(v):
+            return ov.chan_mvp_idx(self.inv, v, L, M, N, idx)
+
+        t = time.perf_counter()
+        _, flag, relres, _, rv = ov.pgmres(A, b, restart, tol, maxit, L1=P)
+        return time.perf_counter() - t, len(rv) - 1, float(relres), int(flag)
+
+
+def _sweep_items(periods, lams):
+    return [(pr, lam) for lam in lams for pr in periods]
+
+
+def _cpu_sample(reqs, key, count):
+    """The first `count` requests of length `key` in arrival order (cycled)."""
+    own = [r for r in sorted(reqs, key=lambda r: r.arrival) if r.key == key]
+    return [own[i % len(own)] for i in range(count)]
+
+
+def cpu_baseline_sweep(args, reqs, band, solves=2):
+    """The oracle on the host cores: `solves` whole requests of the sweep's
+    shortest grating (all threads), as solves/s."""
+    from voxphoton_b200 import serving as sv  # noqa: F401  (request type only)
+    periods = [int(x) for x in args.sweep_periods.split(",")]
+    key = min(periods)
+    threads = os.cpu_count() or 1
+    og = OracleGrating(key, band, threads)
+    ts, its, rr, fl = [], [], [], []
+    for r in _cpu_sample(reqs, key, solves):
+        dt, k, rel, flag = og.solve(r.lam, args.tol, args.restart, 10)
+        ts.append(dt)
+        its.append(k)
+        rr.append(rel)
+        fl.append(flag)
+    L, M, N = og.p.shape
+    return {"value": len(ts) / sum(ts), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{len(ts)} whole requests of the {key}-period grating ({L}x{M}x{N}, the "
+                      f"sweep's shortest, so an upper bound on the CPU rate over the sweep): "
+                      f"numpy complex128 oracle pgmres(A, b, {args.restart}, {args.tol}, 10, "
+                      f"L1 = chan_mvp_idx), operator by lagrange_int over 5 Legendre nodes, "
+                      f"level-1 inverse blocks at the band centre; {sum(ts):.1f} s in pgmres, "
+                      f"{np.mean(its):.1f} iterations, max relres {max(rr):.2e}, flags "
+                      f"{sum(fl)}; setup (assembly with the reference's cubature cores, "
+                      f"{L} dense inverses) {og.setup_s:.1f} s, untimed"}
 
 
 def run_reference(args, world, rank):
-    """--impl reference: the oracle port of the reference CPU path, all host threads.
-    For the sweep, the sample is taken on its middle length (60 periods,
-    1160 x 30 x 11, lambda 1550 nm): a solve of the sweep averages that size."""
+    """--impl reference: the reference's CPU path (its oracle restatement:
+    MATLAB/Octave are absent) on the host cores, whole solves only.
+
+    Sweep: each step is one whole request of the seeded stream on the
+    sweep's shortest grating (20 periods, 520 x 30 x 11), solved as the
+    reference does - operator interpolated over 5 Legendre nodes, level-1
+    preconditioner (all L dense inverse blocks) at the band centre,
+    left-preconditioned pgmres(50) to the tolerance.  The shortest grating
+    is the cheapest solve of the sweep, so this rate is an upper bound on the
+    CPU path's solves/s over the mixed stream."""
     if rank != 0:
         return
-    sweep = args.workload == "sweep"
-    p, G, idx, b, _ = build_problem("bragg20" if sweep else args.workload)
-    from oracle import vie as ov
-    fN = ov.fN_from_toeplitz(G)
-    ones = np.ones(p.shape)
-    Mc = p.Mop()
-    ncores = os.cpu_count() or 1
-    try:
-        import scipy.fft  # noqa: F401  (threaded FFTs for the oracle)
-
-        def A(v):
-            return ov.mv_AN_const(v, fN, ones, Mc, p.Gram, "notransp", idx)
-        ov.set_fft_workers(ncores)
-    except Exception:
-        A = lambda v: ov.mv_AN_const(v, fN, ones, Mc, p.Gram, "notransp", idx)
-    # sweep: one Arnoldi step per step (201 steps by default), otherwise
-    # --cpu-sample-iters steps per step
-    steps = args.steps or 201
-    sample = 1 if sweep else max(1, args.cpu_sample_iters)
-    iters = int(os.environ.get("VOX_REF_ITERS_PER_SOLVE", "0")) or None
-    times = []
-    for s in range(args.warmup + steps):
-        t = time.perf_counter()
-        ov.pgmres_iter(A, np.zeros_like(b), b, sample, None, None, None, None, 0.0)
-        dt = time.perf_counter() - t
-        if s >= args.warmup:
-            times.append(dt)
-    per_iter = float(np.mean(times)) / sample
-    # iterations per solve: a plain complex128 GMRES(50) solve at tol needs this
-    # many Arnoldi steps on this workload (measured by the GPU arm; default
-    # from the same oracle on a single restart cycle if not given)
-    # (the sweep's plain complex128 solves average 31 steps at 1e-5)
-    ips = iters or (31 if sweep else 300)
-    val = 1.0 / (per_iter * ips)
+    threads = os.cpu_count() or 1
+    steps = args.steps or 20
+    if args.workload != "sweep":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"the CPU reference arm covers the sweep workload only "
+                          f"(asked: {args.workload})"}), flush=True)
+        return
+    band = (1500e-9, 1600e-9)
+    periods = [int(x) for x in args.sweep_periods.split(",")]
+    key = min(periods)
+    lams = np.linspace(band[0], band[1], args.sweep_lambdas)
+    reqs = _poisson(_sweep_items(periods, lams), args.sweep_rate, args.seed)
+    og = OracleGrating(key, band, threads)
+    sample = _cpu_sample(reqs, key, args.warmup + steps)
+    for r in sample[:args.warmup]:
+        og.solve(r.lam, args.tol, args.restart, 10)
+    ts, its, rr, fl = [], [], [], []
+    for r in sample[args.warmup:]:
+        dt, k, rel, flag = og.solve(r.lam, args.tol, args.restart, 10)
+        ts.append(dt)
+        its.append(k)
+        rr.append(rel)
+        fl.append(flag)
+    tot = sum(ts)
+    val = steps / tot
+    L, M, N = og.p.shape
+    sample_txt = (f"{steps} whole requests of the {key}-period grating ({L}x{M}x{N}), "
+                  f"numpy complex128 oracle, pgmres(A, b, {args.restart}, {args.tol}, 10, "
+                  f"L1 = chan_mvp_idx), {threads} threads; {np.mean(its):.1f} iterations per "
+                  f"solve, max relres {max(rr):.2e}, flags {sum(fl)}")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "solves/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * per_iter * ips, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * tot / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": ("sweep: mixed-length Bragg gratings, 1500-1600 nm (CPU "
-                                    "sample on the 60-period 1160x30x11 grating)") if sweep
-                       else args.workload, "grid": list(p.shape), "n": int(idx.size),
-                       "tol": args.tol, "restart": args.restart, "precond": args.precond},
-            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": ncores, "kind": "port",
-                             "sample": f"{sample} Arnoldi steps per step of the numpy "
-                                       f"complex128 oracle (scipy.fft workers={ncores}), "
-                                       f"scaled to {ips} steps per solve"},
+            "config": {"workload": f"sweep: mixed-length Bragg gratings of {periods} periods, "
+                                   f"{len(lams)} wavelengths over 1500-1600 nm each = "
+                                   f"{len(reqs)} solves; the CPU reference solves whole "
+                                   f"requests of its shortest grating ({L}x{M}x{N})",
+                       "tol": args.tol, "restart": args.restart,
+                       "precond": "level1 at band centre, left (pgmres L1)",
+                       "setup_s": round(og.setup_s, 1)},
+            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": sample_txt},
             "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _poisson(items, rate, seed):
+    """serving.poisson_stream without importing the package (same draws)."""
+    from types import SimpleNamespace
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(len(items))
+    t = np.cumsum(rng.exponential(1.0 / rate, size=len(items)))
+    return [SimpleNamespace(rid=int(i), key=items[k][0], lam=items[k][1], arrival=float(t[i]))
+            for i, k in enumerate(order)]
 
 
 def _progress(msg, _t0=[time.time()]):
@@ -312,23 +415,30 @@ def _assemble_family_nodes(periods, band, device):
 def run_sweep(args, world, rank, local):
     """Mixed-length Bragg sweep served as a Poisson request stream.
 
-    One step = one wavelength of the sweep at every device length (5 solves);
-    --steps K takes K wavelengths evenly spaced over 1500-1600 nm (201 = the
-    full sweep, 1005 solves).  Each rank serves its own copy of the stream
-    (replicas, weak scaling).  `value`: the stream with every right-hand side
-    already resident in HBM (vox_solve_refined_batch_device); `e2e`: the same
-    stream through the host-buffer C-ABI (vox_solve_refined_batch), inputs
-    copied in and solutions copied out inside the timed region."""
+    The stream is always the whole sweep: 5 gratings x 201 wavelengths over
+    1500-1600 nm = 1005 solves per GPU (each rank serves its own copy:
+    replicas, weak scaling); --steps K only divides it (one step = 1005/K
+    solves, ms_per_step = stream time / K) and --warmup W serves W steps' worth
+    of extra requests before timing.  After a common warm-up, two legs are
+    timed back to back on the same warm lanes:
+
+    * e2e (first): the stream through the host-buffer C-ABI (vox_lane_submit /
+      vox_lane_collect), right-hand sides formed on the host and copied in,
+      solutions copied out, inside the timed region;
+    * value (second): the same stream with every right-hand side already in
+      HBM (vox_lane_submit_device), solutions left there."""
     import torch
     import voxphoton_b200 as vb
-    from voxphoton_b200 import _lib
     from voxphoton_b200 import geometry as geo
     from voxphoton_b200 import serving as sv
     torch.cuda.set_device(local)
     periods = [int(x) for x in args.sweep_periods.split(",")]
     band = (1500e-9, 1600e-9)
-    steps = args.steps if args.steps else 201
-    lams = np.linspace(band[0], band[1], steps)
+    lams = np.linspace(band[0], band[1], args.sweep_lambdas)
+    items = _sweep_items(periods, lams)
+    total = len(items)
+    steps = args.steps if args.steps else 20
+    per_step = total / steps
     t = time.time()
     Gs = _assemble_family_nodes(periods, band, local)
     fams = [sv.Family(pr, geo.bragg(periods=pr, M=30), band, nG=5, device=local,
@@ -338,7 +448,7 @@ def run_sweep(args, world, rank, local):
     _progress("setup")
     # admission by HBM footprint: lanes per length from one lane's bytes
     torch.cuda.synchronize()
-    free0, total = torch.cuda.mem_get_info()
+    free0, total_mem = torch.cuda.mem_get_info()
     fams[-1].add_slot()
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
@@ -356,34 +466,45 @@ def run_sweep(args, world, rank, local):
         for op, pc in f.slots:
             op.torch_stream = torch.cuda.Stream()
             op.set_stream(op.torch_stream.cuda_stream)
-    items = [(pr, lam) for lam in lams for pr in periods]
     reqs = sv.poisson_stream(items, rate=args.sweep_rate, seed=args.seed + rank)
     cfg = sv.ServeConfig(tol=args.tol, side=args.sweep_side, batching=args.sweep_batching,
                          inner_tol=args.inner_tol)
     srv = sv.SweepServer(fams, cfg)
     srv.prepare_device()
-    # warm-up: a full batch on every lane (captures the cycle graphs), then W
-    # untimed steps of the stream
+    # common warm-up: a full batch on every lane (captures the cycle graphs),
+    # then W steps' worth of requests at wavelengths between the sweep's
     srv.warm()
-    _progress("warm")
-    wl = np.linspace(band[0], band[1], max(args.warmup, 1) + 2)[1:-1]
+    n_warm = max(len(periods), int(round(args.warmup * per_step)))
+    wl = np.linspace(band[0], band[1], n_warm // len(periods) + 2)[1:-1]
     srv.serve([sv.Request(-1 - i, pr, lam, 0.0)
-               for i, (pr, lam) in enumerate((pr, l) for l in wl for pr in periods)],
-              realtime=False)
+               for i, (pr, lam) in enumerate(_sweep_items(periods, wl))], realtime=False)
     torch.cuda.synchronize()
+    _progress(f"warm ({n_warm} requests)")
     fam_of = {f.key: f for f in fams}
-    # every request's right-hand side resident in HBM before the timed region
+    lane_ops = [op for f in fams for op, _ in f.slots]
+    clocks = None if args.no_clocks else Clocks(local)
+    if clocks:
+        clocks.start()
+    # leg 1: e2e through the host-buffer C-ABI
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e2.record()
+    res_h, wall_h = srv.serve(reqs, realtime=True)
+    torch.cuda.synchronize()
+    e3.record()
+    torch.cuda.synchronize()
+    e2e_s = e2.elapsed_time(e3) / 1e3
+    summ_h = sv.summarize(res_h, wall_h)
+    _progress(f"host-buffer stream: {len(reqs)} solves in {e2e_s:.2f} s")
+    # every request's right-hand side resident in HBM before the second leg
     dev_b = {}
     for r in reqs:
         b = fam_of[r.key].rhs(geo.C0 / r.lam * geo.N_EXT)
         dev_b[r.rid] = torch.from_numpy(b).to("cuda")
     dev_x = {r.rid: torch.empty_like(dev_b[r.rid]) for r in reqs}
     torch.cuda.synchronize()
-    lane_ops = [op for f in fams for op, _ in f.slots]
+    # leg 2: device-resident
     l0 = sum(op.launches() for op in lane_ops)
-    clocks = None if args.no_clocks else Clocks(local)
-    if clocks:
-        clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
@@ -397,17 +518,6 @@ def run_sweep(args, world, rank, local):
     launches = sum(op.launches() for op in lane_ops) - l0 + 10 * len(reqs)
     summ_dev = sv.summarize(res_dev, wall_dev)
     _progress(f"device-resident stream: {len(reqs)} solves in {dev_s:.2f} s")
-    # e2e: the same stream through the host-buffer C-ABI
-    torch.cuda.synchronize()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record()
-    res_h, wall_h = srv.serve(reqs, realtime=True)
-    torch.cuda.synchronize()
-    e3.record()
-    torch.cuda.synchronize()
-    e2e_s = e2.elapsed_time(e3) / 1e3
-    summ_h = sv.summarize(res_h, wall_h)
-    _progress(f"host-buffer stream: {e2e_s:.2f} s")
     # roofline of the dominant kernel: the inverse-block apply of one lane of
     # the 1160 x 30 x 11 grating at the lane's width (stage timing by CUDA
     # events on the lane's stream)
@@ -421,12 +531,19 @@ def run_sweep(args, world, rank, local):
     alg = info_m["n_blocks"] * n3 * n3 * 8 + 2 * K * L * n3 * 8
     hbm, src = peaks()
     ach = alg / (stage["pc_solve"] * 1e-3) / 1e9
+    mvb = kernel_bytes(op_m.info(), fmid.p.shape, fmid.idx.size, info_m, 20)
+    mv_bytes = K * (mvb["mv_xfwd"] + mvb["mv_plane"] + mvb["mv_xinv"])
+    mv_ms = stage["mv_xfwd"] + stage["mv_plane"] + stage["mv_xinv"]
     roof = {"bound": "hbm", "kernel": f"pc_solve (k_pc_inv_apply, {K} members, "
                                       f"{L}x{M}x{N})",
             "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
             "traffic": measured_traffic("pc_solve", alg), "peak_source": src,
             "bytes_per_launch": alg, "ms_per_launch": stage["pc_solve"],
-            "stage_ms": stage}
+            "stage_ms": stage,
+            "matvec": {"kernels": "k_xfwd + k_plane + k_xinv", "members": K,
+                       "bytes_per_launch": mv_bytes, "ms": mv_ms,
+                       "achieved": mv_bytes / (mv_ms * 1e-3) / 1e9,
+                       "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm}}
     # the lanes are done: free them and the staged vectors before the baseline
     del dev_b, dev_x
     srv._bufs.clear()
@@ -449,6 +566,7 @@ def run_sweep(args, world, rank, local):
     rng = np.random.default_rng(args.seed)
     sub = [reqs[i] for i in rng.choice(len(reqs), size=min(len(reqs), args.sweep_fp64),
                                        replace=False)]
+
     def fp64_serial_run(side):
         srv64 = sv.SweepServer(fams, sv.ServeConfig(tol=args.tol, mode="fp64", side=side))
         for f in fams:
@@ -473,14 +591,12 @@ def run_sweep(args, world, rank, local):
         dev_s, e2e_s = (float(v) for v in tt.tolist())
     value = len(reqs) * world / dev_s
     e2e_val = len(reqs) * world / e2e_s
+    for f in fams:
+        f.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        p_m = fmid.p.with_wavelength(1550e-9)
-        G_m = vb.assemble_toeplitz(p_m.shape, p_m.ko, p_m.res)
-        b_m = vb.jvie_rhs(p_m.e_r, geo.plane_wave(p_m), p_m.Gram, p_m.freq, p_m.idxS3())
-        cpu = cpu_baseline(p_m, G_m, p_m.idxS3(), b_m, int(round(fp64["mean_iters"])),
-                           args.cpu_sample_iters, args.restart)
-        cpu["sample"] += f" on the {L}x{M}x{N} grating"
+        cpu = cpu_baseline_sweep(args, reqs, band)
+        _progress("cpu baseline")
     if rank == 0:
         nbar = int(np.mean([fam_of[r.key].idx.size for r in reqs]))
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
@@ -490,15 +606,19 @@ def run_sweep(args, world, rank, local):
                 "dtype": "c64", "data": "synthetic",
                 "config": {"workload": f"sweep: mixed-length Bragg gratings of {periods} periods "
                                        f"(grids {[list(f.p.shape) for f in fams]}, 20 nm voxels), "
-                                       f"{steps} wavelengths over 1500-1600 nm each = "
+                                       f"{len(lams)} wavelengths over 1500-1600 nm each = "
                                        f"{len(reqs)} solves per GPU, seeded Poisson arrivals at "
                                        f"{args.sweep_rate}/s (seed {args.seed + rank}), sizes "
-                                       f"interleaved; one step = one wavelength at all lengths",
+                                       f"interleaved; one step = {per_step:.2f} solves of the "
+                                       f"stream",
                            "tol": args.tol, "restart": args.restart,
                            "solver": f"complex64 GMRES + FP64 refinement, {args.sweep_batching} "
                                      f"batching",
                            "lanes_per_length": nslots, "members_per_lane": K,
                            "lane_bytes": int(lane_bytes), "setup_s": round(setup_s, 1),
+                           "warmup_requests": n_warm,
+                           "legs": "common warm-up, then e2e (host buffers) first and the "
+                                   "device-resident stream second, on the same lanes",
                            "operator": "Lagrange interpolation of fN over 5 Legendre wavelengths",
                            "precond": f"level1 at band centre, shared per length, "
                                       f"{args.sweep_side} (inner solves)",
@@ -520,17 +640,16 @@ def run_sweep(args, world, rank, local):
                 "speedup_vs_fp64_serial": value / world / fp64_serial,
                 "speedup_vs_fp64_true_residual_serial": value / world / fp64r_serial,
                 "e2e": {"value": e2e_val, "unit": "solves/s",
-                        "h2d_bytes_per_step": nbar * 16 * len(periods),
-                        "d2h_bytes_per_step": nbar * 16 * len(periods),
+                        "h2d_bytes_per_step": int(nbar * 16 * per_step),
+                        "d2h_bytes_per_step": int(nbar * 16 * per_step),
                         "latency_ms": {"p50": summ_h["p50_ms"], "p99": summ_h["p99_ms"]},
-                        "max_relres": summ_h["max_relres"], "flags": summ_h["flags"]},
+                        "max_relres": summ_h["max_relres"], "flags": summ_h["flags"],
+                        "mean_iters": summ_h["mean_iters"]},
                 "gpu_launches": int(launches),
                 "roofline": roof,
                 "cpu_baseline": cpu,
                 "clocks": clk}
         print(json.dumps(line), flush=True)
-    for f in fams:
-        f.close()
 
 
 def run_microdisk(args, world, rank, local):
@@ -944,9 +1063,23 @@ def main():
                 "ms_per_launch": stages[dom], "stage_ms": stages}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        iters_solve = fp64["iters"] if fp64 else int(np.mean(iters))
-        cpu = cpu_baseline(p, G, idx, b, iters_solve, args.cpu_sample_iters, args.restart)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.precond == "none":
+        # one whole unpreconditioned oracle solve on all host threads
+        from oracle import vie as ov
+        threads = os.cpu_count() or 1
+        ov.set_fft_workers(threads)
+        fN = ov.fN_from_toeplitz(G)
+        ones = np.ones(p.shape)
+        Mc = p.Mop()
+        t = time.perf_counter()
+        _, flag, rel, _, rv = ov.pgmres(
+            lambda v: ov.mv_AN_const(v, fN, ones, Mc, p.Gram, "notransp", idx), b,
+            args.restart, args.tol, 20)
+        dt = time.perf_counter() - t
+        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"one whole solve of the numpy complex128 oracle pgmres(A, b, "
+                         f"{args.restart}, {args.tol}, 20): {len(rv) - 1} iterations, relres "
+                         f"{rel:.2e}, {dt:.1f} s"}
 
     if rank == 0:
         line = {

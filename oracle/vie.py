@@ -15,7 +15,7 @@ conventions.
 Parity status: the MATLAB built-ins (fftn, inv, mldivide, gmres) are closed
 MathWorks code that cannot run here, so at that boundary parity is pinned by
 restatement, by a dense O(V^2) Toeplitz direct sum on tiny grids and by
-scipy cross-checks (see tests/test_oracle_*.py).
+scipy cross-checks (tests/test_oracle.py).
 """
 from __future__ import annotations
 
@@ -457,15 +457,22 @@ def level1_inverse_blocks(circ, face3, Gram):
     return [np.linalg.inv(b) for b in level1_blocks(circ, face3, Gram)]
 
 
+def _fft1(x, axis, inverse=False):
+    if _FFT_WORKERS:
+        import scipy.fft as sf
+        return (sf.ifft if inverse else sf.fft)(x, axis=axis, workers=_FFT_WORKERS)
+    return (np.fft.ifft if inverse else np.fft.fft)(x, axis=axis)
+
+
 def chan_mvp_idx(inv_blocks, JIn, L, M, N, idx):
     """chan_mvp_idx.m:2-17: scatter, fft along x, per-mode dense matvec, ifft, gather."""
     V = np.zeros(3 * L * M * N, dtype=complex)
     V[np.asarray(idx, dtype=np.int64) - 1] = JIn
     temp = V.reshape((L, 3 * M * N), order="F")
-    temp = np.fft.fft(temp, axis=0).T
+    temp = _fft1(temp, 0).T
     for i in range(L):
         temp[:, i] = inv_blocks[i] @ temp[:, i]
-    temp = np.fft.ifft(temp.T, axis=0)
+    temp = _fft1(temp.T, 0, inverse=True)
     return temp.reshape(-1, order="F")[np.asarray(idx, dtype=np.int64) - 1]
 
 
@@ -473,6 +480,27 @@ def chan_mvp(inv_blocks, Vrhs, L, M, N):
     """chan_mvp.m:2-12 (no index map)."""
     idx = np.arange(1, 3 * L * M * N + 1)
     return chan_mvp_idx(inv_blocks, Vrhs, L, M, N, idx)
+
+
+def lagrange_int(fN, S, s):
+    """lagrange_int.m:1-12: P = sum_i L_i(S) fN{i}, the Lagrange interpolant of
+    the node operators fN{i} (nodes s) at wavelength S."""
+    n = len(s)
+    P = 0
+    for i in range(n):
+        Li = 1.0
+        for j in range(n):
+            if j != i:
+                Li = Li * (S - s[j]) / (s[i] - s[j])
+        P = P + Li * fN[i]
+    return P
+
+
+def legendre_wavelengths(s_minus, s_plus, nG):
+    """Si_in_SiO2_parameters.m:7-14: s = s_mid + (s_plus - s_minus)/2 * xG with
+    xG the nG Gauss-Legendre points (gauss_1d.m)."""
+    xG, _ = np.polynomial.legendre.leggauss(nG)
+    return 0.5 * (s_plus + s_minus) + 0.5 * (s_plus - s_minus) * xG
 
 
 # --------------------------------------------------------------------------
@@ -802,3 +830,15 @@ def jvie2_system(Einc, e_r, Gram, freq, idxS=None):
     Mc = Mc / Mr
     Mr = np.ones_like(Mr)
     return Mr, Mc, idxS3, Vrhs
+
+
+def transmitted_power(E, res, len_abs, delW):
+    """example_Bragg_1500nm_to_1600nm.m:107-113: sum of |E|^2 over the x-slice
+    xThru = L - round((len_abs + 450e-9)/res) (1-based), trimmed by
+    voxFromEdge = round(delW/2)/res voxels at each y edge (the reference
+    rounds a length in metres, so nanometre corrugations trim nothing)."""
+    L, M = E.shape[:2]
+    xThru = L - int(round((len_abs + 450e-9) / res))
+    voxFromEdge = int(round(round(delW / 2) / res))
+    eThru = E[xThru - 1, voxFromEdge:M - voxFromEdge, :, :]
+    return float(np.sum(np.real(eThru * np.conj(eThru))))

@@ -24,7 +24,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-REF_GAUSS = ("/root/reference/piecewise_constant/src_vie/src_operators/cubatures/gauss_1d.m")
+# REFERENCE: the reference project root (the variable oracle/Makefile reads)
+REF_GAUSS = os.path.join(os.environ.get("REFERENCE", "/root/reference"),
+                         "piecewise_constant/src_vie/src_operators/cubatures/gauss_1d.m")
 
 
 def parse_gauss(path, orders):

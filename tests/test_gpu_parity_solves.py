@@ -1,0 +1,147 @@
+"""Solve-level parity with the oracle on the benchmark's own inputs.
+
+* Straight strip (100 x 25 x 11 at 20 nm, 1550 nm, y-polarised plane wave along
+  the strip): unpreconditioned GMRES(50) to 1e-5 in complex128, run by libvox
+  and by the oracle's pgmres (pgmres.m:70-181) in the test.
+* The sweep's 20-period Bragg grating (520 x 30 x 11): GMRES(50) to 1e-5 with
+  the level-1 circulant preconditioner on the left (the drop-in, pgmres L1)
+  and on the right, and without a preconditioner, against the oracle's solves
+  pinned in tests/golden/bragg_p20_solves.npz (made by
+  tests/golden/make_solve_fixtures.py from the oracle and the reference's
+  compiled cubature cores).  The 60-period grating's complex128 oracle
+  preconditioner (1160 inverse blocks of 990^2, 18 GB) is too heavy for a test
+  host, so the grating of the same cross-section with 20 periods stands in.
+
+Compared: the iteration record, the residual history, the final true relres
+and flag (pgmres.m:175-180), the solution and the transmitted power of
+example_Bragg_1500nm_to_1600nm.m:107-113.  libvox uses classical Gram-Schmidt
+with re-orthogonalisation and Givens rotations where the reference uses
+one-pass CGS and a least-squares backslash: the same Krylov process, so the
+histories agree to rounding within the first restart cycle, the solutions to
+well inside the 1e-5 tolerance, and iteration counts to a step or two over
+many restarts.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import voxphoton_b200 as vb
+from oracle import vie as ov
+from voxphoton_b200 import geometry as geo
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURE = os.path.join(HERE, "golden", "bragg_p20_solves.npz")
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def steps(resvec):
+    return len(resvec) - 1
+
+
+def test_strip_solve_matches_oracle():
+    p = geo.strip()
+    assert p.shape == (100, 25, 11)
+    G = vb.assemble_toeplitz(p.shape, p.ko, p.res)
+    fN = ov.fN_from_toeplitz(G)
+    _, Mc, idx, b = ov.jvie2_system(geo.plane_wave(p), p.e_r, p.Gram, p.freq)
+    op = vb.Operator(Mc, p.Gram, idx, G=G)
+    x, flag, relres, it, resvec = vb.pgmres(op, b, 50, 1e-5, 20)
+    ones = np.ones(p.shape)
+    xr, flag_r, relres_r, it_r, resvec_r = ov.pgmres(
+        lambda v: ov.mv_AN_const(v, fN, ones, Mc, p.Gram, "notransp", idx), b, 50, 1e-5, 20)
+    assert flag == flag_r == 0
+    assert relres <= 1e-5 and relres_r <= 1e-5
+    assert it[1] == it_r[1] and abs(it[0] - it_r[0]) <= 1
+    first = slice(0, min(51, len(resvec), len(resvec_r)))
+    assert np.max(np.abs(resvec[first] - resvec_r[first]) / resvec_r[first]) < 1e-6
+    assert rel(x, xr) < 1e-5
+    op.close()
+
+
+@pytest.fixture(scope="module")
+def p20():
+    ref = np.load(FIXTURE)
+    p = geo.bragg(periods=20, M=30)
+    assert tuple(ref["shape"]) == p.shape and float(ref["lam0"]) == p.lam0
+    L, M, N = p.shape
+    G = vb.assemble_toeplitz(p.shape, p.ko, p.res)
+    idx = p.idxS3()
+    assert idx.size == int(ref["n"])
+    Einc = geo.plane_wave(p)
+    b = vb.jvie_rhs(p.e_r, Einc, p.Gram, p.freq, idx)
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=G)
+    pc = vb.Preconditioner.level1(op, G, p.e_r)
+    V = L * M * N
+    op_full = vb.Operator(p.Mop(), p.Gram, np.arange(1, 3 * V + 1), G=G, precisions=("c128",))
+    yield p, ref, op, pc, op_full, b, idx, Einc
+    pc.close()
+    op.close()
+    op_full.close()
+
+
+def _power(p, op_full, x, idx, Einc):
+    L, M, N = p.shape
+    J = np.zeros(3 * L * M * N, dtype=complex)
+    J[idx - 1] = x
+    E = vb.E_field_Nop_const(J.reshape((L, M, N, 3), order="F"), op_full, p.Gram, p.freq, Einc)
+    return vb.transmitted_power(E, p.res, p.meta["len_abs"], 2 * p.meta["corrugation"])
+
+
+@pytest.mark.parametrize("side", ["left", "right"])
+def test_bragg_p20_level1_solve_matches_oracle(p20, side):
+    p, ref, op, pc, op_full, b, idx, Einc = p20
+    kw = {"L1": pc} if side == "left" else {"R1": pc}
+    x, flag, relres, it, resvec = vb.pgmres(op, b, 50, 1e-5, 10, prec="c128", **kw)
+    it_r = ref[f"{side}_iter"]
+    resvec_r = ref[f"{side}_resvec"]
+    assert flag == int(ref[f"{side}_flag"])
+    assert it[1] == it_r[1] and abs(it[0] - it_r[0]) <= 1
+    k = min(len(resvec), len(resvec_r))
+    assert np.max(np.abs(resvec[:k] - resvec_r[:k]) / resvec_r[:k]) < 1e-6
+    assert abs(relres - float(ref[f"{side}_relres"])) <= 1e-2 * float(ref[f"{side}_relres"])
+    sub = ref["sub"]
+    assert rel(x[sub], ref[f"{side}_xsub"]) < 1e-5
+    assert abs(np.linalg.norm(x) - float(ref[f"{side}_xnorm"])) <= 1e-6 * float(
+        ref[f"{side}_xnorm"])
+    P = _power(p, op_full, x, idx, Einc)
+    Pr = float(ref[f"{side}_power"])
+    assert abs(P - Pr) <= 1e-5 * abs(Pr)
+
+
+def test_bragg_p20_unpreconditioned_solve_matches_oracle(p20):
+    p, ref, op, pc, op_full, b, idx, Einc = p20
+    x, flag, relres, it, resvec = vb.pgmres(op, b, 50, 1e-5, 40, prec="c128")
+    resvec_r = ref["none_resvec"]
+    assert flag == int(ref["none_flag"]) == 0 and relres <= 1e-5
+    # the first restart cycle is the same Krylov process: histories to rounding
+    assert np.max(np.abs(resvec[:51] - resvec_r[:51]) / resvec_r[:51]) < 1e-6
+    # later cycles restart from residuals that carry one-pass CGS vs CGS2
+    # rounding; over ~19 restarts the counts stay within 1 %
+    n, n_r = steps(resvec), steps(resvec_r)
+    assert abs(n - n_r) <= max(2, 0.01 * n_r), (n, n_r)
+    sub = ref["sub"]
+    assert rel(x[sub], ref["none_xsub"]) < 1e-4
+    P = _power(p, op_full, x, idx, Einc)
+    Pr = float(ref["none_power"])
+    assert abs(P - Pr) <= 1e-4 * abs(Pr)
+    # the level-1 preconditioner's effect, as the oracle sees it
+    assert steps(ref["left_resvec"]) * 10 < n_r
+
+
+def test_bragg_p20_mixed_precision_meets_the_tolerance_and_matches(p20):
+    """complex64 GMRES + FP64 refinement (right level-1) reaches the true 1e-5 and
+    agrees with the oracle's solution and transmitted power within it."""
+    p, ref, op, pc, op_full, b, idx, Einc = p20
+    x, info = vb.solve_refined(op, b, tol=1e-5, restart=50, maxit_inner=40, R1=pc)
+    assert info["flag"] == 0 and info["relres"] <= 1e-5
+    sub = ref["sub"]
+    assert rel(x[sub], ref["right_xsub"]) < 1e-4
+    P = _power(p, op_full, x, idx, Einc)
+    Pr = float(ref["right_power"])
+    assert abs(P - Pr) <= 1e-4 * abs(Pr)
