@@ -85,6 +85,9 @@ typedef struct {
   int device;                /* CUDA device ordinal */
 } vox_op_desc;
 
+/* Non-convergence (pgmres.m:176-180) is info.flag = 1 with VOX_OK; a solver
+ * entry point called with info == NULL returns VOX_ERR_NOT_CONVERGED instead,
+ * as the caller could not see the flag. */
 typedef struct {
   int flag;                  /* 0 converged (relres <= tol), 1 not converged */
   double relres;             /* ||b - A x|| / ||b|| in FP64 (pgmres.m:175) */
@@ -100,6 +103,14 @@ typedef struct {
 
 const char* vox_last_error(void);
 int vox_abi_version(void);
+/* Every wait of the library on the device is bounded: it polls against this
+ * limit and returns VOX_ERR_TIMEOUT when the work has not finished (the work
+ * stays queued; the handles stay usable once it drains).  Process-wide; the
+ * default is VOX_WAIT_TIMEOUT_S from the environment, else 600 s; 0 restores
+ * the default.  Teardown (the destroy calls) waits without a limit.  The
+ * reference has no counterpart (MATLAB blocks on gpuArray results). */
+vox_status vox_set_wait_timeout(double seconds);
+double vox_get_wait_timeout(void);
 
 vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out);
 /* An operator with `members` (1..8) independent copies of fN and of all solve
@@ -317,6 +328,46 @@ vox_status vox_lane_state(vox_lane_t lane, int* states);
 vox_status vox_jvie_rhs(int L, int M, int N, const double* er_re, const double* er_im,
                         const double* Einc_re, const double* Einc_im, double gram, double freq,
                         const double* idx, long long n_idx, double* out_re, double* out_im);
+
+/* One-call JVIE solve:
+ * [Je,flag,relres,iter,resvec,solvert] = JVIE_Solver_const(Einc,e_r,r,freq,fN,tol,
+ *     form,solver,precond,max_it,inner_it,outer_it)
+ * piecewise_constant/src_vie/src_solver/JVIE_Solver_const.m:1.  Builds the
+ * support (|e_r - 1| > 1e-12), the contrast and the right-hand side as the
+ * reference does (:133-157), applies the JVIE-II scaling (:243-251), solves
+ * with restarted GMRES (inner_it restart, outer_it cycles) and returns the
+ * current density on the whole grid (L x M x N x 3, zero outside the
+ * scatterer, :521-522).  Implemented: form 2 and solver 'G' (others return
+ * VOX_ERR_UNSUPPORTED; the Python mirror routes 'D' and 'B' to its GMRES-DR
+ * and BiCGStab drivers).  JVIE-II's own preconditioner is Gram * I, to which
+ * GMRES is invariant, so precond 'L' / 'R' give the unpreconditioned
+ * iterates.  prec VOX_C128 is the reference's complex128 pgmres;
+ * VOX_C64 is complex64 GMRES inside FP64 refinement to the same tol.  The
+ * operator is uploaded and freed within the call. */
+typedef struct {
+  int L, M, N;
+  const double* Einc_re;     /* L x M x N x 3, column-major */
+  const double* Einc_im;     /* may be NULL */
+  const double* er_re;       /* relative permittivity, L x M x N */
+  const double* er_im;       /* may be NULL */
+  double dx;                 /* voxel edge: Gram = dx^3 (:140-141) */
+  double freq;               /* Hz */
+  int LfN, MfN, NfN;         /* the N operator fN (as vox_op_desc) ... */
+  const double* fN_re;
+  const double* fN_im;
+  const double* G_re;        /* ... or its Toeplitz tensor: exactly one */
+  const double* G_im;
+  double tol;                /* outside [1e-15, 1): 1e-3, as the reference */
+  int form;                  /* 2 (0 means 2) */
+  char solver;               /* 'G' (0 means 'G') */
+  char precond;              /* 'L', 'R' or 0 */
+  int inner_it;              /* restart length, < 1: 50 */
+  int outer_it;              /* restart cycles (refinement: inner cycles), < 1: 200 */
+  vox_prec prec;
+  int device;
+} vox_jvie_desc;
+vox_status vox_jvie_solve(const vox_jvie_desc* desc, double* Je_re, double* Je_im,
+                          vox_gmres_info* info);
 
 /* Host assembly of the Toeplitz tensor G_mn (L x M x N x 6, column-major),
  * assembly_nop_const(r, ko, dx, 'DEMCEM').  nthreads <= 0 uses all cores. */

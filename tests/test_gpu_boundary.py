@@ -1,0 +1,158 @@
+"""The C-ABI's whole-solve entry point and its status codes, on the GPU.
+
+* vox_jvie_solve / vie.JVIE_Solver_const (JVIE_Solver_const.m:1): the solve
+  from Einc, e_r, the grid and the operator, against the oracle's pgmres on the
+  system the reference builds (:133-157, :243-251), and the GMRES-DR / BiCGStab
+  routes of the Python mirror.
+* Non-convergence (pgmres.m:176-180): flag 1 with VOX_OK when the caller passes
+  an info record, VOX_ERR_NOT_CONVERGED when it cannot see the flag.
+* Admission by footprint: an operator that cannot fit is refused with
+  VOX_ERR_OOM before any device allocation.
+* Bounded waits: with a wait limit far below the work's duration, a solve
+  returns VOX_ERR_TIMEOUT with its work still queued; the context and the
+  operator stay usable once it drains.  No GPU fault is involved: the work
+  runs to completion on its own.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import voxphoton_b200 as vb
+from oracle import vie as ov
+from voxphoton_b200 import _lib
+from voxphoton_b200 import geometry as geo
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def small_bragg(periods=3):
+    return geo.bragg(periods=periods, period=320e-9, len_abs=0.32e-6, res=40e-9, M=16)
+
+
+def grid_r(p):
+    x, y, z = p.centres
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    return np.stack([X, Y, Z], axis=3)
+
+
+@pytest.fixture(scope="module")
+def case():
+    p = small_bragg()
+    G = vb.assemble_toeplitz(p.shape, p.ko, p.res)
+    Einc = geo.plane_wave(p)
+    return p, G, Einc
+
+
+def test_jvie_solve_matches_oracle(case):
+    p, G, Einc = case
+    L, M, N = p.shape
+    Je, flag, relres, it, resvec, solvert, vsol = vb.JVIE_Solver_const(
+        Einc, p.e_r, grid_r(p), p.freq, G=G, tol=1e-8, solver="G", inner_it=30, outer_it=20)
+    assert flag == 0 and relres <= 1e-8 and solvert > 0
+    fN = ov.fN_from_toeplitz(G)
+    _, Mc, idx, b = ov.jvie2_system(Einc, p.e_r, p.Gram, p.freq)
+    ones = np.ones(p.shape)
+    xr, flag_r, relres_r, it_r, resvec_r = ov.pgmres(
+        lambda v: ov.mv_AN_const(v, fN, ones, Mc, p.Gram, "notransp", idx), b, 30, 1e-8, 20)
+    assert it[1] == it_r[1] and abs(it[0] - it_r[0]) <= 1
+    Jr = np.zeros(3 * L * M * N, dtype=complex)
+    Jr[idx - 1] = xr
+    assert rel(Je.reshape(-1, order="F"), Jr) < 1e-6
+    assert rel(vsol, xr) < 1e-6
+    # zero outside the scatterer (JVIE_Solver_const.m:521-522)
+    outside = np.abs(p.e_r - 1.0) <= 1e-12
+    assert np.all(Je[outside] == 0)
+    # the fN form of the same call (circulant_nop_const layout)
+    Je2, flag2, *_ = vb.JVIE_Solver_const(Einc, p.e_r, grid_r(p), p.freq, fN=fN, tol=1e-8,
+                                          solver="G", inner_it=30, outer_it=20)
+    assert flag2 == 0 and rel(Je2, Je) < 1e-9
+
+
+@pytest.mark.parametrize("solver,prec", [("G", "c64"), ("D", "c128"), ("B", "c128")])
+def test_jvie_solver_routes_reach_the_tolerance(case, solver, prec):
+    p, G, Einc = case
+    tol = 1e-6
+    ref = vb.JVIE_Solver_const(Einc, p.e_r, grid_r(p), p.freq, G=G, tol=1e-10, solver="G",
+                               inner_it=50, outer_it=20)[0]
+    Je, flag, relres, it, resvec, solvert, vsol = vb.JVIE_Solver_const(
+        Einc, p.e_r, grid_r(p), p.freq, G=G, tol=tol, solver=solver, inner_it=30,
+        outer_it=40, max_it=400, prec=prec)
+    assert flag == 0
+    assert relres <= tol * (1.01 if solver != "B" else 1.5)
+    assert rel(Je, ref) < 1e3 * tol
+
+
+def test_jvie_solve_refuses_other_forms(case):
+    p, G, Einc = case
+    with pytest.raises(NotImplementedError):
+        vb.JVIE_Solver_const(Einc, p.e_r, grid_r(p), p.freq, G=G, form=1, solver="G")
+
+
+def test_not_converged_is_a_flag_or_a_status(case):
+    p, G, Einc = case
+    idx = p.idxS3()
+    b = vb.jvie_rhs(p.e_r, Einc, p.Gram, p.freq, idx)
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=G)
+    x, flag, relres, it, resvec = vb.pgmres(op, b, 2, 1e-12, 1)
+    assert flag == 1 and relres > 1e-12 and it == [2, 1]
+    lib = _lib.lib()
+    bre, bim = _lib.split(b)
+    xre, xim = np.empty(op.n), np.empty(op.n)
+    st = lib.vox_pgmres(op.handle, None, 0, _lib.VOX_C128, _lib.dptr(bre), _lib.dptr(bim), 2,
+                        1e-12, 1, _lib.dptr(xre), _lib.dptr(xim), None)
+    assert st == _lib.VOX_ERR_NOT_CONVERGED
+    assert b"did not reach" in lib.vox_last_error()
+    # the refined solve, with too few refinements allowed
+    st = lib.vox_solve_refined(op.handle, None, 0, _lib.dptr(bre), _lib.dptr(bim), 1e-12, 2, 1,
+                               0.0, 1, _lib.dptr(xre), _lib.dptr(xim), None)
+    assert st == _lib.VOX_ERR_NOT_CONVERGED
+    op.close()
+
+
+def test_oversized_operator_is_refused_before_allocation():
+    import torch
+    lib = _lib.lib()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    d = _lib.OpDesc()
+    # 2000 x 500 x 500 voxels: the padded circulant alone needs ~0.4 TB
+    d.L, d.M, d.N = 2000, 500, 500
+    one = np.ones(1)
+    d.G_re = _lib.dptr(one)
+    d.Mc_re = _lib.dptr(one)
+    d.idx = _lib.dptr(one)
+    d.n_idx = 1
+    d.device = 0
+    h = ctypes.c_void_p()
+    st = lib.vox_op_create(ctypes.byref(d), ctypes.byref(h))
+    assert st == _lib.VOX_ERR_OOM
+    assert b"bytes of device memory" in lib.vox_last_error()
+    free1, _ = torch.cuda.mem_get_info()
+    assert abs(free1 - free0) < 64 << 20
+
+
+def test_wait_limit_returns_timeout_and_the_operator_recovers(case):
+    import torch
+    p, G, Einc = case
+    idx = p.idxS3()
+    b = vb.jvie_rhs(p.e_r, Einc, p.Gram, p.freq, idx)
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=G)
+    lib = _lib.lib()
+    vb.pgmres(op, b, 50, 1e-8, 10)  # warm: graphs captured, arenas allocated
+    try:
+        _lib.check(lib.vox_set_wait_timeout(1e-7))
+        with pytest.raises(_lib.VoxError) as e:
+            vb.pgmres(op, b, 50, 1e-8, 10)
+        assert e.value.status == _lib.VOX_ERR_TIMEOUT
+    finally:
+        _lib.check(lib.vox_set_wait_timeout(0.0))
+    torch.cuda.synchronize()
+    assert lib.vox_get_wait_timeout() >= 1.0
+    x, flag, relres, it, resvec = vb.pgmres(op, b, 50, 1e-8, 10)
+    assert flag == 0 and relres <= 1e-8
+    op.close()

@@ -102,3 +102,46 @@ def test_transmitted_power_slice_follows_the_reference_example():
     x = 40 - int(round((0.3e-6 + 450e-9) / 20e-9))
     assert x == 2
     assert np.isclose(P, np.sum(np.abs(E[x - 1]) ** 2), rtol=1e-14)
+
+
+def test_wait_limit_setter_validates_and_defaults():
+    """The bounded-wait limit (no device work): bad values are refused, 0
+    restores the default."""
+    lib = _lib.lib()
+    assert lib.vox_set_wait_timeout(-1.0) == _lib.VOX_ERR_BAD_ARG
+    assert lib.vox_set_wait_timeout(float("nan")) == _lib.VOX_ERR_BAD_ARG
+    assert lib.vox_set_wait_timeout(12.5) == _lib.VOX_OK
+    assert lib.vox_get_wait_timeout() == 12.5
+    assert lib.vox_set_wait_timeout(0.0) == _lib.VOX_OK
+    assert lib.vox_get_wait_timeout() > 0
+
+
+def test_jvie_solve_argument_checks_need_no_device():
+    """vox_jvie_solve refuses what it does not implement (form 1, solvers other
+    than GMRES) and malformed descriptors before any device call."""
+    lib = _lib.lib()
+    L, M, N = 4, 3, 2
+    V = L * M * N
+    er = np.full(V, 2.0)
+    Einc = np.ones(3 * V)
+    G = np.zeros(6 * V)
+    out_re, out_im = np.empty(3 * V), np.empty(3 * V)
+    d = _lib.JvieDesc()
+    d.L, d.M, d.N = L, M, N
+    d.Einc_re, d.er_re, d.G_re = _lib.dptr(Einc), _lib.dptr(er), _lib.dptr(G)
+    d.dx, d.freq = 20e-9, 2.8e14
+    d.form = 1
+    st = lib.vox_jvie_solve(ctypes.byref(d), _lib.dptr(out_re), _lib.dptr(out_im), None)
+    assert st == _lib.VOX_ERR_UNSUPPORTED
+    d.form = 2
+    d.solver = b"B"
+    st = lib.vox_jvie_solve(ctypes.byref(d), _lib.dptr(out_re), _lib.dptr(out_im), None)
+    assert st == _lib.VOX_ERR_UNSUPPORTED
+    d.solver = b"G"
+    d.fN_re = _lib.dptr(G)  # both fN and G
+    st = lib.vox_jvie_solve(ctypes.byref(d), _lib.dptr(out_re), _lib.dptr(out_im), None)
+    assert st == _lib.VOX_ERR_BAD_ARG
+    d.fN_re = None
+    d.dx = 0.0
+    st = lib.vox_jvie_solve(ctypes.byref(d), _lib.dptr(out_re), _lib.dptr(out_im), None)
+    assert st == _lib.VOX_ERR_BAD_ARG

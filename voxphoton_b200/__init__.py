@@ -6,12 +6,12 @@ an FP32 + FP64-refinement solver.  See voxphoton_b200.vie for the
 MATLAB-facing calls (mv_AN_const, chan_mvp_idx, pgmres), voxphoton_b200.solvers
 for pgmresDR / bicgstab and voxphoton_b200.mor for the reduced-order sweep.
 """
-from .vie import (E_field_Nop_const, Lane, Operator, Preconditioner, assemble_toeplitz, chan_mvp_idx,
+from .vie import (E_field_Nop_const, JVIE_Solver_const, Lane, Operator, Preconditioner, assemble_toeplitz, chan_mvp_idx,
                   face3_from_Mr, jvie_rhs, mv_AN_const, mv_L_const, pgmres, singular_integrals,
                   solve_refined, solve_refined_batch, transmitted_power)
 from .solvers import bicgstab, pgmresDR
 from .mor import ReducedModel
 
-__all__ = ["E_field_Nop_const", "Lane", "transmitted_power", "Operator", "Preconditioner", "assemble_toeplitz", "chan_mvp_idx", "face3_from_Mr",
+__all__ = ["E_field_Nop_const", "JVIE_Solver_const", "Lane", "transmitted_power", "Operator", "Preconditioner", "assemble_toeplitz", "chan_mvp_idx", "face3_from_Mr",
            "jvie_rhs", "mv_AN_const", "mv_L_const", "pgmres", "singular_integrals",
            "solve_refined", "solve_refined_batch", "pgmresDR", "bicgstab", "ReducedModel"]

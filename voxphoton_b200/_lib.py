@@ -67,10 +67,34 @@ class GmresInfo(ctypes.Structure):
     ]
 
 
+class JvieDesc(ctypes.Structure):
+    _fields_ = [
+        ("L", ctypes.c_int), ("M", ctypes.c_int), ("N", ctypes.c_int),
+        ("Einc_re", _dp), ("Einc_im", _dp),
+        ("er_re", _dp), ("er_im", _dp),
+        ("dx", ctypes.c_double), ("freq", ctypes.c_double),
+        ("LfN", ctypes.c_int), ("MfN", ctypes.c_int), ("NfN", ctypes.c_int),
+        ("fN_re", _dp), ("fN_im", _dp),
+        ("G_re", _dp), ("G_im", _dp),
+        ("tol", ctypes.c_double),
+        ("form", ctypes.c_int),
+        ("solver", ctypes.c_char),
+        ("precond", ctypes.c_char),
+        ("inner_it", ctypes.c_int),
+        ("outer_it", ctypes.c_int),
+        ("prec", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
 # (name, restype, argtypes) for every entry point declared in include/vox.h
 SIGNATURES = [
     ("vox_last_error", ctypes.c_char_p, []),
     ("vox_abi_version", ctypes.c_int, []),
+    ("vox_set_wait_timeout", ctypes.c_int, [ctypes.c_double]),
+    ("vox_get_wait_timeout", ctypes.c_double, []),
+    ("vox_jvie_solve", ctypes.c_int, [ctypes.POINTER(JvieDesc), _dp, _dp,
+                                      ctypes.POINTER(GmresInfo)]),
     ("vox_op_create", ctypes.c_int, [ctypes.POINTER(OpDesc), ctypes.POINTER(ctypes.c_void_p)]),
     ("vox_op_destroy", None, [ctypes.c_void_p]),
     ("vox_op_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstddef>
@@ -15,10 +16,12 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
 #include "../../include/vox.h"
+#include "bulk.cuh"
 #include "krylov.cuh"
 #include "mvp.cuh"
 #include "precond.cuh"
@@ -129,6 +132,87 @@ struct DeviceGuard {
     vox_status s__ = (x);           \
     if (s__ != VOX_OK) return s__;  \
   } while (0)
+
+// ------------------------------------------------------------ bounded waits
+// Every host wait on the device polls the stream against a deadline instead of
+// blocking in cudaStreamSynchronize: a wait that outlasts the limit returns
+// VOX_ERR_TIMEOUT (the work stays queued and the context stays usable; the
+// caller decides whether to wait again or tear down).  The limit is
+// process-wide: VOX_WAIT_TIMEOUT_S in the environment, or vox_set_wait_timeout.
+static std::atomic<double> g_wait_limit_s{-1.0};
+
+static double wait_limit_s() {
+  double v = g_wait_limit_s.load();
+  if (v > 0) return v;
+  const char* e = std::getenv("VOX_WAIT_TIMEOUT_S");
+  v = (e && std::atof(e) > 0) ? std::atof(e) : 600.0;
+  g_wait_limit_s.store(v);
+  return v;
+}
+
+// The module's kernel error word (a bounded in-kernel wait gave up), read
+// after the stream it was left on has drained; cleared once reported.
+static vox_status kernel_err_status(cudaStream_t st) {
+  // a device-to-pageable copy returns once it has landed (the stream is idle)
+  int h = 0;
+  VOX_CUDA(cudaMemcpyFromSymbolAsync(&h, g_kernel_err, sizeof(int), 0, cudaMemcpyDeviceToHost,
+                                     st));
+  if (h != 0) {
+    const int zero = 0;
+    VOX_CUDA(cudaMemcpyToSymbolAsync(g_kernel_err, &zero, sizeof(int), 0,
+                                     cudaMemcpyHostToDevice, st));
+    set_error("a kernel's bounded pipeline wait gave up (error word " + std::to_string(h) +
+              "); its results are invalid");
+    return VOX_ERR_TIMEOUT;
+  }
+  return VOX_OK;
+}
+
+static vox_status wait_stream(cudaStream_t st) {
+  const double lim = wait_limit_s();
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int spin = 0;; spin++) {
+    const cudaError_t e = cudaStreamQuery(st);
+    if (e == cudaSuccess) return kernel_err_status(st);
+    if (e != cudaErrorNotReady) {
+      cudaGetLastError();
+      set_error(std::string("stream wait: ") + cudaGetErrorString(e));
+      return VOX_ERR_CUDA;
+    }
+    const double dt =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (dt > lim) {
+      set_error("device work did not finish within the wait limit of " + std::to_string(lim) +
+                " s (VOX_WAIT_TIMEOUT_S / vox_set_wait_timeout); it is still queued");
+      return VOX_ERR_TIMEOUT;
+    }
+    // spin briefly (short restart cycles), then back off to a light poll
+    if (spin > 64) std::this_thread::sleep_for(std::chrono::microseconds(spin < 2000 ? 20 : 200));
+  }
+}
+
+// The same for one recorded event.
+static vox_status wait_event(cudaEvent_t ev) {
+  const double lim = wait_limit_s();
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int spin = 0;; spin++) {
+    const cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaSuccess) return VOX_OK;
+    if (e != cudaErrorNotReady) {
+      cudaGetLastError();
+      set_error(std::string("event wait: ") + cudaGetErrorString(e));
+      return VOX_ERR_CUDA;
+    }
+    const double dt =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (dt > lim) {
+      set_error("device work did not finish within the wait limit of " + std::to_string(lim) +
+                " s; it is still queued");
+      return VOX_ERR_TIMEOUT;
+    }
+    if (spin > 64) std::this_thread::sleep_for(std::chrono::microseconds(spin < 2000 ? 20 : 200));
+  }
+}
 
 // Bytes of a GmresDev record read back per cycle (everything before sn).
 constexpr size_t kGmresHdr = (offsetof(GmresDev, sn) + 15) / 16 * 16;
@@ -397,7 +481,7 @@ static vox_status fft_axis_d(double2* data, int d0, int d1, int d2, long long s0
   dim3 grid(tilesA * a.d[a.axB], ncomp);
   k_fft_axis<double><<<grid, 256, smem, st>>>(a, p, dtw, sign, data);
   VOX_CUDA(cudaGetLastError());
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   cudaFree(dtw);
   return VOX_OK;
 }
@@ -444,7 +528,7 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
   VOX_TRY(dalloc(&b.Mc, g.V));
   VOX_CUDA(cudaMemcpyAsync(tmp, Mc.data(), g.V * sizeof(double2), cudaMemcpyHostToDevice, st));
   k_to_prec<R><<<nblk(g.V), 256, 0, st>>>(g.V, tmp, 1.0, b.Mc);
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   cudaFree(tmp);
   auto up_tw = [&](int n, Cx<R>** dst) -> vox_status {
     std::vector<double2> w = twiddles(n);
@@ -486,6 +570,8 @@ static void lanes_release(vox_op_s* op);
 static void destroy_op(vox_op_s* op) {
   if (!op) return;
   DeviceGuard dg(op->device);
+  // teardown waits without a limit: freeing memory under queued kernels would
+  // fault the context
   cudaDeviceSynchronize();
   // lanes and preconditioners use the operator's state: they go with it
   lanes_release(op);
@@ -515,6 +601,18 @@ extern "C" {
 
 const char* vox_last_error(void) { return vox::last_error(); }
 int vox_abi_version(void) { return VOX_ABI_VERSION; }
+
+vox_status vox_set_wait_timeout(double seconds) {
+  if (!(seconds >= 0) || seconds > 1e7) {
+    vox::set_error("vox_set_wait_timeout: seconds must be in [0, 1e7]");
+    return VOX_ERR_BAD_ARG;
+  }
+  // 0 returns to the default (VOX_WAIT_TIMEOUT_S or 600 s), read on next use
+  vox::g_wait_limit_s.store(seconds > 0 ? seconds : -1.0);
+  return VOX_OK;
+}
+
+double vox_get_wait_timeout(void) { return vox::wait_limit_s(); }
 
 static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out);
 
@@ -588,6 +686,21 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
     set_error("vox_op_create: no FFT plan for the padded grid");
     return VOX_ERR_UNSUPPORTED;
   }
+  // admission by footprint, before any input array is read or device memory
+  // allocated: the FP64 padded circulant built at setup (6 P complex128) plus
+  // the index map must fit in the device's free memory
+  {
+    const double P = (double)g.Px * g.Py * g.Pz;
+    const double need = 6.0 * P * sizeof(double2) + 12.0 * (double)V;
+    size_t free_b = 0, total_b = 0;
+    VOX_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (need > (double)free_b) {
+      set_error("vox_op_create: the operator needs at least " + std::to_string((long long)need) +
+                " bytes of device memory at setup; " + std::to_string((long long)free_b) +
+                " are free");
+      return VOX_ERR_OOM;
+    }
+  }
   op->gram = desc->gram;
   // index map
   {
@@ -634,7 +747,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
                              st));
     k_embed_from_toeplitz<<<nblk(6 * P), 256, 0, st>>>(g, dG, emb);
     VOX_CUDA(cudaGetLastError());
-    VOX_CUDA(cudaStreamSynchronize(st));
+    VOX_TRY(wait_stream(st));
     cudaFree(dG);
   } else {
     const int L2 = 2 * L, M2 = 2 * M, N2 = 2 * N;
@@ -653,7 +766,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
     k_to_prec<double><<<nblk(6 * Q), 256, 0, st>>>(6 * Q, dF, 1.0 / (double)Q, dF);
     k_embed_from_circ<<<nblk(6 * P), 256, 0, st>>>(g, dF, emb);
     VOX_CUDA(cudaGetLastError());
-    VOX_CUDA(cudaStreamSynchronize(st));
+    VOX_TRY(wait_stream(st));
   }
   // forward 3-D FFT of the padded circulant: z stride 1, y Pz, x Py*Pz
   for (int ax = 0; ax < 3; ax++)
@@ -667,7 +780,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
     k_sym_defect<<<nblk(6 * P), 256, 0, st>>>(g, emb, dd);
     unsigned hv[2];
     VOX_CUDA(cudaMemcpyAsync(hv, dd, sizeof(hv), cudaMemcpyDeviceToHost, st));
-    VOX_CUDA(cudaStreamSynchronize(st));
+    VOX_TRY(wait_stream(st));
     float defect, fmax;
     std::memcpy(&defect, &hv[0], 4);
     std::memcpy(&fmax, &hv[1], 4);
@@ -706,7 +819,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
   VOX_TRY(dalloc(&op->d_out, K * n));
   VOX_TRY(dalloc(&op->f_in, n));
   VOX_TRY(dalloc(&op->f_out, n));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   *out = op.release();
   return VOX_OK;
 }
@@ -789,7 +902,7 @@ static vox_status mv_host(vox_op_s* op, int mode, vox_prec prec, const double* i
     k_to_d2<float><<<nblk(n), 256, 0, st>>>(n, op->f_out, op->gram, op->d_out);
   }
   VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   d2_to_split(op->h_out, n, out_re, out_im);
   return VOX_OK;
 }
@@ -947,7 +1060,7 @@ vox_status vox_assemble_toeplitz_device(int L, int M, int N, double ko, double d
     VOX_CUDA(cudaMemcpyAsync(In[m], c.Ipair + cell * 21, 21 * sizeof(double2),
                              cudaMemcpyDeviceToHost, st));
   }
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   for (long long i = 0; i < V * 6; i++) {
     const long long cell = i % V;
     const int mx = (int)(cell % L), my = (int)((cell / L) % M), mz = (int)(cell / ((long long)L * M));
@@ -990,6 +1103,7 @@ vox_status vox_block_update(long long n, int a, int b, const void* X, long long 
 
 #include "solver.cuh"
 #include "lane.cuh"
+#include "jvie.cuh"
 
 namespace vox {
 static void lanes_release(vox_op_s* op) {

@@ -108,7 +108,7 @@ static vox_status lane_start_inner(vox_lane_s* L, const std::vector<int>& S) {
   for (int b : S)
     VOX_CUDA(cudaMemcpyAsync(&wf.hscal[b], &wf.st[b].scal[1], sizeof(double),
                              cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   for (int b : S) {
     vox_lane_s::Member& mb = L->m[b];
     mb.ibn = std::sqrt(wf.hscal[b]);
@@ -152,7 +152,7 @@ static vox_status lane_refine(vox_lane_s* L, const std::vector<int>& R, std::vec
   for (int b : R)
     VOX_CUDA(cudaMemcpyAsync(&wd.hscal[b], &wd.st[b].scal[2], sizeof(double),
                              cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   for (int b : R) {
     vox_lane_s::Member& mb = L->m[b];
     mb.rel = std::sqrt(wd.hscal[b]) / mb.bn;
@@ -201,7 +201,7 @@ static vox_status lane_submit(vox_lane_s* L, int b, const double2* bdev, double2
   op->launches += 1;
   VOX_CUDA(cudaMemcpyAsync(&wd.hscal[b], &wd.st[b].scal[3], sizeof(double),
                            cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   mb.bn = std::sqrt(wd.hscal[b]);
   mb.rel = 1.0;
   if (mb.bn == 0.0 || mb.rel <= L->tol) {
@@ -241,7 +241,7 @@ static vox_status lane_step(vox_lane_s* L, int* done, int* n_done) {
       if (L->m[b].state == 1 && L->m[b].inner)
         VOX_CUDA(cudaMemcpyAsync(wf.hdr(b), &wf.st[b], offsetof(GmresDev, sn),
                                  cudaMemcpyDeviceToHost, st));
-    VOX_CUDA(cudaStreamSynchronize(st));
+    VOX_TRY(wait_stream(st));
     for (int b = 0; b < K; b++) {
       vox_lane_s::Member& mb = L->m[b];
       if (mb.state != 1 || !mb.inner) continue;
@@ -314,7 +314,7 @@ vox_status vox_lane_create(vox_op_t op, vox_precond_t pc, int side, double tol, 
   L->m.resize(op->K);
   // every member frozen until it takes a right-hand side
   for (int b = 0; b < op->K; b++) VOX_TRY(lane_header(L.get(), b, 0.0, 1));
-  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  VOX_TRY(wait_stream(op->stream));
   if (use_cycle_graphs()) {
     cudaGraphExec_t cyc = nullptr;
     VOX_TRY(get_cycle_graph<float>(op, pc, L->side, op->K, &cyc));
@@ -386,7 +386,7 @@ vox_status vox_lane_collect(vox_lane_t lane, int member, double* x_re, double* x
     double2* hx = op->h_out + member * n;
     VOX_CUDA(cudaMemcpyAsync(hx, mb.x, n * sizeof(double2), cudaMemcpyDeviceToHost,
                              op->stream));
-    VOX_CUDA(cudaStreamSynchronize(op->stream));
+    VOX_TRY(wait_stream(op->stream));
     d2_to_split(hx, n, x_re, x_im);
   }
   if (info) {

@@ -410,7 +410,7 @@ static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector
   VOX_CUDA(cudaGetLastError());
   std::vector<int> info(Lf);
   VOX_CUDA(cudaMemcpyAsync(info.data(), dinfo, Lf * sizeof(int), cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   for (int i = 0; i < Lf; i++)
     if (info[i]) {
       set_error("level-1 preconditioner: block " + std::to_string(i) + " is singular");
@@ -441,7 +441,7 @@ static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector
     k_cast_scale<float><<<nblk(Lf * perp), 256, 0, st>>>(Lf * perp, p->Ad, op->gram, p->Af);
     VOX_CUDA(cudaGetLastError());
   }
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   cudaFree(p->tiles_d);
   cudaFree(p->Dld);
   cudaFree(p->Dud);
@@ -510,7 +510,7 @@ static vox_status build_level2(vox_op_s* op, vox_precond_s* p, const std::vector
   VOX_CUDA(cudaGetLastError());
   std::vector<int> info(nblocks);
   VOX_CUDA(cudaMemcpyAsync(info.data(), dinfo, nblocks * sizeof(int), cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   for (long long i = 0; i < nblocks; i++)
     if (info[i]) {
       set_error("level-2 preconditioner: block " + std::to_string(i) + " is singular");
@@ -523,7 +523,7 @@ static vox_status build_level2(vox_op_s* op, vox_precond_s* p, const std::vector
     k_cast_scale<float><<<nblk(tot), 256, 0, st>>>(tot, p->Ad, op->gram, p->Af);
   }
   VOX_CUDA(cudaGetLastError());
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   p->kind = 1;
   p->Lf = g.L;
   p->paired = 0;
@@ -592,7 +592,7 @@ vox_status vox_precond_create_box(vox_op_t op, int level, int x0, int y0, int Ls
     k_vmap_box<<<nblk(3 * Vs), 256, 0, op->stream>>>(op->g.L, op->g.M, Ns, x0, y0, Ls, Ms,
                                                      op->vmap, dmask, vm);
     VOX_CUDA(cudaGetLastError());
-    VOX_CUDA(cudaStreamSynchronize(op->stream));
+    VOX_TRY(wait_stream(op->stream));
     cudaFree(dmask);
   }
   VOX_TRY(pc_common(op, p.get(), Ls, Ms, Ns, level == 1));
@@ -678,7 +678,7 @@ vox_status vox_precond_create_blocks(vox_op_t op, const double* blk_re, const do
     k_cast_scale<float><<<nblk(tot), 256, 0, op->stream>>>(tot, p->Ad, op->gram, p->Af);
     VOX_CUDA(cudaGetLastError());
   }
-  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  VOX_TRY(wait_stream(op->stream));
   pc_seal(p.get());
   op->pcs.push_back(p.get());
   *out = p.release();
@@ -699,6 +699,7 @@ namespace vox {
 static void pc_release(vox_precond_s* p) {
   vox_op_s* op = p->op;
   DeviceGuard dg(op->device);
+  // teardown waits without a limit (freeing under queued kernels would fault)
   cudaDeviceSynchronize();
   op->pcs.erase(std::remove(op->pcs.begin(), op->pcs.end(), p), op->pcs.end());
   // drop cached GMRES graphs that captured this preconditioner
@@ -746,7 +747,7 @@ vox_status vox_precond_apply(vox_precond_t p, vox_prec prec, const double* in_re
     k_to_d2<float><<<nblk(n), 256, 0, st>>>(n, op->f_out, 1.0 / p->f_scale, op->d_out);
   }
   VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   d2_to_split(op->h_out, n, out_re, out_im);
   return VOX_OK;
 }
@@ -772,7 +773,7 @@ template <typename R>
 static vox_status ensure_work(vox_op_s* op, int m) {
   GmresWork<R>& w = work<R>(op);
   if (w.m == m && w.arena) return VOX_OK;
-  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  VOX_TRY(wait_stream(op->stream));
   w.release();
   const long long n = op->g.n;
   const int K = op->K;
@@ -920,7 +921,7 @@ static vox_status read_scals(vox_op_s* op, int slot, int km, const char* use, do
     if (!use || use[b])
       VOX_CUDA(cudaMemcpyAsync(&w.hscal[b], &w.st[b].scal[slot], sizeof(double),
                                cudaMemcpyDeviceToHost, op->stream));
-  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  VOX_TRY(wait_stream(op->stream));
   for (int b = 0; b < km; b++)
     if (!use || use[b]) v[b] = w.hscal[b];
   return VOX_OK;
@@ -984,7 +985,7 @@ static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, int km, 
     h->frozen = active[b] ? 0 : 1;
     // reset the header fields (everything before resvec) of the member's state
     VOX_CUDA(cudaMemcpyAsync(&w.st[b], hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
-    VOX_CUDA(cudaStreamSynchronize(st));
+    VOX_TRY(wait_stream(st));
   }
   cudaGraphExec_t cyc = nullptr;
   if (use_cycle_graphs()) VOX_TRY(get_cycle_graph<R>(op, pc, side, km, &cyc));
@@ -1006,7 +1007,7 @@ static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, int km, 
       if (active[b])
         VOX_CUDA(cudaMemcpyAsync(w.hdr(b), &w.st[b], offsetof(GmresDev, sn),
                                  cudaMemcpyDeviceToHost, st));
-    VOX_CUDA(cudaStreamSynchronize(st));
+    VOX_TRY(wait_stream(st));
     for (int b = 0; b < km; b++) {
       if (!active[b]) continue;
       const GmresDev* hb = w.hdr(b);
@@ -1086,7 +1087,7 @@ static vox_status pgmres_entry(vox_op_s* op, vox_precond_s* pc, int side, const 
   info->flag = relres <= tol ? 0 : 1;
   k_to_d2<R><<<nblk(n), 256, 0, st>>>(n, w.x, 1.0, x_dev);
   op->launches += 2;
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   fill_resvec(info, rv);
   return VOX_OK;
 }
@@ -1239,6 +1240,18 @@ static vox_status refined_entry(vox_op_s* op, vox_precond_s* pc, int side, const
 
 }  // namespace vox
 
+// pgmres.m:176-180 reports non-convergence as flag = 1, not as an error, and so
+// do the solver entry points when the caller passes an info record.  A caller
+// that passes none cannot see the flag, so it gets VOX_ERR_NOT_CONVERGED.
+static vox_status flag_status(vox_status s, bool caller_info, const vox_gmres_info& inf) {
+  if (s == VOX_OK && !caller_info && inf.flag != 0) {
+    set_error("the solve did not reach the tolerance (relres " + std::to_string(inf.relres) +
+              "); pass a vox_gmres_info to receive flag = 1 instead of this status");
+    return VOX_ERR_NOT_CONVERGED;
+  }
+  return s;
+}
+
 extern "C" {
 
 vox_status vox_pgmres_device(vox_op_t op, vox_precond_t pc, int side, vox_prec prec,
@@ -1251,6 +1264,7 @@ vox_status vox_pgmres_device(vox_op_t op, vox_precond_t pc, int side, vox_prec p
   VOX_TRY(check_prec(op, prec));
   DeviceGuard dg(op->device);
   vox_gmres_info local{};
+  const bool given = info != nullptr;
   if (!info) info = &local;
   auto t0 = std::chrono::steady_clock::now();
   vox_status s = prec == VOX_C128
@@ -1259,7 +1273,7 @@ vox_status vox_pgmres_device(vox_op_t op, vox_precond_t pc, int side, vox_prec p
                      : pgmres_entry<float>(op, pc, side, (const double2*)b, restart, tol, maxit,
                                            (double2*)x, info);
   info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  return s;
+  return flag_status(s, given, *info);
 }
 
 vox_status vox_solve_refined_device(vox_op_t op, vox_precond_t pc, int side, const void* b,
@@ -1271,12 +1285,13 @@ vox_status vox_solve_refined_device(vox_op_t op, vox_precond_t pc, int side, con
   }
   DeviceGuard dg(op->device);
   vox_gmres_info local{};
+  const bool given = info != nullptr;
   if (!info) info = &local;
   auto t0 = std::chrono::steady_clock::now();
   vox_status s = refined_entry(op, pc, side, (const double2*)b, tol, restart, maxit_inner,
                                inner_tol, max_refine, (double2*)x, info);
   info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  return s;
+  return flag_status(s, given, *info);
 }
 
 static vox_status host_solve(vox_op_t op, const double* b_re, const double* b_im, double* x_re,
@@ -1294,7 +1309,7 @@ static vox_status host_solve(vox_op_t op, const double* b_re, const double* b_im
   VOX_CUDA(cudaMemcpyAsync(op->d_in, op->h_in, n * sizeof(double2), cudaMemcpyHostToDevice, st));
   VOX_TRY(fn(op->d_in, op->d_out));
   VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   d2_to_split(op->h_out, n, x_re, x_im);
   if (info)
     info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1310,10 +1325,14 @@ vox_status vox_pgmres(vox_op_t op, vox_precond_t pc, int side, vox_prec prec, co
   }
   vox_gmres_info local{};
   vox_gmres_info* inf = info ? info : &local;
-  return host_solve(op, b_re, b_im, x_re, x_im, inf, [&](const double2* b, double2* x) {
-    return prec == VOX_C128 ? pgmres_entry<double>(op, pc, side, b, restart, tol, maxit, x, inf)
-                            : pgmres_entry<float>(op, pc, side, b, restart, tol, maxit, x, inf);
-  });
+  return flag_status(
+      host_solve(op, b_re, b_im, x_re, x_im, inf,
+                 [&](const double2* b, double2* x) {
+                   return prec == VOX_C128
+                              ? pgmres_entry<double>(op, pc, side, b, restart, tol, maxit, x, inf)
+                              : pgmres_entry<float>(op, pc, side, b, restart, tol, maxit, x, inf);
+                 }),
+      info != nullptr, *inf);
 }
 
 vox_status vox_solve_refined(vox_op_t op, vox_precond_t pc, int side, const double* b_re,
@@ -1322,10 +1341,12 @@ vox_status vox_solve_refined(vox_op_t op, vox_precond_t pc, int side, const doub
                              vox_gmres_info* info) {
   vox_gmres_info local{};
   vox_gmres_info* inf = info ? info : &local;
-  return host_solve(op, b_re, b_im, x_re, x_im, inf, [&](const double2* b, double2* x) {
-    return refined_entry(op, pc, side, b, tol, restart, maxit_inner, inner_tol, max_refine, x,
-                         inf);
-  });
+  return flag_status(host_solve(op, b_re, b_im, x_re, x_im, inf,
+                                [&](const double2* b, double2* x) {
+                                  return refined_entry(op, pc, side, b, tol, restart, maxit_inner,
+                                                       inner_tol, max_refine, x, inf);
+                                }),
+                     info != nullptr, *inf);
 }
 
 vox_status vox_jvie_rhs(int L, int M, int N, const double* er_re, const double* er_im,
@@ -1396,7 +1417,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     VOX_CUDA(cudaEventRecord(e0, st));
     for (int r = 0; r < reps; r++) launch();
     VOX_CUDA(cudaEventRecord(e1, st));
-    VOX_CUDA(cudaEventSynchronize(e1));
+    VOX_TRY(wait_event(e1));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     return ms / reps;
@@ -1467,7 +1488,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     init->tol_abs = -1.0;
     for (int mb = 0; mb < km; mb++)
       VOX_CUDA(cudaMemcpyAsync(&w.st[mb], hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
-    VOX_CUDA(cudaStreamSynchronize(st));
+    VOX_TRY(wait_stream(st));
   }
   out[6] = timeit([&] {
     k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
@@ -1482,7 +1503,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     VOX_CUDA(cudaEventRecord(e0, st));
     k_gs_update_norm<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
     VOX_CUDA(cudaEventRecord(e1, st));
-    VOX_CUDA(cudaEventSynchronize(e1));
+    VOX_TRY(wait_event(e1));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     if (r > 0) tn += ms;
@@ -1496,7 +1517,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   VOX_CUDA(cudaGetLastError());
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   return VOX_OK;
 }
 
@@ -1690,7 +1711,7 @@ vox_status vox_solve_refined_batch_device(vox_op_t op, vox_precond_t pc, int sid
   auto t0 = std::chrono::steady_clock::now();
   VOX_TRY(refined_run(op, pc, side, count, (const double2*)b, tol, restart, maxit_inner,
                       inner_tol, max_refine, (double2*)x, ip.data()));
-  VOX_CUDA(cudaStreamSynchronize(op->stream));
+  VOX_TRY(wait_stream(op->stream));
   const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   for (int i = 0; i < count; i++) infos[i].seconds = sec;
   return VOX_OK;
@@ -1722,7 +1743,7 @@ vox_status vox_solve_refined_batch(vox_op_t op, vox_precond_t pc, int side, int 
                       max_refine, op->d_out, ip.data()));
   VOX_CUDA(cudaMemcpyAsync(op->h_out, op->d_out, count * n * sizeof(double2),
                            cudaMemcpyDeviceToHost, st));
-  VOX_CUDA(cudaStreamSynchronize(st));
+  VOX_TRY(wait_stream(st));
   d2_to_split(op->h_out, count * n, x_re, x_im);
   const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   for (int i = 0; i < count; i++) infos[i].seconds = sec;

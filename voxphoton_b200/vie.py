@@ -576,3 +576,101 @@ def singular_integrals(ko, dx, order=32):
     out = np.empty(10)
     check(lib().vox_singular_integrals(float(ko), float(dx), int(order), dptr(out)))
     return tuple(out[0::2] + 1j * out[1::2])
+
+
+def JVIE_Solver_const(Einc, e_r, r, freq, fN=None, tol=None, form=None, solver=None,
+                      precond=None, max_it=None, inner_it=None, outer_it=None, ritz=None,
+                      gpu_flag=None, logfile=None, G=None, prec="c128"):
+    """[Je, flag, relres, iter, resvec, solvert, vsol] = JVIE_Solver_const(Einc, e_r, r,
+    freq, fN, tol, form, solver, precond, max_it, inner_it, outer_it, ritz, gpu_flag,
+    logfile) (JVIE_Solver_const.m:1-535) on the device.
+
+    Einc: L x M x N x 3, e_r: L x M x N, r: the voxel centres (L x M x N x 3; the
+    voxel edge is r(1,1,2,3) - r(1,1,1,3), as :140), fN the N operator (or
+    ``G=`` its Toeplitz tensor).  Defaults and clamps as the reference: tol 1e-3,
+    form 2, solver 'B' (BiCGStab), max_it 1000, inner_it 50, outer_it 200, ritz 5.
+    solver 'G' runs vox_jvie_solve (restarted GMRES; ``prec="c64"`` gives the
+    complex64 + FP64-refinement solve); 'D' runs pgmresDR and 'B' bicgstab
+    (voxphoton_b200.solvers) on an operator built the same way.  Only form 2
+    (JVIE-II) is implemented; its preconditioner fP = Gram * I leaves GMRES's
+    iterates unchanged, so 'L' / 'R' solve unpreconditioned.  gpu_flag selects
+    the device (ordinal gpu_flag - 1; 0 is refused: there is no CPU path);
+    logfile is accepted and ignored."""
+    import time as _time
+    Einc = np.asarray(Einc)
+    e_r = np.asarray(e_r)
+    L, M, N = e_r.shape
+    tol = 1e-3 if (tol is None or tol < 1e-15 or tol >= 1) else float(tol)
+    form = 2 if form is None else int(form)
+    solver = "B" if solver is None else solver
+    if solver not in ("G", "D"):
+        solver = "B"
+    if precond not in ("L", "R"):
+        precond = None
+    max_it = 1000 if max_it is None else int(max_it)
+    inner_it = 50 if (inner_it is None or inner_it < 1) else int(inner_it)
+    outer_it = 200 if (outer_it is None or outer_it < 1) else int(outer_it)
+    ritz = 5 if (ritz is None or ritz < 1) else int(ritz)
+    gpu_flag = 1 if gpu_flag is None else int(gpu_flag)
+    if gpu_flag < 1:
+        raise ValueError("gpu_flag 0 asks for the CPU path, which this library does not have")
+    device = gpu_flag - 1
+    if form != 2:
+        raise NotImplementedError("only the JVIE-II formulation (form 2) is implemented")
+    if (fN is None) == (G is None):
+        raise ValueError("give exactly one of fN or G")
+    r = np.asarray(r)
+    dx = float(r[0, 0, 1, 2] - r[0, 0, 0, 2])
+    Gram = dx ** 3
+    t0 = _time.perf_counter()
+    V = L * M * N
+    idx = np.flatnonzero(np.abs(fortran_flat(e_r) - 1.0) > 1e-12) + 1
+    idx3 = np.concatenate([idx, V + idx, 2 * V + idx])
+    if solver == "G":
+        d = _lib.JvieDesc()
+        d.L, d.M, d.N = L, M, N
+        e_re, e_im = split(fortran_flat(Einc))
+        r_re, r_im = split(fortran_flat(e_r))
+        d.Einc_re, d.Einc_im, d.er_re, d.er_im = dptr(e_re), dptr(e_im), dptr(r_re), dptr(r_im)
+        d.dx, d.freq = dx, float(freq)
+        if fN is not None:
+            fN = np.asarray(fN)
+            d.LfN, d.MfN, d.NfN = fN.shape[:3]
+            f_re, f_im = split(fortran_flat(fN))
+            d.fN_re, d.fN_im = dptr(f_re), dptr(f_im)
+        else:
+            f_re, f_im = split(fortran_flat(np.asarray(G)))
+            d.G_re, d.G_im = dptr(f_re), dptr(f_im)
+        d.tol = tol
+        d.form = 2
+        d.solver = b"G"
+        d.precond = precond.encode() if precond else b"\0"
+        d.inner_it, d.outer_it = inner_it, outer_it
+        d.prec = _lib.PREC[prec]
+        d.device = device
+        info, buf = _info(inner_it * outer_it * 10 + 11)
+        Je_re = np.empty(3 * V)
+        Je_im = np.empty(3 * V)
+        check(lib().vox_jvie_solve(ctypes.byref(d), dptr(Je_re), dptr(Je_im), ctypes.byref(info)))
+        del e_re, e_im, r_re, r_im, f_re, f_im
+        Je = (Je_re + 1j * Je_im).reshape((L, M, N, 3), order="F")
+        resvec = buf[:min(info.n_resvec, buf.size)].copy()
+        vsol = Je.reshape(-1, order="F")[idx3 - 1]
+        return (Je, info.flag, info.relres, [info.iter_inner, info.iter_outer], resvec,
+                _time.perf_counter() - t0, vsol)
+    # GMRES-DR / BiCGStab on an operator built as :133-157, 243-251
+    from .solvers import bicgstab, pgmresDR
+    b = jvie_rhs(e_r, Einc, Gram, freq, idx3)
+    op = Operator((e_r - 1.0) / e_r, Gram, idx3, fN=fN, G=G, precisions=("c128",),
+                  device=device)
+    try:
+        if solver == "D":
+            x, flag, relres, it, resvec = pgmresDR(op, b, inner_it, tol, outer_it, ritz)
+        else:
+            x, flag, relres, it, resvec = bicgstab(op, b, tol, max_it)
+    finally:
+        op.close()
+    Je = np.zeros(3 * V, dtype=complex)
+    Je[idx3 - 1] = x
+    return (Je.reshape((L, M, N, 3), order="F"), flag, relres, it, resvec,
+            _time.perf_counter() - t0, x)
