@@ -170,11 +170,15 @@ vox_status vox_mv_AN_device(vox_op_t op, int transp, vox_prec prec, const void* 
  * No counterpart in the reference.  The two plane intermediates live in a
  * fixed 64 MiB device array inside libvox (held by every GPU that loads the
  * library until exit), so operators needing more than 64 MiB of intermediates
- * (2 * Px * 3MN complex values) are rejected with VOX_ERR_BAD_ARG.  The first
- * call on a device looks up the array's device address; make that call before
- * any stream capture.  Every call shares the array: calls that overlap on the
- * GPU (different streams or threads) race.  Each call overwrites what it reads,
- * so nothing carries over from the previous call. */
+ * (2 * Px * 3MN complex values) are rejected with VOX_ERR_BAD_ARG, and so are
+ * operators whose planes are too tall for shared memory (split plane kernels,
+ * which need a third intermediate).  The first call on a device looks up the
+ * array's device address and keeps it for the life of that device's primary
+ * context (do not call it again after cudaDeviceReset in the same process);
+ * make that first call before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU (different streams or threads) race.
+ * Each call overwrites what it reads, so nothing carries over from the
+ * previous call. */
 vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, const void* in, void* out,
                              void* stream);
 /* count products of a batched operator in one launch: member m multiplies

@@ -4,8 +4,9 @@ It is meant for callers that cannot call cudaMalloc where they need the
 product (an external memory manager owns all device memory, or allocation is
 forbidden in that region).  The test calls it through the C-ABI on device
 buffers and checks it against the existing vox_mv_AN_device on two calls in a
-row, in both precisions, and that an operator whose intermediates exceed the
-fixed 64 MiB array is refused.  This file is collected last on purpose.
+row, in both precisions and both products (A and A'), once on a caller's
+stream, and that an operator whose intermediates exceed the fixed 64 MiB
+array is refused.  This file is collected last on purpose.
 """
 import ctypes
 
@@ -30,16 +31,18 @@ def _op(shape, seed):
     return vb.Operator(Mc, 0.8, idx, G=G)
 
 
-def _call(fn, op, prec, x, y):
+def _call(fn, op, prec, x, y, transp=0, stream=None):
     import torch
     torch.cuda.synchronize()
-    _lib.check(fn(op.handle, 0, _lib.PREC[prec], ctypes.c_void_p(x.data_ptr()),
-                  ctypes.c_void_p(y.data_ptr()), None))
+    _lib.check(fn(op.handle, transp, _lib.PREC[prec], ctypes.c_void_p(x.data_ptr()),
+                  ctypes.c_void_p(y.data_ptr()),
+                  None if stream is None else ctypes.c_void_p(stream.cuda_stream)))
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("transp", [0, 1])
 @pytest.mark.parametrize("prec", ["c128", "c64"])
-def test_noalloc_matches_device_entry_point_twice(prec):
+def test_noalloc_matches_device_entry_point_twice(prec, transp):
     import torch
     op = _op((20, 9, 6), 0)
     lib = _lib.lib()
@@ -49,10 +52,27 @@ def test_noalloc_matches_device_entry_point_twice(prec):
         x = torch.randn(op.n, dtype=dt, device="cuda", generator=g)
         ref = torch.empty_like(x)
         out = torch.full_like(x, float("nan"))
-        _call(lib.vox_mv_AN_device, op, prec, x, ref)
-        _call(lib.vox_mv_AN_noalloc, op, prec, x, out)
+        _call(lib.vox_mv_AN_device, op, prec, x, ref, transp)
+        _call(lib.vox_mv_AN_noalloc, op, prec, x, out, transp)
         err = (torch.linalg.vector_norm(out - ref) / torch.linalg.vector_norm(ref)).item()
         assert err < TOL[prec], err
+    op.close()
+
+
+def test_noalloc_on_a_caller_stream():
+    """The product enqueued on a non-default torch stream passed as the stream
+    argument equals the device entry point's."""
+    import torch
+    op = _op((20, 9, 6), 2)
+    lib = _lib.lib()
+    x = torch.randn(op.n, dtype=torch.complex64, device="cuda")
+    ref = torch.empty_like(x)
+    out = torch.full_like(x, float("nan"))
+    s = torch.cuda.Stream()
+    _call(lib.vox_mv_AN_device, op, "c64", x, ref)
+    _call(lib.vox_mv_AN_noalloc, op, "c64", x, out, 0, s)
+    err = (torch.linalg.vector_norm(out - ref) / torch.linalg.vector_norm(ref)).item()
+    assert err < TOL["c64"], err
     op.close()
 
 

@@ -331,18 +331,31 @@ struct Members {
   int fs = 0;
 };
 
+// Plane intermediates supplied by the caller instead of the operator's own
+// (one member, unsplit kernel 2 only: vox_mv_AN_noalloc).
+template <typename R>
+struct PlaneScratch {
+  Cx<R>* T1 = nullptr;
+  Cx<R>* T2 = nullptr;
+};
+
 // Launch the three matvec kernels.
 template <typename R>
 static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cudaStream_t st,
-                         const int* skip, Members mm = Members()) {
+                         const int* skip, Members mm = Members(),
+                         PlaneScratch<R> scratch = PlaneScratch<R>()) {
   OpBuffers<R>& b = bufs<R>(op);
   const OpGeom& g = b.geo;
   const size_t cs = sizeof(Cx<R>);
   dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3 * mm.km);
   dim3 gp(g.Px, mm.km);
   const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
-  Cx<R>* T1 = b.T1 + mm.m0 * plane_elems(g);
-  Cx<R>* T2 = b.T2 + mm.m0 * plane_elems(g);
+  if (scratch.T1 && (mm.km != 1 || g.split)) {
+    set_error("matvec: caller scratch serves one member of an unsplit operator");
+    return VOX_ERR_BAD_ARG;
+  }
+  Cx<R>* T1 = scratch.T1 ? scratch.T1 : b.T1 + mm.m0 * plane_elems(g);
+  Cx<R>* T2 = scratch.T2 ? scratch.T2 : b.T2 + mm.m0 * plane_elems(g);
   const Cx<R>* fN = b.fN + mm.m0 * fN_elems(g);
   k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1, skip,
                                             mm.vs, mm.fs);
@@ -1130,7 +1143,8 @@ static std::mutex g_noalloc_mu;
 static std::map<int, void*> g_noalloc_addr;  // device ordinal -> array address
 
 // Device address of the array on `dev` (which must be current).  Looked up
-// once per device; a host-side reference to the symbol is not a device address.
+// once per device and kept while that device's primary context lives; a
+// host-side reference to the symbol is not a device address.
 static vox_status noalloc_scratch(int dev, void** out) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   auto it = g_noalloc_addr.find(dev);
@@ -1151,24 +1165,6 @@ static vox_status noalloc_scratch(int dev, void** out) {
   return VOX_OK;
 }
 
-template <typename R>
-static vox_status matvec_noalloc(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out,
-                                 cudaStream_t st, Cx<R>* T1, Cx<R>* T2) {
-  OpBuffers<R>& b = bufs<R>(op);
-  const OpGeom& g = b.geo;
-  const size_t cs = sizeof(Cx<R>);
-  dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3);
-  const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
-  k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1,
-                                            nullptr, 0, 0);
-  k_plane<R><<<g.Px, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1, b.fN, T2,
-                                               nullptr, 0);
-  k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
-                                            b.gram, scale, b.out_scale, mode, out, nullptr, 0, 0);
-  VOX_CUDA(cudaGetLastError());
-  return VOX_OK;
-}
-
 }  // namespace vox
 
 extern "C" vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, const void* in,
@@ -1182,7 +1178,12 @@ extern "C" vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, 
   const OpGeom& g = prec == VOX_C128 ? op->d.geo : op->f.geo;
   const size_t cs = prec == VOX_C128 ? sizeof(double2) : sizeof(float2);
   const size_t half = ((size_t)g.Px * 3 * g.N * g.M * cs + 255) / 256 * 256;
-  if (2 * half > kNoAllocScratchBytes || g.split) {
+  if (g.split) {
+    set_error("vox_mv_AN_noalloc: operators whose planes do not fit in shared memory (split "
+              "plane kernels, a third intermediate) are not supported; use vox_mv_AN_device");
+    return VOX_ERR_BAD_ARG;
+  }
+  if (2 * half > kNoAllocScratchBytes) {
     set_error("vox_mv_AN_noalloc: this operator needs " + std::to_string(2 * half) +
               " bytes of scratch; the fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
               " bytes (use vox_mv_AN_device)");
@@ -1193,9 +1194,11 @@ extern "C" vox_status vox_mv_AN_noalloc(vox_op_t op, int transp, vox_prec prec, 
   cudaStream_t st = stream ? (cudaStream_t)stream : op->stream;
   const int mode = transp ? MV_AN_T : MV_AN;
   unsigned char* b8 = static_cast<unsigned char*>(base);
-  if (prec == VOX_C128)
-    return matvec_noalloc<double>(op, mode, (const double2*)in, (double2*)out, st,
-                                  (double2*)b8, (double2*)(b8 + half));
-  return matvec_noalloc<float>(op, mode, (const float2*)in, (float2*)out, st, (float2*)b8,
-                               (float2*)(b8 + half));
+  if (prec == VOX_C128) {
+    PlaneScratch<double> sc{(double2*)b8, (double2*)(b8 + half)};
+    return matvec<double>(op, mode, (const double2*)in, (double2*)out, st, nullptr, Members(),
+                          sc);
+  }
+  PlaneScratch<float> sc{(float2*)b8, (float2*)(b8 + half)};
+  return matvec<float>(op, mode, (const float2*)in, (float2*)out, st, nullptr, Members(), sc);
 }
