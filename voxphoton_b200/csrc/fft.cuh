@@ -5,9 +5,9 @@
 // Stage s with radix R and Ns = product of the earlier radices: butterfly j
 // (0 <= j < n/R) reads src[j + r*n/R], multiplies input r by W_{Ns*R}^{r*(j%Ns)},
 // runs a length-R DFT and writes dst[(j/Ns)*Ns*R + j%Ns + r*Ns].
-// Radices 2, 3, 4, 5, 8 are hand-coded; 7, 11, 13 use the paired cos/sin form
-// with compile-time R; any other prime factor up to 64 runs a runtime-R
-// butterfly (only used by one-time operator setup on awkward lengths).
+// Radices 2, 3, 4, 5, 8 are hand-coded; 7, 11, 13 (and, where a kernel asks,
+// the primes 17..37) use the paired cos/sin form with compile-time R; any other
+// prime factor up to 64 runs a runtime-R butterfly.
 //
 // Twiddles come from one table per length n, W_n^m = exp(-2*pi*i*m/n), built on
 // the host in double precision (the float path uses the rounded copy).
@@ -178,6 +178,52 @@ __device__ __forceinline__ void dft_odd(C* v, int sign, const C* __restrict__ tw
   v[0] = y0;
 }
 
+// The same butterfly for the large primes (17..37), written straight to its
+// destination out[q * os]: the sums a_j, b_j replace v_j, v_{R-j} in place, the
+// H distinct cosines and sines are loaded once, and each output pair is formed
+// and stored at once, so the stage holds about R complex values in registers.
+template <int R, typename C>
+__device__ __forceinline__ void dft_odd_store(C* v, int sign, const C* __restrict__ tw,
+                                              int nOverR, C* out, int os) {
+  constexpr int H = (R - 1) / 2;
+  using RT = decltype(v[0].x);
+  // cos and sin of 2 pi q / R (q = 1..H); the angle of pair (j, k) is
+  // q = jk mod R, with cos(R - q) = cos q and sin(R - q) = -sin q
+  RT cs[H], sn[H];
+#pragma unroll
+  for (int q = 1; q <= H; q++) {
+    const C w = tw[q * nOverR];  // (cos, -sin)
+    cs[q - 1] = w.x;
+    sn[q - 1] = -w.y;
+  }
+  C y0 = v[0];
+#pragma unroll
+  for (int j = 1; j <= H; j++) {
+    const C t = v[j];
+    v[j] = cadd(t, v[R - j]);      // a_j
+    v[R - j] = csub(t, v[R - j]);  // b_j
+    y0 = cadd(y0, v[j]);
+  }
+#pragma unroll
+  for (int k = 1; k <= H; k++) {
+    C p = v[0], u = czero<C>();
+#pragma unroll
+    for (int j = 1; j <= H; j++) {
+      const int q = (j * k) % R;
+      const RT c = q <= H ? cs[q - 1] : cs[R - q - 1];
+      const RT sq = q <= H ? sn[q - 1] : -sn[R - q - 1];
+      p.x += v[j].x * c;
+      p.y += v[j].y * c;
+      u.x += v[R - j].x * sq;
+      u.y += v[R - j].y * sq;
+    }
+    const C q = mul_si(u, sign);
+    out[k * os] = cadd(p, q);
+    out[(R - k) * os] = csub(p, q);
+  }
+  out[0] = y0;
+}
+
 template <int R, typename C>
 __device__ __forceinline__ void dft_small(C* v, int sign, const C* __restrict__ tw, int nOverR) {
   if constexpr (R == 2) dft2(v);
@@ -218,10 +264,14 @@ __device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restri
 #pragma unroll
       for (int r = 1; r < R; r++) v[r] = cmul(v[r], tw_get(tw, r * k * twstep, sign));
     }
-    dft_small<R>(v, sign, tw, nR);
     const int idxD = jq * Ns * R + k;
+    if constexpr (R > 13) {
+      dft_odd_store<R>(v, sign, tw, nR, d + idxD, Ns);
+    } else {
+      dft_small<R>(v, sign, tw, nR);
 #pragma unroll
-    for (int r = 0; r < R; r++) d[idxD + r * Ns] = v[r];
+      for (int r = 0; r < R; r++) d[idxD + r * Ns] = v[r];
+    }
     k += dk;
     jq += dq;
     b += db;
@@ -264,10 +314,31 @@ __device__ void fft_stage_generic(const C* __restrict__ src, C* __restrict__ dst
   }
 }
 
+// Compiled butterflies for the primes 17..37 (paired cos/sin form, dft_odd_store).
+template <typename C>
+__device__ __forceinline__ bool big_prime_stage(int R, const C* __restrict__ src,
+                                                C* __restrict__ dst, int n, int Ns, int nseq,
+                                                int sstride, const C* __restrict__ tw, int sign,
+                                                int tid, int nthr) {
+  switch (R) {
+    case 17: fft_stage<17>(src, dst, n, Ns, nseq, sstride, tw, sign, tid, nthr); return true;
+    case 19: fft_stage<19>(src, dst, n, Ns, nseq, sstride, tw, sign, tid, nthr); return true;
+    case 23: fft_stage<23>(src, dst, n, Ns, nseq, sstride, tw, sign, tid, nthr); return true;
+    case 29: fft_stage<29>(src, dst, n, Ns, nseq, sstride, tw, sign, tid, nthr); return true;
+    case 31: fft_stage<31>(src, dst, n, Ns, nseq, sstride, tw, sign, tid, nthr); return true;
+    case 37: fft_stage<37>(src, dst, n, Ns, nseq, sstride, tw, sign, tid, nthr); return true;
+    default: return false;
+  }
+}
+
 // Transform nseq sequences of length p.n held in bufA (stride sstride) in
 // place of ping-pong buffers bufA/bufB.  Returns the buffer holding the result.
 // All threads of the block must call it; it ends with __syncthreads().
-template <typename C>
+// kBigPrimes compiles butterflies for the primes 17..37 as well: lengths with
+// such a factor (the preconditioner's x-FFT of length L, e.g. 1160 = 8*5*29 or
+// 1480 = 8*5*37) then avoid the runtime-radix stage.  Kernels whose lengths
+// are 7-smooth leave it off and keep their register budget.
+template <typename C, bool kBigPrimes = false>
 __device__ C* block_fft(C* bufA, C* bufB, const FftPlan& p, int nseq, int sstride,
                         const C* __restrict__ tw, int sign) {
   C* src = bufA;
@@ -285,7 +356,12 @@ __device__ C* block_fft(C* bufA, C* bufB, const FftPlan& p, int nseq, int sstrid
       case 8: fft_stage<8>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
       case 11: fft_stage<11>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
       case 13: fft_stage<13>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
-      default: fft_stage_generic(src, dst, p.n, R, Ns, nseq, sstride, tw, sign, tid, nthr); break;
+      default:
+        if constexpr (kBigPrimes) {
+          if (big_prime_stage(R, src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr)) break;
+        }
+        fft_stage_generic(src, dst, p.n, R, Ns, nseq, sstride, tw, sign, tid, nthr);
+        break;
     }
     __syncthreads();
     C* t = src;

@@ -76,8 +76,10 @@ __device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b
 }
 
 // --------------------------------------------------------------- apply: x-FFT
-template <typename R>
-__global__ void __launch_bounds__(256) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
+// kBig: the x length L has a prime factor above 13 (compiled big-prime
+// butterflies; a separate instantiation keeps the others' register budget).
+template <typename R, bool kBig>
+__global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
                                                  const Cx<R>* __restrict__ in,
                                                  const int* __restrict__ vmap,
                                                  Cx<R>* __restrict__ T, const int* skip,
@@ -103,7 +105,7 @@ __global__ void __launch_bounds__(256) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<
     bufA[(size_t)l * g.sx + x] = v;
   }
   __syncthreads();
-  C* res = block_fft(bufA, bufB, pl, g.ybx, g.sx, tw, -1);
+  C* res = block_fft<C, kBig>(bufA, bufB, pl, g.ybx, g.sx, tw, -1);
   for (int t = threadIdx.x; t < nl * g.L; t += blockDim.x) {
     const int i = t / nl;
     const int l = t - i * nl;
@@ -111,8 +113,8 @@ __global__ void __launch_bounds__(256) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<
   }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256) k_pc_xinv(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
+template <typename R, bool kBig>
+__global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xinv(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
                                                  const Cx<R>* __restrict__ T,
                                                  const int* __restrict__ vmap, R scale,
                                                  Cx<R>* out, const int* skip, long long vs,
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(256) k_pc_xinv(PcGeom g, FftPlan pl, const Cx<
     bufA[(size_t)l * g.sx + i] = (l < nl) ? T[(long long)i * g.n3 + col0 + l] : czero<C>();
   }
   __syncthreads();
-  C* res = block_fft(bufA, bufB, pl, g.ybx, g.sx, tw, +1);
+  C* res = block_fft<C, kBig>(bufA, bufB, pl, g.ybx, g.sx, tw, +1);
   for (int t = threadIdx.x; t < nl * g.L; t += blockDim.x) {
     const int l = t / g.L;
     const int x = t - l * g.L;

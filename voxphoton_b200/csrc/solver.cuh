@@ -151,6 +151,39 @@ static vox_status l2_apply(vox_precond_s* p, Cx<R>* T, Cx<R>* T2, cudaStream_t s
 // out = M^{-1} in (c128) or f_scale * M^{-1} in (c64 copy), for the members
 // of mm (vectors mm.vs apart, skip flags mm.fs apart); mm.m0 selects the
 // first member's work in this handle.
+// x-FFT kernels of the preconditioner: the big-prime instantiation only for
+// lengths L that need it.
+static bool plan_has_big_prime(const FftPlan& pl) {
+  for (int s = 0; s < pl.nst; s++)
+    if (pl.radix[s] > 13) return true;
+  return false;
+}
+
+template <typename R>
+static void pc_xfwd_launch(vox_precond_s* p, const PcGeom& g, dim3 grid, cudaStream_t st,
+                           const Cx<R>* in, const int* vmap, Cx<R>* T, const int* skip,
+                           long long vs, int fs) {
+  const size_t sm = pc_xsmem(g, sizeof(Cx<R>));
+  if (plan_has_big_prime(p->pl))
+    k_pc_xfwd<R, true><<<grid, 256, sm, st>>>(g, p->pl, pc_tw<R>(p), in, vmap, T, skip, vs, fs);
+  else
+    k_pc_xfwd<R, false><<<grid, 256, sm, st>>>(g, p->pl, pc_tw<R>(p), in, vmap, T, skip, vs, fs);
+}
+
+template <typename R>
+static void pc_xinv_launch(vox_precond_s* p, const PcGeom& g, dim3 grid, cudaStream_t st,
+                           const Cx<R>* T2, const int* vmap, Cx<R>* out, const int* skip,
+                           long long vs, int fs) {
+  const size_t sm = pc_xsmem(g, sizeof(Cx<R>));
+  const R scale = (R)(1.0 / g.L);
+  if (plan_has_big_prime(p->pl))
+    k_pc_xinv<R, true><<<grid, 256, sm, st>>>(g, p->pl, pc_tw<R>(p), T2, vmap, scale, out, skip,
+                                              vs, fs);
+  else
+    k_pc_xinv<R, false><<<grid, 256, sm, st>>>(g, p->pl, pc_tw<R>(p), T2, vmap, scale, out,
+                                               skip, vs, fs);
+}
+
 template <typename R>
 static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaStream_t st,
                            const int* skip, Members mm = Members()) {
@@ -173,23 +206,23 @@ static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaSt
     VOX_CUDA(cudaGetLastError());
     return VOX_OK;
   }
-  k_pc_xfwd<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), in, p->vmap, T, skip,
-                                                  mm.vs, mm.fs);
+  pc_xfwd_launch<R>(p, g, gx, st, in, p->vmap, T, skip, mm.vs, mm.fs);
   if (p->kind == 1) {
     VOX_TRY(l2_apply<R>(p, T, T2, st, skip, mm.fs, mm.km));
   } else {
     VOX_TRY(inv_apply<R>(p, T, T2, st, skip, mm.fs, mm.km));
   }
-  k_pc_xinv<R><<<gx, 256, pc_xsmem(g, cs), st>>>(g, p->pl, pc_tw<R>(p), T2, p->vmap,
-                                                  (R)(1.0 / g.L), out, skip, mm.vs, mm.fs);
+  pc_xinv_launch<R>(p, g, gx, st, T2, p->vmap, out, skip, mm.vs, mm.fs);
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
 }
 
 template <typename R>
 static vox_status pc_attrs() {
-  VOX_TRY(smem_cap(k_pc_xfwd<R>));
-  VOX_TRY(smem_cap(k_pc_xinv<R>));
+  VOX_TRY(smem_cap(k_pc_xfwd<R, false>));
+  VOX_TRY(smem_cap(k_pc_xinv<R, false>));
+  VOX_TRY(smem_cap(k_pc_xfwd<R, true>));
+  VOX_TRY(smem_cap(k_pc_xinv<R, true>));
   VOX_TRY(smem_cap(k_pc_inv_apply<R, 2>));
   VOX_TRY(smem_cap(k_pc_inv_apply<R, 4>));
   VOX_TRY(smem_cap(k_pc_inv_apply<R, 8>));
@@ -1456,8 +1489,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     const int nb = (pg.n3 + pg.ybx - 1) / pg.ybx;
     Cx<R>* T = pc_T<R>(pc, 0);
     out[3] = timeit([&] {
-      k_pc_xfwd<R><<<dim3(nb, km), 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc), w.V,
-                                                                 op->vmap, T, nullptr, w.vs, 0);
+      pc_xfwd_launch<R>(pc, pg, dim3(nb, km), st, w.V, pc->vmap, T, nullptr, w.vs, 0);
     });
     vox_status ps = VOX_OK;
     out[4] = timeit([&] {
@@ -1465,10 +1497,8 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     });
     if (ps != VOX_OK) return ps;
     out[5] = timeit([&] {
-      k_pc_xinv<R><<<dim3(nb, km), 256, pc_xsmem(pg, cs), st>>>(pg, pc->pl, pc_tw<R>(pc),
-                                                                 pc_T<R>(pc, 1), op->vmap,
-                                                                 (R)(1.0 / pg.L), w.t, nullptr,
-                                                                 w.vs, 0);
+      pc_xinv_launch<R>(pc, pg, dim3(nb, km), st, pc_T<R>(pc, 1), pc->vmap, w.t, nullptr, w.vs,
+                        0);
     });
   }
   // Gram-Schmidt at basis size kgs+1 (done flag cleared before every launch)
