@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>*
   if (skip && skip[(long long)mb * fs]) return;
   in += mb * vs;
   T1 += mb * plane_elems(g);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int y0 = blockIdx.x * g.ybx;
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
   T1 += mb * plane_elems(g);
   T2 += mb * plane_elems(g);
   fN += mb * fN_elems(g);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int rows = 3 * g.N;
   C* ybuf = reinterpret_cast<C*>(smem_raw);          // [3N][sy]
   C* wA = ybuf + (size_t)rows * g.sy;
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(256) k_ysplit_fwd(OpGeom g, FftPlan py,
   using C = Cx<R>;
   const int mb = blockIdx.z;
   if (skip && skip[(long long)mb * fs]) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* wA = reinterpret_cast<C*>(smem_raw);
   C* wB = wA + (size_t)g.ry * g.sy;
   C* tys = wB + (size_t)g.ry * g.sy;
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256) k_zsplit(OpGeom g, FftPlan pz,
   using C = Cx<R>;
   const int mb = blockIdx.z;
   if (skip && skip[(long long)mb * fs]) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* wA = reinterpret_cast<C*>(smem_raw);
   C* wB = wA + (size_t)3 * g.kcs * g.sz;
   C* tzs = wB + (size_t)3 * g.kcs * g.sz;
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(256) k_ysplit_inv(OpGeom g, FftPlan py,
   using C = Cx<R>;
   const int mb = blockIdx.z;
   if (skip && skip[(long long)mb * fs]) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* wA = reinterpret_cast<C*>(smem_raw);
   C* wB = wA + (size_t)g.ry * g.sy;
   C* tys = wB + (size_t)g.ry * g.sy;
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>*
   T2 += mb * plane_elems(g);
   in += mb * vs;
   out += mb * vs;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int y0 = blockIdx.x * g.ybx;
@@ -469,7 +469,7 @@ template <typename R>
 __global__ void k_fft_axis(AxisDesc a, FftPlan p, const Cx<R>* __restrict__ tw, int sign,
                            Cx<R>* data) {
   using C = Cx<R>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)a.lb * a.sstride;
   const int nA = a.d[a.axA];

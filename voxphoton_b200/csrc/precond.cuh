@@ -19,6 +19,7 @@
 // plain per-mode GEMV instead.
 #pragma once
 
+#include "bulk.cuh"
 #include "fft.cuh"
 #include "krylov.cuh"
 
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xfwd
   if (skip && skip[(long long)mb * fs]) return;
   in += mb * vs;
   T += mb * pc_work_elems(g);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int col0 = blockIdx.x * g.ybx;
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xinv
   if (skip && skip[(long long)mb * fs]) return;
   T += mb * pc_work_elems(g);
   out += mb * vs;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int col0 = blockIdx.x * g.ybx;
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(256) k_level2_blocks(int L, int M, int N, long
                                                        const double2* __restrict__ tw,
                                                        const double2* __restrict__ Cf,
                                                        double2* __restrict__ B2) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int sy = pad_stride(M);
   double2* a = reinterpret_cast<double2*>(smem_raw);
   double2* b = a + sy;
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(256) k_level2_blocks(int L, int M, int N, long
 // failing column when a pivot is zero.
 __global__ void __launch_bounds__(128) k_small_inv(int n, double2* __restrict__ A,
                                                    int* __restrict__ info) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   double2* a = reinterpret_cast<double2*>(smem_raw);  // n x 2n, column-major, ld n
   __shared__ int piv_row;
   __shared__ double2 pinv;
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(256) k_l2_yfwd(PcGeom g, FftPlan py, const Cx<
   const int mb = blockIdx.y / g.L;
   const int i = blockIdx.y - mb * g.L;
   if (skip && skip[(long long)mb * fs]) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int sy = pad_stride(g.M);
   C* a = reinterpret_cast<C*>(smem_raw);
   C* b = a + kL2Lines * sy;
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(256) k_l2_yinv(PcGeom g, FftPlan py, const Cx<
   const int n2 = 3 * g.N;
   const int mb = blockIdx.y / g.L;
   if (skip && skip[(long long)mb * fs]) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int sy = pad_stride(g.M);
   C* a = reinterpret_cast<C*>(smem_raw);
   C* b = a + kL2Lines * sy;
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(256) k_l2_gemv(PcGeom g, const Cx<R>* __restri
   const int n2 = 3 * g.N;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long im = (long long)blockIdx.x * 8 + warp;  // i * M + m
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* xw = reinterpret_cast<C*>(smem_raw) + (size_t)warp * n2 * P;  // this warp's columns
   if (im >= (long long)g.L * g.M) return;
   const long long ws = (long long)g.L * g.n3;  // member stride of the work
@@ -482,7 +483,7 @@ __global__ void k_vmap_box(int L, int M, int N, int x0, int y0, int Ls, int Ms,
 template <typename R>
 __global__ void __launch_bounds__(512) k_lu_batched(int n, int ld, Cx<R>* A, int* piv, int* info) {
   using C = Cx<R>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* P = reinterpret_cast<C*>(smem_raw);  // panel: (n) x kLuNb, column-major, ld = n
   __shared__ int s_piv[kLuNb];
   __shared__ R s_best[32];
@@ -960,7 +961,7 @@ __global__ void __launch_bounds__(32 * kRoundTiles) k_lu_inv_cols(
   using C = double2;
   constexpr int B = kTrsvNb;
   constexpr int S = Ring2<double>::value;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* ring = reinterpret_cast<C*>(smem_raw);
   const int n = g.n3;
   const int nb = (n + B - 1) / B;
@@ -1016,7 +1017,7 @@ __global__ void __launch_bounds__(kInvThreads) k_pc_inv_apply(
     for (int b = 0; b < km; b++) all = all && skip[(long long)b * fs] != 0;
     if (all) return;
   }
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* X = reinterpret_cast<C*>(smem_raw);  // X[k * P + col]; later the partial sums
   const int n = g.n3;
   const int MN = n / 3;
@@ -1084,6 +1085,188 @@ __global__ void __launch_bounds__(kInvThreads) k_pc_inv_apply(
     C s = red[rl * P + q];
 #pragma unroll
     for (int gg = 1; gg < kInvKG; gg++) s = cadd(s, red[(gg * kInvRows + rl) * P + q]);
+    if ((q & 1) == 0) {
+      Tout[b * wstride + (long long)f * n + row] = s;
+    } else if (two) {
+      Tout[b * wstride + (long long)i2 * n + row] = (row < MN) ? cscale(s, (R)-1) : s;
+    }
+  }
+}
+
+
+// ------------------------------------------------ apply: streamed inverse blocks
+// The same product as k_pc_inv_apply (T2_f = inv(B_f) T_f for P columns, the
+// modes f and L-f of every member), with the block's rows streamed through a
+// shared-memory ring by bulk asynchronous copies: one producer warp issues, per
+// stage, KC column segments of the CTA's 128 rows (one copy each, no
+// registers held by the loads), and the 256 consumer threads multiply out of
+// shared memory.  Up to kStrMaxStages stages are in flight per CTA, which is
+// what keeps HBM busy; the per-thread arithmetic, its order and the final sum
+// of the four column groups are those of k_pc_inv_apply, so the two kernels
+// give the same bits.  grid (ld / 128 rounded up, blocks), kStrThreads
+// threads, shared memory str_smem().
+constexpr int kStrRows = 128;
+constexpr int kStrGroups = 4;
+constexpr int kStrConsumers = (kStrRows / 2) * kStrGroups;  // 256
+constexpr int kStrThreads = kStrConsumers + 32;             // + one producer warp
+constexpr int kStrMaxStages = 8;
+
+// columns per stage: a 16 KB stage of 128 rows in either precision
+template <typename R>
+constexpr int str_kc() {
+  return sizeof(R) == 4 ? 16 : 8;
+}
+template <typename R>
+constexpr size_t str_stage_bytes() {
+  return (size_t)str_kc<R>() * kStrRows * sizeof(Cx<R>);
+}
+// right-hand sides [ld][P] + ring [stages][KC][128]; the final partial sums
+// (4 groups x 128 rows x P) reuse the same space
+template <typename R>
+inline size_t str_smem(int ld, int P, int stages) {
+  const size_t xr = (size_t)ld * P * sizeof(Cx<R>) + (size_t)stages * str_stage_bytes<R>();
+  const size_t red = (size_t)kStrGroups * kStrRows * P * sizeof(Cx<R>);
+  return xr > red ? xr : red;
+}
+
+// named barrier of the 256 consumer threads (the producer warp may have left)
+__device__ __forceinline__ int consumers_sync_or(int pred) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.s32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(pred), "n"(kStrConsumers)
+      : "memory");
+  return r;
+}
+
+template <typename R, int P>
+__global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
+    PcGeom g, int paired, int ld, int stages, const Cx<R>* __restrict__ Binv,
+    const Cx<R>* __restrict__ Tin, Cx<R>* __restrict__ Tout, const int* skip, int fs, int km) {
+  using C = Cx<R>;
+  constexpr int KS = P / 2;
+  constexpr int KC = str_kc<R>();
+  static_assert(P % 2 == 0, "columns come in mode pairs");
+  if (kernel_err_set()) return;
+  if (skip) {
+    bool all = true;
+    for (int b = 0; b < km; b++) all = all && skip[(long long)b * fs] != 0;
+    if (all) return;
+  }
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full[kStrMaxStages];
+  __shared__ __align__(8) uint64_t empty[kStrMaxStages];
+  C* X = reinterpret_cast<C*>(smem_raw);  // X[k * P + col], k < ld
+  C* ring = X + (size_t)ld * P;          // [stages][KC][kStrRows]
+  const int n = g.n3;
+  const int MN = n / 3;
+  const int f = blockIdx.y;
+  const int i2 = g.L - f;
+  const bool two = paired && f != 0 && i2 != f;
+  const long long wstride = pc_work_elems(g);
+  const int r0 = blockIdx.x * kStrRows;
+  const int nrows = min(kStrRows, ld - r0);
+  const int nkb = ld / KC;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < stages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kStrConsumers / 32);
+    }
+    mbar_init_fence();
+  }
+  for (int b = 0; b < KS; b++) {
+    const C* T1 = Tin + b * wstride + (long long)f * n;
+    const C* T2 = Tin + b * wstride + (long long)(two ? i2 : f) * n;
+    for (int k = tid; k < ld; k += blockDim.x) {
+      C v1 = czero<C>(), v2 = czero<C>();
+      if (b < km && k < n) {
+        v1 = T1[k];
+        if (two) {
+          v2 = T2[k];
+          if (k < MN) v2 = cscale(v2, (R)-1);
+        }
+      }
+      X[P * k + 2 * b] = v1;
+      X[P * k + 2 * b + 1] = v2;
+    }
+  }
+  __syncthreads();
+  if (tid >= kStrConsumers) {
+    // producer warp: lane j copies column j of each stage
+    const int lane = tid & 31;
+    const C* Bf = Binv + (long long)f * ld * ld + r0;
+    const unsigned bytes = (unsigned)(nrows * sizeof(C));
+    for (int kb = 0; kb < nkb; kb++) {
+      const int s = kb % stages;
+      if (kb >= stages && !mbar_wait(&empty[s], ((kb / stages) - 1) & 1)) return;
+      if (lane == 0) mbar_arrive_expect_tx(&full[s], bytes * KC);
+      __syncwarp();
+      if (lane < KC)
+        bulk_g2s(ring + ((size_t)s * KC + lane) * kStrRows, Bf + (long long)(kb * KC + lane) * ld,
+                 bytes, &full[s]);
+    }
+    return;
+  }
+  const int rp = tid % (kStrRows / 2);  // row pair within the chunk
+  const int kg = tid / (kStrRows / 2);  // column group
+  const bool active = 2 * rp < nrows;
+  C a0[P], a1[P];
+#pragma unroll
+  for (int q = 0; q < P; q++) a0[q] = a1[q] = czero<C>();
+  int failed = 0;
+  for (int kb = 0; kb < nkb; kb++) {
+    const int s = kb % stages;
+    if (!mbar_wait(&full[s], (kb / stages) & 1)) {
+      failed = 1;
+      break;
+    }
+    if (active) {
+      const C* st = ring + (size_t)s * KC * kStrRows + 2 * rp;
+#pragma unroll
+      for (int c = kg; c < KC; c += kStrGroups) {
+        const int k = kb * KC + c;
+        if (k < n) {
+          C b0, b1;
+          ld_pair(st + c * kStrRows, b0, b1);
+          const C* xk = X + P * k;
+#pragma unroll
+          for (int q = 0; q < P; q += 2) {
+            C x0, x1;
+            ld_pair(xk + q, x0, x1);
+            cmac(a0[q], b0, x0);
+            cmac(a0[q + 1], b0, x1);
+            cmac(a1[q], b1, x0);
+            cmac(a1[q + 1], b1, x1);
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+  }
+  // every consumer past its last stage (or one gave up): the ring and X are free
+  if (consumers_sync_or(failed)) return;
+  C* red = X;  // red[(kg * kStrRows + row) * P + col]
+#pragma unroll
+  for (int q = 0; q < P; q++) {
+    red[(kg * kStrRows + 2 * rp) * P + q] = a0[q];
+    red[(kg * kStrRows + 2 * rp + 1) * P + q] = a1[q];
+  }
+  consumers_sync_or(0);
+  for (int idx = tid; idx < kStrRows * P; idx += kStrConsumers) {
+    const int q = idx / kStrRows;
+    const int rl = idx - q * kStrRows;
+    const int row = r0 + rl;
+    const int b = q >> 1;
+    if (row >= n || b >= km) continue;
+    C s = red[rl * P + q];
+#pragma unroll
+    for (int gg = 1; gg < kStrGroups; gg++) s = cadd(s, red[(gg * kStrRows + rl) * P + q]);
     if ((q & 1) == 0) {
       Tout[b * wstride + (long long)f * n + row] = s;
     } else if (two) {

@@ -70,31 +70,46 @@ static int lu_cols(int km) {
   while (ks < km) ks *= 2;
   return 2 * ks;
 }
-// Members per launch: at 8 columns a block is still streamed at close to the
-// HBM rate (the FMAs per byte fit the SM), and shared memory allows three
-// CTAs per SM; more members are applied in groups of this size.
-constexpr int kApplyMembers = 4;
+// Members per launch: every block is streamed once per launch, and the FMAs
+// per streamed byte grow with the members; complex64 takes up to 8 members
+// (16 columns: FP32 issue and HBM time about balance), complex128 up to 4
+// (its right-hand sides fill shared memory).  More members are applied in
+// groups of this size.
+template <typename R>
+constexpr int apply_members() {
+  return sizeof(R) == 4 ? 8 : 4;
+}
+
+// Ring stages that fit beside the right-hand sides (at least 2 needed).
+template <typename R>
+static int str_stages(int ld, int P) {
+  const long long room = (long long)kSmemCap - (long long)ld * P * sizeof(Cx<R>);
+  return (int)std::min<long long>(kStrMaxStages, room / (long long)str_stage_bytes<R>());
+}
 
 template <typename R, int P>
 static void launch_inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStream_t st,
                              const int* skip, int fs, int km) {
   const PcGeom& g = p->g;
-  const dim3 grid((p->ld + kInvRows - 1) / kInvRows, p->Lf);
-  k_pc_inv_apply<R, P><<<grid, kInvThreads, inv_apply_smem<R>(g.n3, P), st>>>(
-      g, p->paired, p->ld, pc_A<R>(p), T, T2, skip, fs, km);
+  const int stages = str_stages<R>(p->ld, P);
+  const dim3 grid((p->ld + kStrRows - 1) / kStrRows, p->Lf);
+  k_pc_inv_stream<R, P><<<grid, kStrThreads, str_smem<R>(p->ld, P, stages), st>>>(
+      g, p->paired, p->ld, stages, pc_A<R>(p), T, T2, skip, fs, km);
 }
 
 // T2 = per-mode inverse blocks applied to T, for km members (in groups of
-// kApplyMembers, each group one launch).
+// apply_members, each group one launch).
 template <typename R>
 static vox_status inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStream_t st,
                             const int* skip, int fs, int km) {
   const long long ws = pc_work_elems(p->g);
-  for (int m0 = 0; m0 < km; m0 += kApplyMembers) {
-    const int kg = std::min(kApplyMembers, km - m0);
+  for (int m0 = 0; m0 < km; m0 += apply_members<R>()) {
+    const int kg = std::min(apply_members<R>(), km - m0);
     const int P = lu_cols(kg);
-    if (inv_apply_smem<R>(p->g.n3, P) > (size_t)kSmemCap) {
-      set_error("preconditioner: too many members for one apply in this precision");
+    if (str_stages<R>(p->ld, P) < 2 || str_smem<R>(p->ld, P, 2) > (size_t)kSmemCap) {
+      set_error("preconditioner: blocks of " + std::to_string(p->ld) +
+                " rows leave no room for the streaming ring at " + std::to_string(kg) +
+                " members in this precision");
       return VOX_ERR_UNSUPPORTED;
     }
     const Cx<R>* Tg = T + m0 * ws;
@@ -103,7 +118,10 @@ static vox_status inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStr
     switch (P) {
       case 2: launch_inv_apply<R, 2>(p, Tg, T2g, st, sg, fs, kg); break;
       case 4: launch_inv_apply<R, 4>(p, Tg, T2g, st, sg, fs, kg); break;
-      default: launch_inv_apply<R, 8>(p, Tg, T2g, st, sg, fs, kg); break;
+      case 8: launch_inv_apply<R, 8>(p, Tg, T2g, st, sg, fs, kg); break;
+      default:
+        if constexpr (sizeof(R) == 4) launch_inv_apply<R, 16>(p, Tg, T2g, st, sg, fs, kg);
+        break;
     }
   }
   return VOX_OK;
@@ -223,9 +241,10 @@ static vox_status pc_attrs() {
   VOX_TRY(smem_cap(k_pc_xinv<R, false>));
   VOX_TRY(smem_cap(k_pc_xfwd<R, true>));
   VOX_TRY(smem_cap(k_pc_xinv<R, true>));
-  VOX_TRY(smem_cap(k_pc_inv_apply<R, 2>));
-  VOX_TRY(smem_cap(k_pc_inv_apply<R, 4>));
-  VOX_TRY(smem_cap(k_pc_inv_apply<R, 8>));
+  VOX_TRY(smem_cap(k_pc_inv_stream<R, 2>));
+  VOX_TRY(smem_cap(k_pc_inv_stream<R, 4>));
+  VOX_TRY(smem_cap(k_pc_inv_stream<R, 8>));
+  if constexpr (sizeof(R) == 4) VOX_TRY(smem_cap(k_pc_inv_stream<R, 16>));
   VOX_TRY(smem_cap(k_l2_yfwd<R>));
   VOX_TRY(smem_cap(k_l2_yinv<R>));
   VOX_TRY(smem_cap(k_l2_gemv<R, 1>));
@@ -351,10 +370,11 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p, int L, int M, int N,
     return VOX_ERR_UNSUPPORTED;
   }
   // the LU panel bound (n3 <= 1760) also keeps the streamed solve's
-  // ring + right-hand sides (64 KiB + 32 B * n3) under the cap
+  // ring + right-hand sides (64 KiB + 32 B * n3) and the streamed apply's
+  // (two 16 KiB stages + 32 B * ld) under the cap
   if (lu && ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
              lu_stream2_smem<double>(lu_npad(g.n3), kInvBuildCols) > (size_t)kSmemCap ||
-             inv_apply_smem<double>(g.n3, 2) > (size_t)kSmemCap)) {
+             str_smem<double>((g.n3 + 31) / 32 * 32, 2, 2) > (size_t)kSmemCap)) {
     set_error("preconditioner: 3*M*N too large for the batched LU panel");
     return VOX_ERR_UNSUPPORTED;
   }
