@@ -400,6 +400,8 @@ static vox_status set_smem_attrs() {
   VOX_TRY(smem_cap(k_ysplit_fwd<R>));
   VOX_TRY(smem_cap(k_zsplit<R>));
   VOX_TRY(smem_cap(k_ysplit_inv<R>));
+  VOX_TRY(smem_cap(k_gs_pass<R, false>));
+  VOX_TRY(smem_cap(k_gs_pass<R, true>));
   return VOX_OK;
 }
 

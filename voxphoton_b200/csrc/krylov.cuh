@@ -19,6 +19,7 @@
 // would run alone and its arithmetic does not depend on the other members.
 #pragma once
 
+#include "bulk.cuh"
 #include "vox_common.cuh"
 
 namespace vox {
@@ -329,6 +330,50 @@ __device__ __forceinline__ void givens(double2 a, double2 b, double* c, double2*
   *r = make_double2(ph.x * nrm, ph.y * nrm);
 }
 
+// Hessenberg column k from h1 + h2 and the norm of the orthogonalised w, the
+// previous rotations, a new Givens rotation, the residual estimate and the
+// cycle's stopping tests (one thread).
+__device__ __forceinline__ void gs_column(GmresDev* st, int k, double nrm) {
+  const int m = st->m;
+  const int ld = m + 1;
+  double2* Hc = st->H + (size_t)k * ld;
+  double2* Rc = st->Rm + (size_t)k * ld;
+  for (int j = 0; j <= k; j++) {
+    Hc[j] = make_double2(st->h1[j].x + st->h2[j].x, st->h1[j].y + st->h2[j].y);
+    Rc[j] = Hc[j];
+  }
+  Hc[k + 1] = make_double2(nrm, 0.0);
+  Rc[k + 1] = Hc[k + 1];
+  // apply previous rotations
+  for (int i = 0; i < k; i++) {
+    const double c = st->cs[i];
+    const double2 sv = st->sn[i];
+    const double2 a = Rc[i], b = Rc[i + 1];
+    // a' = c a + s b ; b' = -conj(s) a + c b
+    Rc[i] = make_double2(c * a.x + sv.x * b.x - sv.y * b.y, c * a.y + sv.x * b.y + sv.y * b.x);
+    Rc[i + 1] = make_double2(-(sv.x * a.x + sv.y * a.y) + c * b.x,
+                             -(sv.x * a.y - sv.y * a.x) + c * b.y);
+  }
+  double c;
+  double2 sv, r;
+  givens(Rc[k], Rc[k + 1], &c, &sv, &r);
+  st->cs[k] = c;
+  st->sn[k] = sv;
+  Rc[k] = r;
+  Rc[k + 1] = make_double2(0.0, 0.0);
+  const double2 gk = st->g[k];
+  st->g[k] = make_double2(c * gk.x, c * gk.y);
+  // g(k+1) = -conj(s) g(k)
+  st->g[k + 1] = make_double2(-(sv.x * gk.x + sv.y * gk.y), -(sv.x * gk.y - sv.y * gk.x));
+  const double resid = hypot(st->g[k + 1].x, st->g[k + 1].y);
+  st->resvec[k] = resid;
+  st->k = k + 1;
+  st->inv_norm = (nrm > 0.0) ? 1.0 / nrm : 0.0;
+  if (resid < st->tol_abs) st->converged = 1;
+  if (nrm == 0.0) st->breakdown = 1;
+  if (st->converged || st->breakdown || k + 1 >= m) st->done = 1;
+}
+
 // w <- w - V h2 ; ||w||^2 ; last block: Hessenberg column, Givens, residual.
 template <typename R>
 __global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, int k,
@@ -352,45 +397,7 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_update_norm(GmresDev* st, in
     reduce_partials(st->partial, 1, gridDim.x, tot, sh);
     if (threadIdx.x == 0) {
       st->ticket = 0;
-      const int m = st->m;
-      const int ld = m + 1;
-      const double nrm = sqrt(tot[0].x);
-      double2* Hc = st->H + (size_t)k * ld;
-      double2* Rc = st->Rm + (size_t)k * ld;
-      for (int j = 0; j <= k; j++) {
-        Hc[j] = make_double2(st->h1[j].x + st->h2[j].x, st->h1[j].y + st->h2[j].y);
-        Rc[j] = Hc[j];
-      }
-      Hc[k + 1] = make_double2(nrm, 0.0);
-      Rc[k + 1] = Hc[k + 1];
-      // apply previous rotations
-      for (int i = 0; i < k; i++) {
-        const double c = st->cs[i];
-        const double2 sv = st->sn[i];
-        const double2 a = Rc[i], b = Rc[i + 1];
-        // a' = c a + s b ; b' = -conj(s) a + c b
-        Rc[i] = make_double2(c * a.x + sv.x * b.x - sv.y * b.y, c * a.y + sv.x * b.y + sv.y * b.x);
-        Rc[i + 1] = make_double2(-(sv.x * a.x + sv.y * a.y) + c * b.x,
-                                 -(sv.x * a.y - sv.y * a.x) + c * b.y);
-      }
-      double c;
-      double2 sv, r;
-      givens(Rc[k], Rc[k + 1], &c, &sv, &r);
-      st->cs[k] = c;
-      st->sn[k] = sv;
-      Rc[k] = r;
-      Rc[k + 1] = make_double2(0.0, 0.0);
-      const double2 gk = st->g[k];
-      st->g[k] = make_double2(c * gk.x, c * gk.y);
-      // g(k+1) = -conj(s) g(k)
-      st->g[k + 1] = make_double2(-(sv.x * gk.x + sv.y * gk.y), -(sv.x * gk.y - sv.y * gk.x));
-      const double resid = hypot(st->g[k + 1].x, st->g[k + 1].y);
-      st->resvec[k] = resid;
-      st->k = k + 1;
-      st->inv_norm = (nrm > 0.0) ? 1.0 / nrm : 0.0;
-      if (resid < st->tol_abs) st->converged = 1;
-      if (nrm == 0.0) st->breakdown = 1;
-      if (st->converged || st->breakdown || k + 1 >= m) st->done = 1;
+      gs_column(st, k, sqrt(tot[0].x));
     }
   }
 }
@@ -570,6 +577,183 @@ __global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     y[i] = cadd(y[i], x[i]);
+}
+
+
+// ------------------------------------------- Gram-Schmidt in two basis reads
+// For restart lengths up to kGsMaxCols - 1 an Arnoldi step reads the basis
+// twice (it read it four times in the kernels above):
+//   k_gs_pass<false>: h1 = V^H w;
+//   k_gs_pass<true>:  w' = w - V h1 (written back), h2 = V^H w' and ||w'||^2
+//                     in the same read; its last CTA forms the Hessenberg
+//                     column with ||w''||^2 = ||w'||^2 - ||h2||^2 (w'' = w' - V h2
+//                     and h2 = V^H w' with V orthonormal);
+//   k_gs_finish:      V(:,k+1) = (w' - V h2) / ||w''||.
+// The two passes stage each chunk of gs_rows() rows of all k+1 basis columns
+// (and of w) in shared memory with bulk asynchronous copies, two chunks in
+// flight per CTA; the dot products run out of shared memory, one warp per
+// column, accumulating in FP64 in a fixed order (deterministic).
+constexpr int kGsMaxCols = 51;
+constexpr int kGsWarps = kRedThreads / 32;
+constexpr int kGsColsPerWarp = (kGsMaxCols + kGsWarps - 1) / kGsWarps;
+constexpr int kGsBlocks = 296;  // two CTAs per SM on 148 SMs
+
+template <typename R>
+constexpr int gs_rows() {
+  return sizeof(R) == 4 ? 128 : 64;
+}
+// two stages of [nj][rows] basis values + [rows] of w
+template <typename R>
+inline size_t gs_pass_smem(int nj) {
+  return 2ull * ((size_t)nj + 1) * gs_rows<R>() * sizeof(Cx<R>);
+}
+
+template <typename R, bool kUpdate>
+__global__ void __launch_bounds__(kRedThreads, 2) k_gs_pass(GmresDev* st, int k,
+                                                            const Cx<R>* __restrict__ V,
+                                                            long long ldv, Cx<R>* w, long long n,
+                                                            long long vs) {
+  using C = Cx<R>;
+  constexpr int RW = gs_rows<R>();
+  __shared__ double2 sh[32];
+  __shared__ C hs[kGsMaxCols];
+  __shared__ __align__(8) uint64_t full[2];
+  __shared__ double2 tot[1];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  st += blockIdx.y;
+  V += blockIdx.y * vs;
+  w += blockIdx.y * vs;
+  if (st->done || kernel_err_set()) return;
+  const int nj = k + 1;
+  const size_t stage = ((size_t)nj + 1) * RW;  // elements of one stage
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init_fence();
+  }
+  if (kUpdate)
+    for (int j = tid; j < nj; j += blockDim.x) hs[j] = from_d2<C>(st->h1[j]);
+  __syncthreads();
+  const long long nch = (n + RW - 1) / RW;
+  // the copies of chunk c into stage s (warp 0: lane j copies column j,
+  // j = nj is w); sizes round up to 16 bytes inside the column padding
+  auto issue = [&](long long c, int s) {
+    const long long r0 = c * RW;
+    const int rows = (int)min((long long)RW, n - r0);
+    const unsigned bytes = (unsigned)(((size_t)rows * sizeof(C) + 15) / 16 * 16);
+    if (lane == 0) mbar_arrive_expect_tx(&full[s], bytes * (nj + 1));
+    __syncwarp();
+    C* dst = buf + (size_t)s * stage;
+    for (int j = lane; j <= nj; j += 32) {
+      const C* src = (j < nj) ? V + (long long)j * ldv + r0 : w + r0;
+      bulk_g2s(dst + (size_t)j * RW, src, bytes, &full[s]);
+    }
+  };
+  double2 acc[kGsColsPerWarp];
+#pragma unroll
+  for (int q = 0; q < kGsColsPerWarp; q++) acc[q] = make_double2(0.0, 0.0);
+  double nrm = 0.0;
+  int it = 0, failed = 0;
+  if (warp == 0 && blockIdx.x < nch) issue(blockIdx.x, 0);
+  for (long long c = blockIdx.x; c < nch; c += gridDim.x, it++) {
+    const int s = it & 1;
+    // prefetch the next chunk into the other stage (freed by the last barrier)
+    if (warp == 0 && c + gridDim.x < nch) issue(c + gridDim.x, s ^ 1);
+    if (!mbar_wait(&full[s], (it >> 1) & 1)) failed = 1;
+    if (__syncthreads_or(failed)) return;
+    const C* Vs = buf + (size_t)s * stage;
+    C* ws = buf + (size_t)s * stage + (size_t)nj * RW;
+    const long long r0 = c * RW;
+    const int rows = (int)min((long long)RW, n - r0);
+    if (kUpdate) {
+      if (tid < rows) {
+        C wi = ws[tid];
+        for (int j = 0; j < nj; j++) {
+          const C v = Vs[(size_t)j * RW + tid];
+          const C h = hs[j];
+          wi.x -= v.x * h.x - v.y * h.y;
+          wi.y -= v.x * h.y + v.y * h.x;
+        }
+        ws[tid] = wi;
+        w[r0 + tid] = wi;
+        nrm += (double)wi.x * wi.x + (double)wi.y * wi.y;
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < kGsColsPerWarp; q++) {
+      const int j = warp + q * kGsWarps;
+      if (j < nj) {
+        for (int i = lane; i < rows; i += 32) {
+          const double2 v = to_d2(Vs[(size_t)j * RW + i]);
+          const double2 x = to_d2(ws[i]);
+          acc_cdot(acc[q], v.x, v.y, x.x, x.y);
+        }
+      }
+    }
+    // every thread is done with stage s before warp 0 refills it
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < kGsColsPerWarp; q++) {
+    const int j = warp + q * kGsWarps;
+    const double2 v = warp_sum(acc[q]);
+    if (j < nj && lane == 0) st->partial[j * gridDim.x + blockIdx.x] = v;
+  }
+  if (kUpdate) {
+    const double2 t = block_sum(make_double2(nrm, 0.0), sh);
+    if (tid == 0) st->partial[nj * gridDim.x + blockIdx.x] = t;
+  }
+  if (last_block(&st->ticket)) {
+    if (!kUpdate) {
+      reduce_partials(st->partial, nj, gridDim.x, st->h1, sh);
+      if (tid == 0) st->ticket = 0;
+    } else {
+      reduce_partials(st->partial, nj, gridDim.x, st->h2, sh);
+      reduce_partials(st->partial + (size_t)nj * gridDim.x, 1, gridDim.x, tot, sh);
+      if (tid == 0) {
+        st->ticket = 0;
+        double hh = 0.0;
+        for (int j = 0; j < nj; j++) hh += st->h2[j].x * st->h2[j].x + st->h2[j].y * st->h2[j].y;
+        gs_column(st, k, sqrt(fmax(tot[0].x - hh, 0.0)));
+      }
+    }
+  }
+}
+
+// V(:,k+1) = (w' - V h2) * inv_norm, for the step that just completed (also
+// when it ended the cycle: the restart residual needs that column).
+template <typename R>
+__global__ void __launch_bounds__(kRedThreads) k_gs_finish(GmresDev* st, int k,
+                                                           const Cx<R>* __restrict__ V,
+                                                           long long ldv, const Cx<R>* w,
+                                                           Cx<R>* __restrict__ Vnext,
+                                                           long long n, long long vs) {
+  using C = Cx<R>;
+  __shared__ C hs[kGsMaxCols];
+  st += blockIdx.y;
+  V += blockIdx.y * vs;
+  w += blockIdx.y * vs;
+  Vnext += blockIdx.y * vs;
+  if (st->frozen || st->k != k + 1) return;
+  const int nj = k + 1;
+  for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<C>(st->h2[j]);
+  __syncthreads();
+  const R s = (R)st->inv_norm;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    C wi = w[i];
+#pragma unroll 8
+    for (int j = 0; j < nj; j++) {
+      const C v = V[(long long)j * ldv + i];
+      const C h = hs[j];
+      wi.x -= v.x * h.x - v.y * h.y;
+      wi.y -= v.x * h.y + v.y * h.x;
+    }
+    Vnext[i] = cscale(wi, s);
+  }
 }
 
 }  // namespace vox

@@ -890,11 +890,22 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
       VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, skip, mm));
       wv = w.t;
     }
-    k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
-    k_gs_update_dots<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
-    k_gs_update_norm<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
-    k_gs_scale<R><<<ge, 256, 0, st>>>(d, k, w.V + (long long)(k + 1) * ld, wv, n, w.vs);
-    *nk += 3 + ((right || left) ? 3 : 0) + 4;
+    if (m + 1 <= kGsMaxCols) {
+      // CGS2 in two reads of the basis
+      const dim3 gp(kGsBlocks, km);
+      const size_t sm = gs_pass_smem<R>(k + 1);
+      k_gs_pass<R, false><<<gp, kRedThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs);
+      k_gs_pass<R, true><<<gp, kRedThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs);
+      k_gs_finish<R><<<ge, kRedThreads, 0, st>>>(d, k, w.V, ld, wv,
+                                                 w.V + (long long)(k + 1) * ld, n, w.vs);
+      *nk += 3 + ((right || left) ? 3 : 0) + 3;
+    } else {
+      k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
+      k_gs_update_dots<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
+      k_gs_update_norm<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
+      k_gs_scale<R><<<ge, 256, 0, st>>>(d, k, w.V + (long long)(k + 1) * ld, wv, n, w.vs);
+      *nk += 3 + ((right || left) ? 3 : 0) + 4;
+    }
   }
   k_cycle_ls<<<g1, 32, 0, st>>>(d);
   if (right) {
@@ -1540,30 +1551,52 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
       VOX_CUDA(cudaMemcpyAsync(&w.st[mb], hdr.data(), hdr.size(), cudaMemcpyHostToDevice, st));
     VOX_TRY(wait_stream(st));
   }
-  out[6] = timeit([&] {
-    k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
-  });
-  out[7] = timeit([&] {
-    k_gs_update_dots<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
-  });
-  // update_norm sets done at the last column; time it at k < m-1 and clear after
-  double tn = 0;
-  for (int r = 0; r < reps + 1; r++) {
+  // the pass that forms the Hessenberg column sets done at the last column:
+  // time it at k < m-1 with done cleared before every launch
+  auto timed_clear = [&](auto&& launch) -> double {
+    double tn = 0;
+    for (int r = 0; r < reps + 1; r++) {
+      clear();
+      VOX_CUDA(cudaEventRecord(e0, st));
+      launch();
+      VOX_CUDA(cudaEventRecord(e1, st));
+      VOX_TRY(wait_event(e1));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (r > 0) tn += ms;
+    }
+    return tn / reps;
+  };
+  if (restart + 1 <= kGsMaxCols) {
+    const dim3 gp(kGsBlocks, km);
+    const size_t sm = gs_pass_smem<R>(k + 1);
+    out[6] = timeit([&] {
+      k_gs_pass<R, false><<<gp, kRedThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+    });
+    out[7] = timed_clear([&] {
+      k_gs_pass<R, true><<<gp, kRedThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+    });
     clear();
-    VOX_CUDA(cudaEventRecord(e0, st));
-    k_gs_update_norm<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
-    VOX_CUDA(cudaEventRecord(e1, st));
-    VOX_TRY(wait_event(e1));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (r > 0) tn += ms;
+    out[8] = timeit([&] {
+      k_gs_finish<R><<<dim3(nb, km), kRedThreads, 0, st>>>(
+          w.st, k, w.V, ld, w.w, w.V + (long long)(k + 1) * ld, n, w.vs);
+    });
+  } else {
+    out[6] = timeit([&] {
+      k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+    });
+    out[7] = timeit([&] {
+      k_gs_update_dots<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+    });
+    out[8] = timed_clear([&] {
+      k_gs_update_norm<R><<<gr, kRedThreads, 0, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+    });
+    clear();
+    out[9] = timeit([&] {
+      k_gs_scale<R><<<dim3(nb, km), 256, 0, st>>>(w.st, k, w.V + (long long)(k + 1) * ld, w.w,
+                                                   n, w.vs);
+    });
   }
-  out[8] = tn / reps;
-  clear();
-  out[9] = timeit([&] {
-    k_gs_scale<R><<<dim3(nb, km), 256, 0, st>>>(w.st, k, w.V + (long long)(k + 1) * ld, w.w, n,
-                                                 w.vs);
-  });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   VOX_CUDA(cudaGetLastError());
