@@ -24,6 +24,7 @@
 #include "bulk.cuh"
 #include "krylov.cuh"
 #include "mvp.cuh"
+#include "plane.cuh"
 #include "precond.cuh"
 #include "block.cuh"
 #include "cubature.cuh"
@@ -331,6 +332,44 @@ struct Members {
   int fs = 0;
 };
 
+// Every launch shape is checked against kSmemCap before use.  The attribute
+// below is a property of the kernel (per device), not of one operator, so it
+// is always raised to this one fixed cap: operators and preconditioners of
+// different sizes then coexist, and setting it from several host threads is
+// idempotent.
+static const int kSmemCap = 220 * 1024;
+
+// Kernel 2 of the matvec for km members: the register/shuffle plane kernel
+// when the padded plane is 64 x 24 (the Bragg gratings), the split kernels
+// when a plane does not fit in shared memory, else the general k_plane.
+template <typename R>
+static bool plane64_ok(const OpGeom& g) {
+  return !g.split && g.Py == kPlPy && g.Pz == kPlPz && g.M <= kPlPy && g.N <= kPlPz &&
+         plane64_smem<R>(g.N) <= (size_t)kSmemCap;
+}
+
+template <typename R>
+static void launch_plane(vox_op_s* op, const OpBuffers<R>& b, const Cx<R>* T1, const Cx<R>* fN,
+                         Cx<R>* T2, Cx<R>* TY, int km, const int* skip, int fs, cudaStream_t st) {
+  const OpGeom& g = b.geo;
+  const size_t cs = sizeof(Cx<R>);
+  if (g.split) {
+    const int rows = 3 * g.N;
+    const dim3 gy(g.Px, (rows + g.ry - 1) / g.ry, km);
+    const dim3 gz(g.Px, (g.Py + g.kcs - 1) / g.kcs, km);
+    const size_t ysm = ysmem(g, cs), zsm = zsmem(g, cs);
+    k_ysplit_fwd<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, T1, TY, skip, fs);
+    k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, fN, TY, skip, fs);
+    k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, TY, T2, skip, fs);
+  } else if (plane64_ok<R>(g)) {
+    k_plane64<R><<<dim3(g.Px, km), kPlThreads, plane64_smem<R>(g.N), st>>>(g, b.twY, b.twZ, T1,
+                                                                          fN, T2, skip, fs);
+  } else {
+    k_plane<R><<<dim3(g.Px, km), 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1,
+                                                           fN, T2, skip, fs);
+  }
+}
+
 // Plane intermediates supplied by the caller instead of the operator's own
 // (one member, unsplit kernel 2 only: vox_mv_AN_noalloc).
 template <typename R>
@@ -348,7 +387,6 @@ static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cu
   const OpGeom& g = b.geo;
   const size_t cs = sizeof(Cx<R>);
   dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3 * mm.km);
-  dim3 gp(g.Px, mm.km);
   const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
   if (scratch.T1 && (mm.km != 1 || g.split)) {
     set_error("matvec: caller scratch serves one member of an unsplit operator");
@@ -359,19 +397,8 @@ static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cu
   const Cx<R>* fN = b.fN + mm.m0 * fN_elems(g);
   k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1, skip,
                                             mm.vs, mm.fs);
-  if (g.split) {
-    Cx<R>* TY = b.TY + mm.m0 * planey_elems(g);
-    const int rows = 3 * g.N;
-    const dim3 gy(g.Px, (rows + g.ry - 1) / g.ry, mm.km);
-    const dim3 gz(g.Px, (g.Py + g.kcs - 1) / g.kcs, mm.km);
-    const size_t ysm = ysmem(g, cs), zsm = zsmem(g, cs);
-    k_ysplit_fwd<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, T1, TY, skip, mm.fs);
-    k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, fN, TY, skip, mm.fs);
-    k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, TY, T2, skip, mm.fs);
-  } else {
-    k_plane<R><<<gp, 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1, fN, T2, skip,
-                                               mm.fs);
-  }
+  launch_plane<R>(op, b, T1, fN, T2, g.split ? b.TY + mm.m0 * planey_elems(g) : nullptr, mm.km,
+                  skip, mm.fs, st);
   k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
                                             b.gram, scale, b.out_scale, mode, out, skip, mm.vs,
                                             mm.fs);
@@ -379,12 +406,6 @@ static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cu
   return VOX_OK;
 }
 
-// Every launch shape is checked against kSmemCap before use.  The attribute
-// below is a property of the kernel (per device), not of one operator, so it
-// is always raised to this one fixed cap: operators and preconditioners of
-// different sizes then coexist, and setting it from several host threads is
-// idempotent.
-static const int kSmemCap = 220 * 1024;
 
 template <typename K>
 static vox_status smem_cap(K* kernel) {
@@ -400,6 +421,7 @@ static vox_status set_smem_attrs() {
   VOX_TRY(smem_cap(k_ysplit_fwd<R>));
   VOX_TRY(smem_cap(k_zsplit<R>));
   VOX_TRY(smem_cap(k_ysplit_inv<R>));
+  VOX_TRY(smem_cap(k_plane64<R>));
   VOX_TRY(smem_cap(k_gs_pass<R, false>));
   VOX_TRY(smem_cap(k_gs_pass<R, true>));
   return VOX_OK;

@@ -1493,20 +1493,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, w.V, op->vmap, b.Mc, MV_AN, b.T1,
                                               nullptr, w.vs, 0);
   });
-  out[1] = timeit([&] {
-    if (g.split) {
-      const int rows = 3 * g.N;
-      const dim3 gy(g.Px, (rows + g.ry - 1) / g.ry, km);
-      const dim3 gz(g.Px, (g.Py + g.kcs - 1) / g.kcs, km);
-      const size_t ysm = ysmem(g, cs), zsm = zsmem(g, cs);
-      k_ysplit_fwd<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, b.T1, b.TY, nullptr, 0);
-      k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, b.fN, b.TY, nullptr, 0);
-      k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, b.TY, b.T2, nullptr, 0);
-    } else {
-      k_plane<R><<<dim3(g.Px, km), 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ,
-                                                             b.T1, b.fN, b.T2, nullptr, 0);
-    }
-  });
+  out[1] = timeit([&] { launch_plane<R>(op, b, b.T1, b.fN, b.T2, b.TY, km, nullptr, 0, st); });
   out[2] = timeit([&] {
     k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, w.V, b.Mr, b.Mc,
                                               b.gram, scale, b.out_scale, MV_AN, w.w, nullptr,
