@@ -9,10 +9,11 @@ Per device length (a "family") the loop keeps resident on the device:
 * one level-1 circulant preconditioner built at the band centre and shared by
   every wavelength of that length (vox_precond_share: one factor copy, per-slot
   work buffers);
-* a number of solve slots ("lanes"), each a batched operator of K members
+* solve slots ("lanes"), each a batched operator of K members
   (vox_op_create_batch: K copies of fN and of the GMRES state) + its own CUDA
-  stream.  The number of lanes is set by the HBM footprint of one lane
-  against a memory budget ("admission by footprint").
+  stream.  With a pool budget (SweepServer pool_bytes) lanes are admitted by
+  their measured HBM footprint as the queues of the lengths fill, and idle
+  lanes of lengths with nothing waiting are retired to make room.
 
 A request (length, wavelength) waits until it has arrived and a lane of its
 length is free.  The lane then takes every request of its length that has
@@ -229,14 +230,44 @@ class ServeConfig:
                                  # each one at the remaining FP64 target directly
 
 
-class SweepServer:
-    """Serves a request stream over several families with per-family slots."""
+class _LaneCtx:
+    """One continuously batched lane of a family inside the HBM pool."""
 
-    def __init__(self, families, cfg: ServeConfig = None):
+    def __init__(self, fam, op, pc, lane, nbytes):
+        self.fam = fam
+        self.op = op
+        self.pc = pc
+        self.lane = lane
+        self.nbytes = nbytes
+        self.inflight = {}      # member -> (request, start time)
+        self.retire = False     # asked to leave the pool once idle
+        self.stop = False       # the stream is over
+        self.thread = None
+
+
+class SweepServer:
+    """Serves a request stream over several families with per-family slots.
+
+    pool_bytes (continuous batching only): admission by HBM footprint.  The
+    lanes of every family share one device-memory budget; a family whose
+    arrived requests outnumber its free member slots gets a new lane when the
+    lane's measured footprint fits in what is left (and max_lanes allows),
+    and otherwise an idle lane of a family with nothing waiting is retired to
+    make room (every family keeps one), so lanes move between device lengths
+    as the mix of the stream changes.  JVIE_Solver_const.m:200-201 admits a
+    solve to the GPU when its estimated memory fits the device; here every
+    lane is admitted the same way."""
+
+    def __init__(self, families, cfg: ServeConfig = None, pool_bytes=None, max_lanes=None):
         self.families = {f.key: f for f in families}
         self.cfg = cfg or ServeConfig()
         self._bufs = {}
         self._lanes = {}
+        self.pool_bytes = pool_bytes
+        self.max_lanes = max_lanes  # per family, on top of the byte budget (None: no cap)
+        self.lane_bytes = {}     # family key -> measured bytes of one lane
+        self._pool = []          # _LaneCtx of every lane in the pool
+        self.pool_events = []    # ("add" | "retire", family key, bytes, time)
 
     def _solve_batch(self, fam: Family, op, pc, reqs):
         """Mixed-precision solves of reqs (len <= members) in lockstep on one
@@ -361,10 +392,191 @@ class SweepServer:
             ln.close()
         self._lanes = {}
 
+    # ------------------------------------------------------- HBM pool
+    def pool_used(self):
+        return sum(c.nbytes for c in self._pool)
+
+    def pool_summary(self):
+        """Lanes per family now, bytes admitted per lane, lanes added and retired."""
+        out = {}
+        for fam in self.families.values():
+            k = fam.key
+            out[str(k)] = {"lanes": sum(1 for c in self._pool if c.fam is fam),
+                           "lane_bytes": self.lane_bytes.get(k),
+                           "added": sum(1 for e in self.pool_events if e[0] == "add" and e[1] == k),
+                           "retired": sum(1 for e in self.pool_events
+                                          if e[0] == "retire" and e[1] == k)}
+        return {"budget_bytes": self.pool_bytes, "used_bytes": self.pool_used(),
+                "families": out}
+
+    def pool_peak(self):
+        """Largest sum of admitted lane bytes over the pool's history."""
+        used = peak = 0
+        for ev, _, nb, _ in self.pool_events:
+            used += nb if ev == "add" else -nb
+            peak = max(peak, used)
+        return peak
+
+    def _new_lane(self, fam):
+        """A lane for fam inside the pool: batched operator, shared
+        preconditioner handle, lane state and its own stream; its bytes are
+        measured once per family (operator, work, Krylov arenas)."""
+        import torch
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        op, pc = fam.add_slot(torch.cuda.Stream())
+        lane = self._lane(fam, op, pc)
+        if fam.key not in self.lane_bytes:
+            # one warm solve allocates the lane's arenas and captures its graph
+            lam = float(np.mean(fam.nodes))
+            op.interp(fam.node_ops, lagrange_weights(lam, fam.nodes), member=0)
+            lane.submit(0, fam.rhs(geo.C0 / lam * geo.N_EXT))
+            while not lane.step():
+                pass
+            lane.collect(0, host=False)
+            torch.cuda.synchronize()
+            free1, _ = torch.cuda.mem_get_info()
+            self.lane_bytes[fam.key] = max(int(free0 - free1), 1)
+        ctx = _LaneCtx(fam, op, pc, lane, self.lane_bytes[fam.key])
+        self._pool.append(ctx)
+        self.pool_events.append(("add", fam.key, ctx.nbytes, time.perf_counter()))
+        return ctx
+
+    def _drop_lane(self, ctx):
+        """Free a lane that has left the pool (its worker has stopped)."""
+        self._lanes.pop(id(ctx.op), None)
+        ctx.lane.close()
+        if ctx.pc is not None:
+            ctx.pc.close()
+        ctx.op.close()
+        ctx.fam.slots = [sl for sl in ctx.fam.slots if sl[0] is not ctx.op]
+        self._pool.remove(ctx)
+        self.pool_events.append(("retire", ctx.fam.key, ctx.nbytes, time.perf_counter()))
+
+    def prepare_pool(self, lanes_per_family=1):
+        """At least lanes_per_family lanes per family in the pool (each lane
+        measured and warm), within the budget."""
+        for fam in self.families.values():
+            while sum(1 for c in self._pool if c.fam is fam) < lanes_per_family:
+                if self._pool and self.pool_used() + self.lane_bytes.get(fam.key, 0) > \
+                        self.pool_bytes:
+                    break
+                self._new_lane(fam)
+
+    def close_pool(self):
+        for ctx in list(self._pool):
+            self._drop_lane(ctx)
+
+    def _serve_pool(self, requests, realtime, device_io):
+        """Continuous batching with lanes admitted and retired by footprint."""
+        queues = {k: deque() for k in self.families}
+        for r in sorted(requests, key=lambda r: r.arrival):
+            queues[r.key].append(r)
+        qlock = threading.Lock()
+        results = []
+        res_lock = threading.Lock()
+        errors = []
+        t0 = time.perf_counter()
+        pending = [len(requests)]
+
+        def arrived(key, now):
+            return sum(1 for r in queues[key] if not realtime or r.arrival <= now)
+
+        def worker(ctx):
+            fam, op, lane = ctx.fam, ctx.op, ctx.lane
+            q = queues[fam.key]
+            try:
+                while True:
+                    free = [m for m in range(lane.members) if m not in ctx.inflight]
+                    admit = []
+                    with qlock:
+                        if not ctx.retire:
+                            now = time.perf_counter() - t0
+                            while free and q and (not realtime or q[0].arrival <= now):
+                                admit.append((free.pop(0), q.popleft()))
+                    for m, req in admit:
+                        op.interp(fam.node_ops, lagrange_weights(req.lam, fam.nodes), member=m)
+                        if device_io is not None:
+                            dev_b, dev_x = device_io
+                            lane.submit_device(m, dev_b[req.rid].data_ptr(),
+                                               dev_x[req.rid].data_ptr())
+                        else:
+                            lane.submit(m, fam.rhs(geo.C0 / req.lam * geo.N_EXT))
+                        ctx.inflight[m] = (req, time.perf_counter() - t0)
+                    if not ctx.inflight:
+                        if ctx.retire or ctx.stop:
+                            return
+                        time.sleep(2e-4)
+                        continue
+                    for m in lane.step():
+                        req, start = ctx.inflight.pop(m)
+                        x, info = lane.collect(m, host=device_io is None)
+                        done = time.perf_counter() - t0
+                        with res_lock:
+                            results.append(Result(req.rid, req.key, req.lam,
+                                                  req.arrival if realtime else 0.0, start, done,
+                                                  info["iters"], info["relres"], info["flag"],
+                                                  x if self.cfg.keep_x else None))
+                            pending[0] -= 1
+            except Exception as e:  # surfaced after the threads join
+                errors.append(e)
+
+        def start(ctx):
+            ctx.stop = ctx.retire = False
+            ctx.thread = threading.Thread(target=worker, args=(ctx,), daemon=True)
+            ctx.thread.start()
+
+        for ctx in self._pool:
+            start(ctx)
+        try:
+            while pending[0] > 0 and not errors:
+                now = time.perf_counter() - t0
+                for fam in self.families.values():
+                    mine = [c for c in self._pool if c.fam is fam and not c.retire]
+                    with qlock:
+                        want = arrived(fam.key, now)
+                    free_slots = sum(c.lane.members - len(c.inflight) for c in mine)
+                    if want <= free_slots or want == 0:
+                        continue
+                    if self.max_lanes is not None and len(mine) >= self.max_lanes:
+                        continue
+                    need = self.lane_bytes.get(fam.key)
+                    if need is None or self.pool_used() + need > self.pool_bytes:
+                        # retire an idle lane of a family with nothing waiting
+                        # (every family keeps one lane, warm for its next request)
+                        for c in self._pool:
+                            if c.fam is fam or c.retire or c.inflight:
+                                continue
+                            if sum(1 for o in self._pool if o.fam is c.fam) <= 1:
+                                continue
+                            with qlock:
+                                waiting = arrived(c.fam.key, now)
+                            if waiting == 0:
+                                c.retire = True
+                                c.thread.join()
+                                self._drop_lane(c)
+                                break
+                    if need is None or self.pool_used() + need <= self.pool_bytes:
+                        start(self._new_lane(fam))
+                time.sleep(1e-3)
+        finally:
+            for ctx in self._pool:
+                ctx.stop = True
+            for ctx in self._pool:
+                if ctx.thread is not None:
+                    ctx.thread.join()
+        wall = time.perf_counter() - t0
+        if errors:
+            raise errors[0]
+        return sorted(results, key=lambda r: r.rid), wall
+
     def serve(self, requests, realtime=True, device_io=None):
         """Run the stream; returns (results, wall seconds).  device_io =
         (dev_b, dev_x) serves right-hand sides already in device memory and
         leaves the solutions there."""
+        if self.pool_bytes is not None and self.cfg.batching == "continuous" and \
+                self.cfg.mode == "mixed":
+            return self._serve_pool(requests, realtime, device_io)
         queues = {k: deque() for k in self.families}
         for r in sorted(requests, key=lambda r: r.arrival):
             queues[r.key].append(r)
