@@ -446,34 +446,21 @@ def run_sweep(args, world, rank, local):
             for pr in periods]
     setup_s = time.time() - t
     _progress("setup")
-    # admission by HBM footprint: lanes per length from one lane's bytes
+    # admission by HBM footprint: one device-memory pool for the lanes of
+    # every length, less room for the device-resident right-hand sides and
+    # solutions; lanes are admitted (and retired) by their measured bytes as
+    # the queues of the lengths fill, up to --sweep-slots lanes per length
     torch.cuda.synchronize()
     free0, total_mem = torch.cuda.mem_get_info()
-    fams[-1].add_slot()
-    torch.cuda.synchronize()
-    free1, _ = torch.cuda.mem_get_info()
-    lane_bytes = max(free0 - free1, 1)
-    # keep room for the device-resident right-hand sides and solutions
     io_bytes = 2 * 16 * len(lams) * sum(f.idx.size for f in fams)
-    budget = 0.6 * (free1 - io_bytes)
-    nslots = int(max(1, min(args.sweep_slots, budget // (lane_bytes * len(fams)))))
-    for f in fams:
-        while len(f.slots) < nslots:
-            f.add_slot()
-    # lanes run on torch streams, so the device-resident leg can stage
-    # right-hand sides on the same stream as the solve
-    for f in fams:
-        for op, pc in f.slots:
-            op.torch_stream = torch.cuda.Stream()
-            op.set_stream(op.torch_stream.cuda_stream)
+    budget = int(0.6 * (free0 - io_bytes))
     reqs = sv.poisson_stream(items, rate=args.sweep_rate, seed=args.seed + rank)
     cfg = sv.ServeConfig(tol=args.tol, side=args.sweep_side, batching=args.sweep_batching,
                          inner_tol=args.inner_tol)
-    srv = sv.SweepServer(fams, cfg)
-    srv.prepare_device()
-    # common warm-up: a full batch on every lane (captures the cycle graphs),
-    # then W steps' worth of requests at wavelengths between the sweep's
-    srv.warm()
+    srv = sv.SweepServer(fams, cfg, pool_bytes=budget, max_lanes=args.sweep_slots)
+    srv.prepare_pool(1)
+    # common warm-up: W steps' worth of requests at wavelengths between the
+    # sweep's (admits the lanes the queues ask for and captures their graphs)
     n_warm = max(len(periods), int(round(args.warmup * per_step)))
     wl = np.linspace(band[0], band[1], n_warm // len(periods) + 2)[1:-1]
     srv.serve([sv.Request(-1 - i, pr, lam, 0.0)
@@ -481,7 +468,6 @@ def run_sweep(args, world, rank, local):
     torch.cuda.synchronize()
     _progress(f"warm ({n_warm} requests)")
     fam_of = {f.key: f for f in fams}
-    lane_ops = [op for f in fams for op, _ in f.slots]
     clocks = None if args.no_clocks else Clocks(local)
     if clocks:
         clocks.start()
@@ -504,6 +490,7 @@ def run_sweep(args, world, rank, local):
     dev_x = {r.rid: torch.empty_like(dev_b[r.rid]) for r in reqs}
     torch.cuda.synchronize()
     # leg 2: device-resident
+    lane_ops = [op for f in fams for op, _ in f.slots]
     l0 = sum(op.launches() for op in lane_ops)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -515,7 +502,12 @@ def run_sweep(args, world, rank, local):
     clk = clocks.stop() if clocks else {"sm_mhz": None, "sm_max_mhz": None,
                                         "reasons": ["not sampled (--no-clocks)"]}
     dev_s = e0.elapsed_time(e1) / 1e3
-    launches = sum(op.launches() for op in lane_ops) - l0 + 10 * len(reqs)
+    lane_ops_end = [op for f in fams for op, _ in f.slots]
+    launches = (sum(op.launches() for op in lane_ops_end if op in lane_ops) - l0 +
+                sum(op.launches() for op in lane_ops_end if op not in lane_ops) +
+                10 * len(reqs))
+    pool = srv.pool_summary()
+    pool["peak_bytes"] = srv.pool_peak()
     summ_dev = sv.summarize(res_dev, wall_dev)
     _progress(f"device-resident stream: {len(reqs)} solves in {dev_s:.2f} s")
     # roofline of the dominant kernel: the inverse-block apply of one lane of
@@ -546,13 +538,8 @@ def run_sweep(args, world, rank, local):
                        "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm}}
     # the lanes are done: free them and the staged vectors before the baseline
     del dev_b, dev_x
-    srv._bufs.clear()
+    srv.close_pool()
     srv.close()
-    for f in fams:
-        for op, pc in f.slots:
-            pc.close()
-            op.close()
-        f.slots = []
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     _progress("lanes released")
@@ -614,8 +601,9 @@ def run_sweep(args, world, rank, local):
                            "tol": args.tol, "restart": args.restart,
                            "solver": f"complex64 GMRES + FP64 refinement, {args.sweep_batching} "
                                      f"batching",
-                           "lanes_per_length": nslots, "members_per_lane": K,
-                           "lane_bytes": int(lane_bytes), "setup_s": round(setup_s, 1),
+                           "admission": "HBM pool", "members_per_lane": K,
+                           "max_lanes_per_length": args.sweep_slots,
+                           "pool": pool, "setup_s": round(setup_s, 1),
                            "warmup_requests": n_warm,
                            "legs": "common warm-up, then e2e (host buffers) first and the "
                                    "device-resident stream second, on the same lanes",
@@ -713,7 +701,12 @@ def run_microdisk(args, world, rank, local):
     clk = clocks.stop() if clocks else {"sm_mhz": None, "sm_max_mhz": None,
                                         "reasons": ["not sampled (--no-clocks)"]}
     dev_s = e0.elapsed_time(e1) / 1e3
-    launches = sum(op.launches() for op in lane_ops) - l0 + 10 * len(reqs)
+    lane_ops_end = [op for f in fams for op, _ in f.slots]
+    launches = (sum(op.launches() for op in lane_ops_end if op in lane_ops) - l0 +
+                sum(op.launches() for op in lane_ops_end if op not in lane_ops) +
+                10 * len(reqs))
+    pool = srv.pool_summary()
+    pool["peak_bytes"] = srv.pool_peak()
     summ = sv.summarize(res, wall)
     _progress(f"device-resident: {len(reqs)} solves in {dev_s:.2f} s")
     res_h, wall_h = srv.serve(reqs, realtime=False)
