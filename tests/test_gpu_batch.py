@@ -111,7 +111,9 @@ def test_stage_profile_of_a_batch(family):
     op = vb.Operator(p.Mop(), p.Gram, idx, G=Gs[1], members=4)
     pcb = pc.share(op)
     st = op.profile_stages(pcb, prec="c64", restart=20, kgs=5, reps=3)
-    assert all(v > 0 for v in st.values())
+    # on the two-read Gram-Schmidt path (restart <= 50) the column finish
+    # includes the scaling, so gs_scale is not a separate launch
+    assert all(v > 0 for k, v in st.items() if k != "gs_scale")
     pcb.close()
     op.close()
 

@@ -70,7 +70,9 @@ def test_jvie_solve_matches_oracle(case):
     # the fN form of the same call (circulant_nop_const layout)
     Je2, flag2, *_ = vb.JVIE_Solver_const(Einc, p.e_r, grid_r(p), p.freq, fN=fN, tol=1e-8,
                                           solver="G", inner_it=30, outer_it=20)
-    assert flag2 == 0 and rel(Je2, Je) < 1e-9
+    # fN transformed by numpy vs by the device from G: rounding-level operator
+    # differences, amplified by the solve at 1e-8
+    assert flag2 == 0 and rel(Je2, Je) < 1e-7
 
 
 @pytest.mark.parametrize("solver,prec", [("G", "c64"), ("D", "c128"), ("B", "c128")])

@@ -1099,15 +1099,16 @@ __global__ void __launch_bounds__(kInvThreads) k_pc_inv_apply(
 // modes f and L-f of every member), with the block's rows streamed through a
 // shared-memory ring by bulk asynchronous copies: one producer warp issues, per
 // stage, KC column segments of the CTA's 128 rows (one copy each, no
-// registers held by the loads), and the 256 consumer threads multiply out of
+// registers held by the loads), and 512 consumer threads (64 row pairs x 8
+// column groups, enough warps to keep the FMA pipes issuing) multiply out of
 // shared memory.  Up to kStrMaxStages stages are in flight per CTA, which is
-// what keeps HBM busy; the per-thread arithmetic, its order and the final sum
-// of the four column groups are those of k_pc_inv_apply, so the two kernels
-// give the same bits.  grid (ld / 128 rounded up, blocks), kStrThreads
-// threads, shared memory str_smem().
+// what keeps HBM busy.  Each group sums its columns in increasing order and the
+// eight group sums are added in a fixed order, so a column's result does not
+// depend on P or on the other members.  grid (ld / 128 rounded up, blocks),
+// kStrThreads threads, shared memory str_smem().
 constexpr int kStrRows = 128;
-constexpr int kStrGroups = 4;
-constexpr int kStrConsumers = (kStrRows / 2) * kStrGroups;  // 256
+constexpr int kStrGroups = 8;
+constexpr int kStrConsumers = (kStrRows / 2) * kStrGroups;  // 512
 constexpr int kStrThreads = kStrConsumers + 32;             // + one producer warp
 constexpr int kStrMaxStages = 8;
 
@@ -1129,7 +1130,7 @@ inline size_t str_smem(int ld, int P, int stages) {
   return xr > red ? xr : red;
 }
 
-// named barrier of the 256 consumer threads (the producer warp may have left)
+// named barrier of the consumer threads (the producer warp may have left)
 __device__ __forceinline__ int consumers_sync_or(int pred) {
   int r;
   asm volatile(
