@@ -344,8 +344,8 @@ static const int kSmemCap = 220 * 1024;
 // when a plane does not fit in shared memory, else the general k_plane.
 template <typename R>
 static bool plane64_ok(const OpGeom& g) {
-  return !g.split && g.Py == kPlPy && g.Pz == kPlPz && g.M <= kPlPy && g.N <= kPlPz &&
-         plane64_smem<R>(g.N) <= (size_t)kSmemCap;
+  return !g.split && g.sym && g.Py == kPlPy && g.Pz == kPlPz && g.M <= kPlPy &&
+         3 * g.N <= kPlRowsPerWarp * (kPlThreads / 32) && plane64_smem<R>(g.N) <= (size_t)kSmemCap;
 }
 
 template <typename R>

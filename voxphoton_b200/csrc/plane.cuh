@@ -13,8 +13,9 @@
 //   C  inverse y-FFT of the rows, one warp per row, five shuffle (radix-2 DIT)
 //      steps on the bit-reversed input and one in-lane step, natural order
 //      out, cropped to M.
-// One CTA per (kx, member); three barriers per plane.  Arithmetic as k_plane
-// (no scaling here: 1/P is applied by k_xinv).
+// One CTA per (kx, member); three barriers per plane; the plane's octant of fN
+// is staged in shared memory while the rows are transformed.  Arithmetic as
+// k_plane (no scaling here: 1/P is applied by k_xinv).
 #pragma once
 
 #include "mvp.cuh"
@@ -28,10 +29,16 @@ constexpr int kPlSy = kPlPy + 1;  // row stride of the y-transformed plane
 
 __device__ __forceinline__ int brev5(int v) { return (int)(__brev((unsigned)v) >> 27); }
 
-// shared memory: y-transformed rows [3N][65] + z spectra [3][64][24 + 1]
+// the plane's octant of fN: (Py/2 + 1) x (Pz/2 + 1) x 6
+constexpr int kPlFn = (kPlPy / 2 + 1) * (kPlPz / 2 + 1) * 6;
+// rows one warp preloads in phases A and C (3N <= 36 rows over 8 warps)
+constexpr int kPlRowsPerWarp = 5;
+
+// shared memory: y-transformed rows [3N][65] + z spectra [3][64][24 + 1] + the
+// plane's octant of fN
 template <typename R>
 constexpr size_t plane64_smem(int N) {
-  return ((size_t)3 * N * kPlSy + (size_t)3 * kPlPy * (kPlPz + 1)) * sizeof(Cx<R>);
+  return ((size_t)3 * N * kPlSy + (size_t)3 * kPlPy * (kPlPz + 1) + kPlFn) * sizeof(Cx<R>);
 }
 
 template <typename C>
@@ -123,12 +130,20 @@ __global__ void __launch_bounds__(kPlThreads, 2)
   const int rows = 3 * N;
   C* yb = reinterpret_cast<C*>(smem_raw);  // [3N][kPlSy], columns bit-reversed
   C* zb = yb + (size_t)rows * kPlSy;        // [3][64][25] z spectra
+  C* fsm = zb + (size_t)3 * kPlPy * (kPlPz + 1);  // the plane's fN octant
   const int kx = blockIdx.x;
   const C* tin = T1 + (long long)kx * rows * M;
   C* tout = T2 + (long long)kx * rows * M;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // fN is stored as one octant (the operator's parity holds: plane64_ok)
+  const int fx = 2 * kx > g.Px;
+  const int hy = g.Py / 2 + 1, hz = g.Pz / 2 + 1;
+  {
+    const C* fplane = fN + (long long)(fx ? g.Px - kx : kx) * hy * hz * 6;
+    for (int t = tid; t < kPlFn; t += kPlThreads) fsm[t] = fplane[t];
+  }
 
-  // ---- A: forward y-FFT, one warp per row
+  // ---- A: forward y-FFT, one warp per row (the warp's rows loaded first)
   {
     C tw[5];
 #pragma unroll
@@ -137,11 +152,19 @@ __global__ void __launch_bounds__(kPlThreads, 2)
       tw[s] = tw_get(twY, (lane & (h - 1)) * (32 / h), -1);  // W_{2h}^{j} = W64^{j*32/h}
     }
     const C w64 = tw_get(twY, lane, -1);
-    for (int r = warp; r < rows; r += kPlThreads / 32) {
-      const C x0 = lane < M ? tin[(long long)r * M + lane] : czero<C>();
-      const C x1 = lane + 32 < M ? tin[(long long)r * M + 32 + lane] : czero<C>();
-      C a = cadd(x0, x1);
-      C b = cmul(csub(x0, x1), w64);
+    C x0[kPlRowsPerWarp], x1[kPlRowsPerWarp];
+#pragma unroll
+    for (int i = 0; i < kPlRowsPerWarp; i++) {
+      const int r = warp + i * (kPlThreads / 32);
+      x0[i] = (r < rows && lane < M) ? tin[(long long)r * M + lane] : czero<C>();
+      x1[i] = (r < rows && lane + 32 < M) ? tin[(long long)r * M + 32 + lane] : czero<C>();
+    }
+#pragma unroll
+    for (int i = 0; i < kPlRowsPerWarp; i++) {
+      const int r = warp + i * (kPlThreads / 32);
+      if (r >= rows) break;
+      C a = cadd(x0[i], x1[i]);
+      C b = cmul(csub(x0[i], x1[i]), w64);
       a = warp_dif32(a, tw, lane);
       b = warp_dif32(b, tw, lane);
       // lane l: X[2 br(l)] (a) and X[2 br(l) + 1] (b): bit-reversed order of 64
@@ -152,9 +175,6 @@ __global__ void __launch_bounds__(kPlThreads, 2)
   __syncthreads();
 
   // ---- B: z-FFT per (column, component), product, inverse z-FFT
-  const int fx = g.sym && (2 * kx > g.Px);
-  const int hy = g.sym ? g.Py / 2 + 1 : g.Py, hz = g.sym ? g.Pz / 2 + 1 : g.Pz;
-  const C* fplane = fN + (long long)(fx ? g.Px - kx : kx) * hy * hz * 6;
   const int j = tid % kPlPy;  // physical column
   const int c = tid / kPlPy;  // component (threads 192..255 idle in B)
   const int ky = j < 32 ? 2 * brev5(j) : 2 * brev5(j - 32) + 1;
@@ -170,7 +190,7 @@ __global__ void __launch_bounds__(kPlThreads, 2)
   }
   __syncthreads();
   if (c < 3) {
-    const int fy = g.sym && (2 * ky > g.Py);
+    const int fy = 2 * ky > g.Py;
     const int yo = fy ? g.Py - ky : ky;
     // row c of the symmetric tensor: components (c,0), (c,1), (c,2) of
     // [xx, xy, xz, yy, yz, zz]
@@ -183,8 +203,8 @@ __global__ void __launch_bounds__(kPlThreads, 2)
     C P[kPlPz], y[kPlPz];
 #pragma unroll
     for (int kz = 0; kz < kPlPz; kz++) {
-      const int fz = g.sym && (2 * kz > g.Pz);
-      const C* f = fplane + ((long long)yo * hz + (fz ? g.Pz - kz : kz)) * 6;
+      const int fz = 2 * kz > g.Pz;
+      const C* f = fsm + (yo * hz + (fz ? g.Pz - kz : kz)) * 6;
       // octant parity: xy flips with fx^fy, xz with fx^fz, yz with fy^fz
       C f0 = f[i0], f1 = f[i1], f2 = f[i2];
       const R sxy = (fx ^ fy) ? (R)-1 : (R)1, sxz = (fx ^ fz) ? (R)-1 : (R)1,
