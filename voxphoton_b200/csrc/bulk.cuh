@@ -75,6 +75,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   return false;
 }
 
+// named barrier `id` over NT threads, true in all of them if pred is true in any
+template <int NT>
+__device__ __forceinline__ int named_bar_or(int id, int pred) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.s32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(pred), "r"(id), "n"(NT)
+      : "memory");
+  return r;
+}
+
 // bytes (a multiple of 16, both addresses 16-byte aligned) from global src to
 // shared dst, completing on bar's transaction count
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,

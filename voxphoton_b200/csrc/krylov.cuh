@@ -589,35 +589,52 @@ __global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x
 //                     column with ||w''||^2 = ||w'||^2 - ||h2||^2 (w'' = w' - V h2
 //                     and h2 = V^H w' with V orthonormal);
 //   k_gs_finish:      V(:,k+1) = (w' - V h2) / ||w''||.
-// The two passes stage each chunk of gs_rows() rows of all k+1 basis columns
-// (and of w) in shared memory with bulk asynchronous copies, two chunks in
-// flight per CTA; the dot products run out of shared memory, one warp per
-// column, accumulating in FP64 in a fixed order (deterministic).
+// The two passes are producer/consumer pipelines: one producer warp streams
+// chunks of gs_rows() rows of all k+1 basis columns and of w into a ring of
+// shared-memory stages with bulk asynchronous copies (mbarrier completion,
+// bounded waits), and eight consumer warps take the dot products out of shared
+// memory, one warp per column, accumulating in FP64 in a fixed order
+// (deterministic); the update of w' (pass<true>) runs one thread per row
+// before the dots of the same stage.
 constexpr int kGsMaxCols = 51;
-constexpr int kGsWarps = kRedThreads / 32;
+constexpr int kGsWarps = kRedThreads / 32;  // consumer warps
+constexpr int kGsThreads = kRedThreads + 32;  // + one producer warp
 constexpr int kGsColsPerWarp = (kGsMaxCols + kGsWarps - 1) / kGsWarps;
 constexpr int kGsBlocks = 296;  // two CTAs per SM on 148 SMs
+constexpr int kGsMaxStages = 6;
+constexpr size_t kGsSmemBudget = 100 * 1024;
 
 template <typename R>
 constexpr int gs_rows() {
   return sizeof(R) == 4 ? 128 : 64;
 }
-// two stages of [nj][rows] basis values + [rows] of w
+// ring stages of [nj + 1][rows] (basis columns and w) within the budget
+template <typename R>
+inline int gs_stages(int nj) {
+  const size_t st = ((size_t)nj + 1) * gs_rows<R>() * sizeof(Cx<R>);
+  const size_t s = kGsSmemBudget / st;
+  return (int)(s < 2 ? 2 : (s > kGsMaxStages ? kGsMaxStages : s));
+}
 template <typename R>
 inline size_t gs_pass_smem(int nj) {
-  return 2ull * ((size_t)nj + 1) * gs_rows<R>() * sizeof(Cx<R>);
+  return (size_t)gs_stages<R>(nj) * ((size_t)nj + 1) * gs_rows<R>() * sizeof(Cx<R>);
+}
+
+__device__ __forceinline__ void consumer_bar() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kRedThreads) : "memory");
 }
 
 template <typename R, bool kUpdate>
-__global__ void __launch_bounds__(kRedThreads, 2) k_gs_pass(GmresDev* st, int k,
-                                                            const Cx<R>* __restrict__ V,
-                                                            long long ldv, Cx<R>* w, long long n,
-                                                            long long vs) {
+__global__ void __launch_bounds__(kGsThreads, 2) k_gs_pass(GmresDev* st, int k,
+                                                           const Cx<R>* __restrict__ V,
+                                                           long long ldv, Cx<R>* w, long long n,
+                                                           long long vs, int stages) {
   using C = Cx<R>;
   constexpr int RW = gs_rows<R>();
   __shared__ double2 sh[32];
   __shared__ C hs[kGsMaxCols];
-  __shared__ __align__(8) uint64_t full[2];
+  __shared__ __align__(8) uint64_t full[kGsMaxStages];
+  __shared__ __align__(8) uint64_t empty[kGsMaxStages];
   __shared__ double2 tot[1];
   extern __shared__ __align__(128) unsigned char smem_raw[];
   st += blockIdx.y;
@@ -628,45 +645,52 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gs_pass(GmresDev* st, int k,
   const size_t stage = ((size_t)nj + 1) * RW;  // elements of one stage
   C* buf = reinterpret_cast<C*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long nch = (n + RW - 1) / RW;
+  const int mine = nch > blockIdx.x ? (int)((nch - 1 - blockIdx.x) / gridDim.x + 1) : 0;
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
+    for (int s = 0; s < stages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kGsWarps);
+    }
     mbar_init_fence();
   }
   if (kUpdate)
     for (int j = tid; j < nj; j += blockDim.x) hs[j] = from_d2<C>(st->h1[j]);
   __syncthreads();
-  const long long nch = (n + RW - 1) / RW;
-  // the copies of chunk c into stage s (warp 0: lane j copies column j,
-  // j = nj is w); sizes round up to 16 bytes inside the column padding
-  auto issue = [&](long long c, int s) {
-    const long long r0 = c * RW;
-    const int rows = (int)min((long long)RW, n - r0);
-    const unsigned bytes = (unsigned)(((size_t)rows * sizeof(C) + 15) / 16 * 16);
-    if (lane == 0) mbar_arrive_expect_tx(&full[s], bytes * (nj + 1));
-    __syncwarp();
-    C* dst = buf + (size_t)s * stage;
-    for (int j = lane; j <= nj; j += 32) {
-      const C* src = (j < nj) ? V + (long long)j * ldv + r0 : w + r0;
-      bulk_g2s(dst + (size_t)j * RW, src, bytes, &full[s]);
+  if (warp == kGsWarps) {
+    // producer: chunk i of this CTA into stage i % stages; lane j copies
+    // column j (j = nj is w), sizes rounded up to 16 bytes inside the padding
+    for (int i = 0; i < mine; i++) {
+      const int s = i % stages;
+      if (i >= stages && !mbar_wait(&empty[s], ((i / stages) - 1) & 1)) return;
+      const long long r0 = (blockIdx.x + (long long)i * gridDim.x) * RW;
+      const int rows = (int)min((long long)RW, n - r0);
+      const unsigned bytes = (unsigned)(((size_t)rows * sizeof(C) + 15) / 16 * 16);
+      if (lane == 0) mbar_arrive_expect_tx(&full[s], bytes * (nj + 1));
+      __syncwarp();
+      C* dst = buf + (size_t)s * stage;
+      for (int j = lane; j <= nj; j += 32) {
+        const C* src = (j < nj) ? V + (long long)j * ldv + r0 : w + r0;
+        bulk_g2s(dst + (size_t)j * RW, src, bytes, &full[s]);
+      }
     }
-  };
+    return;
+  }
   double2 acc[kGsColsPerWarp];
 #pragma unroll
   for (int q = 0; q < kGsColsPerWarp; q++) acc[q] = make_double2(0.0, 0.0);
   double nrm = 0.0;
-  int it = 0, failed = 0;
-  if (warp == 0 && blockIdx.x < nch) issue(blockIdx.x, 0);
-  for (long long c = blockIdx.x; c < nch; c += gridDim.x, it++) {
-    const int s = it & 1;
-    // prefetch the next chunk into the other stage (freed by the last barrier)
-    if (warp == 0 && c + gridDim.x < nch) issue(c + gridDim.x, s ^ 1);
-    if (!mbar_wait(&full[s], (it >> 1) & 1)) failed = 1;
-    if (__syncthreads_or(failed)) return;
+  // a consumer whose wait gave up keeps taking part in every consumer barrier
+  // (its later waits return at once: the error word is set) and skips the work
+  int failed = 0;
+  for (int i = 0; i < mine; i++) {
+    const int s = i % stages;
+    const bool ok = mbar_wait(&full[s], (i / stages) & 1);
+    failed |= !ok;
     const C* Vs = buf + (size_t)s * stage;
     C* ws = buf + (size_t)s * stage + (size_t)nj * RW;
-    const long long r0 = c * RW;
-    const int rows = (int)min((long long)RW, n - r0);
+    const long long r0 = (blockIdx.x + (long long)i * gridDim.x) * RW;
+    const int rows = ok ? (int)min((long long)RW, n - r0) : 0;
     if (kUpdate) {
       if (tid < rows) {
         C wi = ws[tid];
@@ -680,22 +704,23 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gs_pass(GmresDev* st, int k,
         w[r0 + tid] = wi;
         nrm += (double)wi.x * wi.x + (double)wi.y * wi.y;
       }
-      __syncthreads();
+      consumer_bar();
     }
 #pragma unroll
     for (int q = 0; q < kGsColsPerWarp; q++) {
       const int j = warp + q * kGsWarps;
       if (j < nj) {
-        for (int i = lane; i < rows; i += 32) {
-          const double2 v = to_d2(Vs[(size_t)j * RW + i]);
-          const double2 x = to_d2(ws[i]);
+        for (int r = lane; r < rows; r += 32) {
+          const double2 v = to_d2(Vs[(size_t)j * RW + r]);
+          const double2 x = to_d2(ws[r]);
           acc_cdot(acc[q], v.x, v.y, x.x, x.y);
         }
       }
     }
-    // every thread is done with stage s before warp 0 refills it
-    __syncthreads();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
   }
+  if (named_bar_or<kRedThreads>(1, failed)) return;  // nothing of this CTA is reduced
 #pragma unroll
   for (int q = 0; q < kGsColsPerWarp; q++) {
     const int j = warp + q * kGsWarps;
@@ -703,22 +728,47 @@ __global__ void __launch_bounds__(kRedThreads, 2) k_gs_pass(GmresDev* st, int k,
     if (j < nj && lane == 0) st->partial[j * gridDim.x + blockIdx.x] = v;
   }
   if (kUpdate) {
-    const double2 t = block_sum(make_double2(nrm, 0.0), sh);
-    if (tid == 0) st->partial[nj * gridDim.x + blockIdx.x] = t;
+    // consumer-only block sum of ||w'||^2
+    double2 t = make_double2(nrm, 0.0);
+    t = warp_sum(t);
+    if (lane == 0) sh[warp] = t;
+    consumer_bar();
+    if (tid == 0) {
+      double2 a = make_double2(0.0, 0.0);
+      for (int q = 0; q < kGsWarps; q++) a.x += sh[q].x;
+      st->partial[nj * gridDim.x + blockIdx.x] = a;
+    }
   }
-  if (last_block(&st->ticket)) {
-    if (!kUpdate) {
-      reduce_partials(st->partial, nj, gridDim.x, st->h1, sh);
-      if (tid == 0) st->ticket = 0;
-    } else {
-      reduce_partials(st->partial, nj, gridDim.x, st->h2, sh);
-      reduce_partials(st->partial + (size_t)nj * gridDim.x, 1, gridDim.x, tot, sh);
-      if (tid == 0) {
-        st->ticket = 0;
-        double hh = 0.0;
-        for (int j = 0; j < nj; j++) hh += st->h2[j].x * st->h2[j].x + st->h2[j].y * st->h2[j].y;
-        gs_column(st, k, sqrt(fmax(tot[0].x - hh, 0.0)));
-      }
+  // the last CTA (consumer threads only: the producer warp has left)
+  __shared__ bool amlast;
+  __threadfence();
+  consumer_bar();
+  if (tid == 0) amlast = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+  consumer_bar();
+  if (!amlast) return;
+  __threadfence();
+  const int nr = kUpdate ? nj + 1 : nj;
+  for (int j = warp; j < nr; j += kGsWarps) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int b = lane; b < (int)gridDim.x; b += 32) {
+      const double2 p = __ldcg(&st->partial[j * gridDim.x + b]);
+      v.x += p.x;
+      v.y += p.y;
+    }
+    v = warp_sum(v);
+    if (lane == 0) {
+      if (!kUpdate) st->h1[j] = v;
+      else if (j < nj) st->h2[j] = v;
+      else tot[0] = v;
+    }
+  }
+  consumer_bar();
+  if (tid == 0) {
+    st->ticket = 0;
+    if (kUpdate) {
+      double hh = 0.0;
+      for (int j = 0; j < nj; j++) hh += st->h2[j].x * st->h2[j].x + st->h2[j].y * st->h2[j].y;
+      gs_column(st, k, sqrt(fmax(tot[0].x - hh, 0.0)));
     }
   }
 }

@@ -97,21 +97,36 @@ __global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>*
   const int c = blockIdx.z - 3 * mb;
   const int YB = g.ybx;
   const long long cellbase = (long long)g.L * ((long long)g.M * z);
-  // gather J along x for YB pencils; zero-pad
-  for (int t = threadIdx.x; t < YB * g.Px; t += blockDim.x) {
-    const int yb = t / g.Px;
-    const int x = t - yb * g.Px;
-    const int y = y0 + yb;
-    C v = czero<C>();
-    if (x < g.L && y < g.M) {
-      const long long cell = cellbase + (long long)g.L * y + x;
-      const int m = vmap[(long long)c * g.V + cell];
-      if (m >= 0) {
-        v = in[m];
-        if (mode == MV_AN_T) v = cmul(Mc[cell], cconj(v));  // conj(conj(Mc) .* J)
-      }
+  // gather J along x for YB pencils; zero-pad.  Batches of kGather elements
+  // per thread: the index-map loads, then the vector loads, then the stores,
+  // so a thread keeps several dependent global reads in flight.
+  constexpr int kGather = 4;
+  for (int t0 = threadIdx.x; t0 < YB * g.Px; t0 += kGather * blockDim.x) {
+    int mm[kGather];
+    long long cl[kGather];
+#pragma unroll
+    for (int u = 0; u < kGather; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int yb = t / g.Px;
+      const int x = t - yb * g.Px;
+      const int y = y0 + yb;
+      mm[u] = -1;
+      cl[u] = cellbase + (long long)g.L * y + x;
+      if (t < YB * g.Px && x < g.L && y < g.M) mm[u] = vmap[(long long)c * g.V + cl[u]];
     }
-    bufA[(size_t)yb * g.sx + x] = v;
+    C v[kGather];
+#pragma unroll
+    for (int u = 0; u < kGather; u++) v[u] = mm[u] >= 0 ? in[mm[u]] : czero<C>();
+#pragma unroll
+    for (int u = 0; u < kGather; u++) {
+      const int t = t0 + u * blockDim.x;
+      if (t >= YB * g.Px) break;
+      const int yb = t / g.Px;
+      const int x = t - yb * g.Px;
+      C w = v[u];
+      if (mode == MV_AN_T && mm[u] >= 0) w = cmul(Mc[cl[u]], cconj(w));  // conj(conj(Mc) .* J)
+      bufA[(size_t)yb * g.sx + x] = w;
+    }
   }
   __syncthreads();
   C* res = block_fft(bufA, bufB, px, YB, g.sx, tw, -1);
@@ -427,28 +442,49 @@ __global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>*
   __syncthreads();
   C* res = block_fft(bufA, bufB, px, YB, g.sx, tw, +1);
   const long long cellbase = (long long)g.L * ((long long)g.M * z);
-  for (int t = threadIdx.x; t < YB * g.L; t += blockDim.x) {
-    const int yb = t / g.L;
-    const int x = t - yb * g.L;
-    if (yb >= ny) continue;
-    const long long cell = cellbase + (long long)g.L * (y0 + yb) + x;
-    const int m = vmap[(long long)c * g.V + cell];
-    if (m < 0) continue;
-    const C nj = cscale(res[(size_t)yb * g.sx + x], scale);
-    const C J = in[m];
-    C o;
-    if (mode == MV_AN) {
-      C a = cscale(J, gram);
-      if (Mr) a = cmul(Mr[cell], a);
-      o = csub(a, cmul(Mc[cell], nj));
-    } else if (mode == MV_AN_T) {
-      C a = cscale(J, gram);
-      if (Mr) a = cmul(cconj(Mr[cell]), a);
-      o = csub(a, cconj(nj));
-    } else {
-      o = csub(nj, cscale(J, gram));
+  // batches of kScatter elements per thread: index-map loads, then the
+  // vector and contrast loads, then the combination and the stores
+  constexpr int kScatter = 4;
+  for (int t0 = threadIdx.x; t0 < YB * g.L; t0 += kScatter * blockDim.x) {
+    int mm[kScatter];
+    long long cl[kScatter];
+#pragma unroll
+    for (int u = 0; u < kScatter; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int yb = t / g.L;
+      const int x = t - yb * g.L;
+      mm[u] = -1;
+      cl[u] = cellbase + (long long)g.L * (y0 + yb) + x;
+      if (t < YB * g.L && yb < ny) mm[u] = vmap[(long long)c * g.V + cl[u]];
     }
-    out[m] = cscale(o, out_scale);
+    C J[kScatter], mc[kScatter];
+#pragma unroll
+    for (int u = 0; u < kScatter; u++) {
+      J[u] = mm[u] >= 0 ? in[mm[u]] : czero<C>();
+      mc[u] = (mm[u] >= 0 && mode == MV_AN) ? Mc[cl[u]] : czero<C>();
+    }
+#pragma unroll
+    for (int u = 0; u < kScatter; u++) {
+      if (mm[u] < 0) continue;
+      const int t = t0 + u * blockDim.x;
+      const int yb = t / g.L;
+      const int x = t - yb * g.L;
+      const long long cell = cl[u];
+      const C nj = cscale(res[(size_t)yb * g.sx + x], scale);
+      C o;
+      if (mode == MV_AN) {
+        C a = cscale(J[u], gram);
+        if (Mr) a = cmul(Mr[cell], a);
+        o = csub(a, cmul(mc[u], nj));
+      } else if (mode == MV_AN_T) {
+        C a = cscale(J[u], gram);
+        if (Mr) a = cmul(cconj(Mr[cell]), a);
+        o = csub(a, cconj(nj));
+      } else {
+        o = csub(nj, cscale(J[u], gram));
+      }
+      out[mm[u]] = cscale(o, out_scale);
+    }
   }
 }
 

@@ -75,6 +75,13 @@ __device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b
   a = p[0];
   b = p[1];
 }
+__device__ __forceinline__ void st_pair(float2* p, float2 a, float2 b) {
+  *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void st_pair(double2* p, double2 a, double2 b) {
+  p[0] = a;
+  p[1] = b;
+}
 
 // --------------------------------------------------------------- apply: x-FFT
 // kBig: the x length L has a prime factor above 13 (compiled big-prime
@@ -1180,25 +1187,10 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     }
     mbar_init_fence();
   }
-  for (int b = 0; b < KS; b++) {
-    const C* T1 = Tin + b * wstride + (long long)f * n;
-    const C* T2 = Tin + b * wstride + (long long)(two ? i2 : f) * n;
-    for (int k = tid; k < ld; k += blockDim.x) {
-      C v1 = czero<C>(), v2 = czero<C>();
-      if (b < km && k < n) {
-        v1 = T1[k];
-        if (two) {
-          v2 = T2[k];
-          if (k < MN) v2 = cscale(v2, (R)-1);
-        }
-      }
-      X[P * k + 2 * b] = v1;
-      X[P * k + 2 * b + 1] = v2;
-    }
-  }
   __syncthreads();
   if (tid >= kStrConsumers) {
-    // producer warp: lane j copies column j of each stage
+    // producer warp: lane j copies column j of each stage; it starts at once,
+    // while the consumers gather the right-hand sides
     const int lane = tid & 31;
     const C* Bf = Binv + (long long)f * ld * ld + r0;
     const unsigned bytes = (unsigned)(nrows * sizeof(C));
@@ -1213,6 +1205,34 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     }
     return;
   }
+  // right-hand sides X[k][2b + (0 | 1)] = (T_f, D T_{L-f}) of member b, member
+  // fastest (one 16-byte pair per thread and row), loads issued in batches
+  {
+    constexpr int kU = 4;
+    const int tot = KS * ld;
+    for (int t0 = tid; t0 < tot; t0 += kU * kStrConsumers) {
+      C v1[kU], v2[kU];
+#pragma unroll
+      for (int u = 0; u < kU; u++) {
+        const int t = t0 + u * kStrConsumers;
+        const int b = t % KS, k = t / KS;
+        v1[u] = v2[u] = czero<C>();
+        if (t < tot && b < km && k < n) {
+          v1[u] = Tin[b * wstride + (long long)f * n + k];
+          if (two) {
+            v2[u] = Tin[b * wstride + (long long)i2 * n + k];
+            if (k < MN) v2[u] = cscale(v2[u], (R)-1);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kU; u++) {
+        const int t = t0 + u * kStrConsumers;
+        if (t < tot) st_pair(X + (size_t)P * (t / KS) + 2 * (t % KS), v1[u], v2[u]);
+      }
+    }
+  }
+  consumers_sync_or(0);
   const int rp = tid % (kStrRows / 2);  // row pair within the chunk
   const int kg = tid / (kStrRows / 2);  // column group
   const bool active = 2 * rp < nrows;
@@ -1252,12 +1272,11 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   }
   // every consumer past its last stage (or one gave up): the ring and X are free
   if (consumers_sync_or(failed)) return;
-  C* red = X;  // red[(kg * kStrRows + row) * P + col]
+  // partial sums red[(q * groups + kg) * kStrRows + row]: rows of a warp adjacent
+  C* red = X;
 #pragma unroll
-  for (int q = 0; q < P; q++) {
-    red[(kg * kStrRows + 2 * rp) * P + q] = a0[q];
-    red[(kg * kStrRows + 2 * rp + 1) * P + q] = a1[q];
-  }
+  for (int q = 0; q < P; q++)
+    st_pair(red + ((size_t)q * kStrGroups + kg) * kStrRows + 2 * rp, a0[q], a1[q]);
   consumers_sync_or(0);
   for (int idx = tid; idx < kStrRows * P; idx += kStrConsumers) {
     const int q = idx / kStrRows;
@@ -1265,9 +1284,10 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     const int row = r0 + rl;
     const int b = q >> 1;
     if (row >= n || b >= km) continue;
-    C s = red[rl * P + q];
+    const C* rq = red + (size_t)q * kStrGroups * kStrRows + rl;
+    C s = rq[0];
 #pragma unroll
-    for (int gg = 1; gg < kStrGroups; gg++) s = cadd(s, red[(gg * kStrRows + rl) * P + q]);
+    for (int gg = 1; gg < kStrGroups; gg++) s = cadd(s, rq[gg * kStrRows]);
     if ((q & 1) == 0) {
       Tout[b * wstride + (long long)f * n + row] = s;
     } else if (two) {
@@ -1275,5 +1295,6 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     }
   }
 }
+
 
 }  // namespace vox

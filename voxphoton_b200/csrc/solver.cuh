@@ -894,8 +894,9 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
       // CGS2 in two reads of the basis
       const dim3 gp(kGsBlocks, km);
       const size_t sm = gs_pass_smem<R>(k + 1);
-      k_gs_pass<R, false><<<gp, kRedThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs);
-      k_gs_pass<R, true><<<gp, kRedThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs);
+      const int ns = gs_stages<R>(k + 1);
+      k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns);
+      k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns);
       k_gs_finish<R><<<ge, kRedThreads, 0, st>>>(d, k, w.V, ld, wv,
                                                  w.V + (long long)(k + 1) * ld, n, w.vs);
       *nk += 3 + ((right || left) ? 3 : 0) + 3;
@@ -1557,11 +1558,12 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
   if (restart + 1 <= kGsMaxCols) {
     const dim3 gp(kGsBlocks, km);
     const size_t sm = gs_pass_smem<R>(k + 1);
+    const int ns = gs_stages<R>(k + 1);
     out[6] = timeit([&] {
-      k_gs_pass<R, false><<<gp, kRedThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+      k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs, ns);
     });
     out[7] = timed_clear([&] {
-      k_gs_pass<R, true><<<gp, kRedThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs);
+      k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs, ns);
     });
     clear();
     out[8] = timeit([&] {
