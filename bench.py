@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--inner-tol", type=float, default=0.0,
-                    help="complex64 inner GMRES tolerance (0: aim at the target directly)")
+                    help="complex64 inner GMRES tolerance (0: aim at the target directly, "
+                         "f * tol * ||b|| / ||r|| with the library's f; negative: f = -value)")
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")

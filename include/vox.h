@@ -263,7 +263,9 @@ vox_status vox_pgmres(vox_op_t op, vox_precond_t pc, int side, vox_prec prec, co
  * products, norms and Givens in FP64) inside FP64 iterative refinement:
  * repeat { r = b - A x (FP64); d = GMRES_c64(A, r/|r|, inner_tol); x += |r| d }
  * until ||b - A x|| / ||b|| <= tol.  inner_tol <= 0 aims each inner solve at
- * the remaining target directly (0.3 * tol * ||b|| / ||r||). */
+ * the remaining target directly, f * tol * ||b|| / ||r||, with f = 0.3 for a
+ * left preconditioner (GMRES then sees the preconditioned residual) and 0.9
+ * otherwise; a negative inner_tol sets f = -inner_tol (at most 1). */
 vox_status vox_solve_refined(vox_op_t op, vox_precond_t pc, int side, const double* b_re,
                              const double* b_im, double tol, int restart, int maxit_inner,
                              double inner_tol, int max_refine, double* x_re, double* x_im,

@@ -89,7 +89,7 @@ static vox_status lane_start_inner(vox_lane_s* L, const std::vector<int>& S) {
     vox_lane_s::Member& mb = L->m[b];
     mb.rn = mb.rel * mb.bn;
     k_cast_scale<float><<<nb, 256, 0, st>>>(n, wd.mem(wd.r, b), 1.0 / mb.rn, wf.mem(wf.b, b));
-    const double fac = inner_target_factor(L->pc, L->side);
+    const double fac = inner_target_factor(L->pc, L->side, L->inner_tol);
     mb.itol = auto_tol ? std::min(0.5, fac * L->tol * mb.bn / mb.rn)
                        : std::min(0.5, std::max(L->inner_tol, 0.5 * L->tol * mb.bn / mb.rn));
     VOX_CUDA(cudaMemsetAsync(wf.mem(wf.x, b), 0, n * sizeof(float2), st));

@@ -1168,7 +1168,8 @@ __global__ void k_axpy_d2_from(long long n, const float2* __restrict__ d, double
 // Fraction of the remaining relative target that an automatic inner solve aims
 // at: its residual is the true one with a right preconditioner or none, the
 // preconditioned one with a left preconditioner.
-static double inner_target_factor(const vox_precond_s* pc, int side) {
+static double inner_target_factor(const vox_precond_s* pc, int side, double inner_tol) {
+  if (inner_tol < 0) return std::min(1.0, -inner_tol);  // the caller's factor
   return (pc && side == VOX_PREC_LEFT) ? 0.3 : 0.9;
 }
 
@@ -1197,7 +1198,7 @@ static vox_status refined_run(vox_op_s* op, vox_precond_s* pc, int side, int cou
   // between the preconditioned residual GMRES minimises and the true one),
   // f = 0.9 otherwise (GMRES minimises the true residual of the complex64 system)
   const bool auto_tol = inner_tol <= 0;
-  const double fac = inner_target_factor(pc, side);
+  const double fac = inner_target_factor(pc, side, inner_tol);
   if (max_refine < 1) max_refine = 10;
   VOX_TRY(ensure_work<float>(op, restart));
   if (!op->wd.arena) VOX_TRY(ensure_work<double>(op, 1));
