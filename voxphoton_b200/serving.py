@@ -80,6 +80,7 @@ class Result:
     relres: float
     flag: int
     x: object = None  # the solution, when ServeConfig.keep_x
+    refinements: int = 0  # FP64 refinement steps (mixed-precision solves)
 
     @property
     def latency(self):
@@ -516,7 +517,8 @@ class SweepServer:
                             results.append(Result(req.rid, req.key, req.lam,
                                                   req.arrival if realtime else 0.0, start, done,
                                                   info["iters"], info["relres"], info["flag"],
-                                                  x if self.cfg.keep_x else None))
+                                                  x if self.cfg.keep_x else None,
+                                                  info.get("refinements", 0)))
                             pending[0] -= 1
             except Exception as e:  # surfaced after the threads join
                 errors.append(e)
@@ -657,7 +659,8 @@ class SweepServer:
                             results.append(Result(req.rid, req.key, req.lam,
                                                   req.arrival if realtime else 0.0, start, done,
                                                   info["iters"], info["relres"], info["flag"],
-                                                  x if self.cfg.keep_x else None))
+                                                  x if self.cfg.keep_x else None,
+                                                  info.get("refinements", 0)))
             except Exception as e:  # surfaced after the threads join
                 errors.append(e)
 
@@ -682,4 +685,5 @@ def summarize(results, wall):
             "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "mean_iters": float(np.mean([r.iters for r in results])),
             "max_relres": float(np.max([r.relres for r in results])),
+            "mean_refinements": float(np.mean([r.refinements for r in results])),
             "flags": int(np.sum([r.flag for r in results]))}
