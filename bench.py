@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="vox", choices=["vox", "reference"])
     ap.add_argument("--workload", default="sweep",
-                    help="sweep (default) | microdisk | mor | bragg20 | bragg20-p<N> | strip | bragg10")
+                    help="sweep (default) | microdisk | mor | stages | bragg20 | bragg20-p<N> | "
+                         "strip | bragg10")
     ap.add_argument("--precond", default="level1", choices=["none", "level1"])
     ap.add_argument("--tol", type=float, default=1e-5)
     ap.add_argument("--restart", type=int, default=50)
@@ -81,6 +82,9 @@ def parse():
                     help="tolerance of the model's solves (the script's 1e-4)")
     ap.add_argument("--mor-check", type=int, default=5,
                     help="wavelengths compared against full solves")
+    ap.add_argument("--stage-periods", type=int, default=60,
+                    help="stages workload: grating periods (60 = 1160 x 30 x 11)")
+    ap.add_argument("--stage-prec", default="c64", choices=["c64", "c128"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-clocks", action="store_true",
                     help="do not spawn the nvidia-smi clock sampler (profiler runs)")
@@ -180,12 +184,12 @@ def build_problem(name):
     return p, G, idx, b, t_asm
 
 
-def kernel_bytes(op_info, shape, n, pc_info, k):
-    """Algorithmic bytes per launch of each stage, complex64 (8 B per value)."""
+def kernel_bytes(op_info, shape, n, pc_info, k, c=8):
+    """Algorithmic bytes per launch of each stage for one member, c bytes per
+    complex value (8: complex64, 16: complex128); int32 index maps."""
     L, M, N = shape
     V = L * M * N
     Px, Py, Pz = op_info["Px"], op_info["Py"], op_info["Pz"]
-    c = 8
     T = Px * 3 * N * M * c
     n3 = 3 * M * N
     if op_info.get("octant_fN"):
@@ -641,6 +645,49 @@ def run_sweep(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_stages(args, world, rank, local):
+    """Per-kernel device time of one GMRES iteration (vox_profile_stages) on a
+    batched operator of one grating of the sweep: --stage-periods periods,
+    --sweep-members members, --stage-prec precision, level-1 preconditioner,
+    restart 50, Gram-Schmidt at a basis of 21 vectors.  The small, repeatable
+    case the ncu captures in profiles/ are taken on."""
+    import torch
+    import voxphoton_b200 as vb
+    from voxphoton_b200 import geometry as geo
+    torch.cuda.set_device(local)
+    p = geo.bragg(periods=args.stage_periods, M=30)
+    G = vb.assemble_toeplitz(p.shape, p.ko, p.res, device=local)
+    idx = p.idxS3()
+    op1 = vb.Operator(p.Mop(), p.Gram, idx, G=G, device=local)
+    pc1 = vb.Preconditioner.level1(op1, G, p.e_r)
+    K = args.sweep_members
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=G, device=local, members=K)
+    pc = pc1.share(op)
+    stage = op.profile_stages(pc, prec=args.stage_prec, restart=args.restart, kgs=20,
+                              reps=max(1, args.steps or 10))
+    info, pinfo = op.info(), pc.info()
+    L, M, N = p.shape
+    n3 = 3 * M * N
+    c = 8 if args.stage_prec == "c64" else 16
+    nbytes = {k: v * K for k, v in kernel_bytes(info, p.shape, idx.size, pinfo, 20, c).items()}
+    # the blocks are streamed once for every member of the launch
+    nbytes["pc_solve"] = pinfo["n_blocks"] * n3 * n3 * c + 2 * K * L * n3 * c
+    hbm, src = peaks()
+    if rank == 0:
+        print(json.dumps({"workload": f"stages: grating of {args.stage_periods} periods "
+                                      f"({L}x{M}x{N}), {K} members, {args.stage_prec}",
+                          "stage_ms": stage,
+                          "bytes": nbytes,
+                          "frac_of_hbm": {k: (nbytes[k] / (stage[k] * 1e-3) / 1e9 / hbm)
+                                          for k in nbytes if stage.get(k, 0) > 0},
+                          "peak_gbs": hbm, "peak_source": src, "op": info, "pc": pinfo}),
+              flush=True)
+    pc.close()
+    op.close()
+    pc1.close()
+    op1.close()
+
+
 def run_microdisk(args, world, rank, local):
     """Large resonator served broadband: Si microdisk (radius 5 um) side-coupled
     to a bus waveguide, 560 x 540 x 11 at 20 nm, 41 wavelengths over
@@ -904,7 +951,7 @@ def run_mor(args, world, rank, local):
 
 def main():
     args = parse()
-    if args.steps is None and args.workload not in ("sweep", "microdisk", "mor"):
+    if args.steps is None and args.workload not in ("sweep", "microdisk", "mor", "stages"):
         args.steps = 10
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -917,6 +964,9 @@ def main():
         return
     if args.workload == "mor":
         run_mor(args, world, rank, local)
+        return
+    if args.workload == "stages":
+        run_stages(args, world, rank, local)
         return
     if args.workload == "sweep":
         if world > 1:
