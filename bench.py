@@ -452,13 +452,13 @@ def run_sweep(args, world, rank, local):
     setup_s = time.time() - t
     _progress("setup")
     # admission by HBM footprint: one device-memory pool for the lanes of
-    # every length, less room for the device-resident right-hand sides and
-    # solutions; lanes are admitted (and retired) by their measured bytes as
+    # every length (80 % of what is free after setup, less room for the
+    # device-resident right-hand sides and solutions); lanes are admitted (and retired) by their measured bytes as
     # the queues of the lengths fill, up to --sweep-slots lanes per length
     torch.cuda.synchronize()
     free0, total_mem = torch.cuda.mem_get_info()
     io_bytes = 2 * 16 * len(lams) * sum(f.idx.size for f in fams)
-    budget = int(0.6 * (free0 - io_bytes))
+    budget = int(0.8 * (free0 - io_bytes))
     reqs = sv.poisson_stream(items, rate=args.sweep_rate, seed=args.seed + rank)
     cfg = sv.ServeConfig(tol=args.tol, side=args.sweep_side, batching=args.sweep_batching,
                          inner_tol=args.inner_tol)
