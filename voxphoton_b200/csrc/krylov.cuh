@@ -597,40 +597,42 @@ __global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x
 // (deterministic); the update of w' (pass<true>) runs one thread per row
 // before the dots of the same stage.
 constexpr int kGsMaxCols = 51;
-constexpr int kGsWarps = kRedThreads / 32;  // consumer warps
-constexpr int kGsThreads = kRedThreads + 32;  // + one producer warp
+constexpr int kGsConsumers = 512;
+constexpr int kGsWarps = kGsConsumers / 32;  // consumer warps
+constexpr int kGsThreads = kGsConsumers + 32;  // + one producer warp
 constexpr int kGsColsPerWarp = (kGsMaxCols + kGsWarps - 1) / kGsWarps;
-constexpr int kGsBlocks = 296;  // two CTAs per SM on 148 SMs
+constexpr int kGsBlocks = 148;  // one CTA per SM
 constexpr int kGsMaxStages = 6;
-constexpr size_t kGsSmemBudget = 100 * 1024;
+constexpr size_t kGsSmemBudget = 220 * 1024;
 
+// Rows per chunk: each column segment of a chunk is one bulk copy, 4 KB when
+// two stages of such chunks fit the budget, else 2 KB (long bases).
 template <typename R>
-constexpr int gs_rows() {
-  return sizeof(R) == 4 ? 128 : 64;
+inline int gs_rows(int nj) {
+  const int r4 = 4096 / (int)sizeof(Cx<R>);
+  return 2ull * (nj + 1) * r4 * sizeof(Cx<R>) <= kGsSmemBudget ? r4 : r4 / 2;
 }
-// ring stages of [nj + 1][rows] (basis columns and w) within the budget
 template <typename R>
 inline int gs_stages(int nj) {
-  const size_t st = ((size_t)nj + 1) * gs_rows<R>() * sizeof(Cx<R>);
+  const size_t st = ((size_t)nj + 1) * gs_rows<R>(nj) * sizeof(Cx<R>);
   const size_t s = kGsSmemBudget / st;
   return (int)(s < 2 ? 2 : (s > kGsMaxStages ? kGsMaxStages : s));
 }
 template <typename R>
 inline size_t gs_pass_smem(int nj) {
-  return (size_t)gs_stages<R>(nj) * ((size_t)nj + 1) * gs_rows<R>() * sizeof(Cx<R>);
+  return (size_t)gs_stages<R>(nj) * ((size_t)nj + 1) * gs_rows<R>(nj) * sizeof(Cx<R>);
 }
 
 __device__ __forceinline__ void consumer_bar() {
-  asm volatile("bar.sync 1, %0;" ::"n"(kRedThreads) : "memory");
+  asm volatile("bar.sync 1, %0;" ::"n"(kGsConsumers) : "memory");
 }
 
 template <typename R, bool kUpdate>
-__global__ void __launch_bounds__(kGsThreads, 2) k_gs_pass(GmresDev* st, int k,
+__global__ void __launch_bounds__(kGsThreads, 1) k_gs_pass(GmresDev* st, int k,
                                                            const Cx<R>* __restrict__ V,
                                                            long long ldv, Cx<R>* w, long long n,
-                                                           long long vs, int stages) {
+                                                           long long vs, int stages, int RW) {
   using C = Cx<R>;
-  constexpr int RW = gs_rows<R>();
   __shared__ double2 sh[32];
   __shared__ C hs[kGsMaxCols];
   __shared__ __align__(8) uint64_t full[kGsMaxStages];
@@ -720,7 +722,7 @@ __global__ void __launch_bounds__(kGsThreads, 2) k_gs_pass(GmresDev* st, int k,
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
-  if (named_bar_or<kRedThreads>(1, failed)) return;  // nothing of this CTA is reduced
+  if (named_bar_or<kGsConsumers>(1, failed)) return;  // nothing of this CTA is reduced
 #pragma unroll
   for (int q = 0; q < kGsColsPerWarp; q++) {
     const int j = warp + q * kGsWarps;

@@ -1102,53 +1102,40 @@ __global__ void __launch_bounds__(kInvThreads) k_pc_inv_apply(
 
 
 // ------------------------------------------------ apply: streamed inverse blocks
-// The same product as k_pc_inv_apply (T2_f = inv(B_f) T_f for P columns, the
-// modes f and L-f of every member), with the block's rows streamed through a
-// shared-memory ring by bulk asynchronous copies: one producer warp issues, per
-// stage, KC column segments of the CTA's 128 rows (one copy each, no
-// registers held by the loads), and 512 consumer threads (64 row pairs x 8
-// column groups, enough warps to keep the FMA pipes issuing) multiply out of
-// shared memory.  Up to kStrMaxStages stages are in flight per CTA, which is
-// what keeps HBM busy.  Each group sums its columns in increasing order and the
-// eight group sums are added in a fixed order, so a column's result does not
-// depend on P or on the other members.  grid (ld / 128 rounded up, blocks),
-// kStrThreads threads, shared memory str_smem().
-constexpr int kStrRows = 128;
-constexpr int kStrGroups = 8;
-constexpr int kStrConsumers = (kStrRows / 2) * kStrGroups;  // 512
-constexpr int kStrThreads = kStrConsumers + 32;             // + one producer warp
+// The product T2_f = inv(B_f) T_f for P columns (the modes f and L-f of every
+// member) with one CTA per stored block: the block (column-major, ld rows) is
+// streamed through a ring of shared-memory stages, each stage KC whole
+// consecutive columns, which are contiguous in memory and so arrive as ONE bulk
+// asynchronous copy of KC * ld values (16 KB in either precision); a producer
+// warp issues the copies and 512 consumer threads, two rows each, multiply out
+// of shared memory.  Up to kStrMaxStages stages are in flight per CTA, which is
+// what keeps HBM busy; the producer starts while the consumers gather the
+// right-hand sides.  Each row's sums run over the columns in increasing order,
+// so a column's result does not depend on P or on the other members (batched
+// and single solves agree bit for bit).  grid (blocks), kStrThreads threads,
+// shared memory str_smem().
+constexpr int kStrConsumers = 512;
+constexpr int kStrThreads = kStrConsumers + 32;  // + one producer warp
 constexpr int kStrMaxStages = 8;
 
-// columns per stage: a 16 KB stage of 128 rows in either precision
+// whole columns per stage: 16 KB at ld = 1024 in either precision
 template <typename R>
 constexpr int str_kc() {
-  return sizeof(R) == 4 ? 16 : 8;
+  return sizeof(R) == 4 ? 2 : 1;
 }
 template <typename R>
-constexpr size_t str_stage_bytes() {
-  return (size_t)str_kc<R>() * kStrRows * sizeof(Cx<R>);
+inline size_t str_stage_bytes(int ld) {
+  return (size_t)str_kc<R>() * ld * sizeof(Cx<R>);
 }
-// right-hand sides [ld][P] + ring [stages][KC][128]; the final partial sums
-// (4 groups x 128 rows x P) reuse the same space
+// right-hand sides [ld][P] + ring [stages][KC][ld]
 template <typename R>
 inline size_t str_smem(int ld, int P, int stages) {
-  const size_t xr = (size_t)ld * P * sizeof(Cx<R>) + (size_t)stages * str_stage_bytes<R>();
-  const size_t red = (size_t)kStrGroups * kStrRows * P * sizeof(Cx<R>);
-  return xr > red ? xr : red;
+  return (size_t)ld * P * sizeof(Cx<R>) + (size_t)stages * str_stage_bytes<R>(ld);
 }
 
 // named barrier of the consumer threads (the producer warp may have left)
 __device__ __forceinline__ int consumers_sync_or(int pred) {
-  int r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.s32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, %2, p;\n\t"
-      "selp.s32 %0, 1, 0, q;\n\t}"
-      : "=r"(r)
-      : "r"(pred), "n"(kStrConsumers)
-      : "memory");
-  return r;
+  return named_bar_or<kStrConsumers>(1, pred);
 }
 
 template <typename R, int P>
@@ -1169,16 +1156,14 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   __shared__ __align__(8) uint64_t full[kStrMaxStages];
   __shared__ __align__(8) uint64_t empty[kStrMaxStages];
   C* X = reinterpret_cast<C*>(smem_raw);  // X[k * P + col], k < ld
-  C* ring = X + (size_t)ld * P;          // [stages][KC][kStrRows]
+  C* ring = X + (size_t)ld * P;          // [stages][KC][ld]
   const int n = g.n3;
   const int MN = n / 3;
-  const int f = blockIdx.y;
+  const int f = blockIdx.x;
   const int i2 = g.L - f;
   const bool two = paired && f != 0 && i2 != f;
   const long long wstride = pc_work_elems(g);
-  const int r0 = blockIdx.x * kStrRows;
-  const int nrows = min(kStrRows, ld - r0);
-  const int nkb = ld / KC;
+  const int nkb = (n + KC - 1) / KC;  // stages of columns < n (padding columns skipped)
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < stages; s++) {
@@ -1189,19 +1174,18 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   }
   __syncthreads();
   if (tid >= kStrConsumers) {
-    // producer warp: lane j copies column j of each stage; it starts at once,
-    // while the consumers gather the right-hand sides
+    // producer warp: stage kb = columns kb*KC .. kb*KC+KC-1, one contiguous copy
     const int lane = tid & 31;
-    const C* Bf = Binv + (long long)f * ld * ld + r0;
-    const unsigned bytes = (unsigned)(nrows * sizeof(C));
+    const C* Bf = Binv + (long long)f * ld * ld;
+    const unsigned bytes = (unsigned)(KC * ld * sizeof(C));
     for (int kb = 0; kb < nkb; kb++) {
       const int s = kb % stages;
       if (kb >= stages && !mbar_wait(&empty[s], ((kb / stages) - 1) & 1)) return;
-      if (lane == 0) mbar_arrive_expect_tx(&full[s], bytes * KC);
+      if (lane == 0) {
+        mbar_arrive_expect_tx(&full[s], bytes);
+        bulk_g2s(ring + (size_t)s * KC * ld, Bf + (long long)kb * KC * ld, bytes, &full[s]);
+      }
       __syncwarp();
-      if (lane < KC)
-        bulk_g2s(ring + ((size_t)s * KC + lane) * kStrRows, Bf + (long long)(kb * KC + lane) * ld,
-                 bytes, &full[s]);
     }
     return;
   }
@@ -1233,27 +1217,24 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     }
   }
   consumers_sync_or(0);
-  const int rp = tid % (kStrRows / 2);  // row pair within the chunk
-  const int kg = tid / (kStrRows / 2);  // column group
-  const bool active = 2 * rp < nrows;
+  const int r = 2 * tid;  // this thread's rows r, r + 1
+  const bool active = r < n;
   C a0[P], a1[P];
 #pragma unroll
   for (int q = 0; q < P; q++) a0[q] = a1[q] = czero<C>();
   int failed = 0;
   for (int kb = 0; kb < nkb; kb++) {
     const int s = kb % stages;
-    if (!mbar_wait(&full[s], (kb / stages) & 1)) {
-      failed = 1;
-      break;
-    }
-    if (active) {
-      const C* st = ring + (size_t)s * KC * kStrRows + 2 * rp;
+    const bool ok = mbar_wait(&full[s], (kb / stages) & 1);
+    failed |= !ok;
+    if (ok && active) {
+      const C* st = ring + (size_t)s * KC * ld + r;
 #pragma unroll
-      for (int c = kg; c < KC; c += kStrGroups) {
+      for (int c = 0; c < KC; c++) {
         const int k = kb * KC + c;
         if (k < n) {
           C b0, b1;
-          ld_pair(st + c * kStrRows, b0, b1);
+          ld_pair(st + (size_t)c * ld, b0, b1);
           const C* xk = X + P * k;
 #pragma unroll
           for (int q = 0; q < P; q += 2) {
@@ -1270,31 +1251,22 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     __syncwarp();
     if ((tid & 31) == 0) mbar_arrive(&empty[s]);
   }
-  // every consumer past its last stage (or one gave up): the ring and X are free
-  if (consumers_sync_or(failed)) return;
-  // partial sums red[(q * groups + kg) * kStrRows + row]: rows of a warp adjacent
-  C* red = X;
+  if (consumers_sync_or(failed) || !active) return;
 #pragma unroll
-  for (int q = 0; q < P; q++)
-    st_pair(red + ((size_t)q * kStrGroups + kg) * kStrRows + 2 * rp, a0[q], a1[q]);
-  consumers_sync_or(0);
-  for (int idx = tid; idx < kStrRows * P; idx += kStrConsumers) {
-    const int q = idx / kStrRows;
-    const int rl = idx - q * kStrRows;
-    const int row = r0 + rl;
+  for (int q = 0; q < P; q++) {
     const int b = q >> 1;
-    if (row >= n || b >= km) continue;
-    const C* rq = red + (size_t)q * kStrGroups * kStrRows + rl;
-    C s = rq[0];
-#pragma unroll
-    for (int gg = 1; gg < kStrGroups; gg++) s = cadd(s, rq[gg * kStrRows]);
-    if ((q & 1) == 0) {
-      Tout[b * wstride + (long long)f * n + row] = s;
-    } else if (two) {
-      Tout[b * wstride + (long long)i2 * n + row] = (row < MN) ? cscale(s, (R)-1) : s;
+    if (b >= km) continue;
+    for (int h = 0; h < 2; h++) {
+      const int row = r + h;
+      if (row >= n) continue;
+      const C v = h ? a1[q] : a0[q];
+      if ((q & 1) == 0) {
+        Tout[b * wstride + (long long)f * n + row] = v;
+      } else if (two) {
+        Tout[b * wstride + (long long)i2 * n + row] = (row < MN) ? cscale(v, (R)-1) : v;
+      }
     }
   }
 }
-
 
 }  // namespace vox

@@ -84,7 +84,7 @@ constexpr int apply_members() {
 template <typename R>
 static int str_stages(int ld, int P) {
   const long long room = (long long)kSmemCap - (long long)ld * P * sizeof(Cx<R>);
-  return (int)std::min<long long>(kStrMaxStages, room / (long long)str_stage_bytes<R>());
+  return (int)std::min<long long>(kStrMaxStages, room / (long long)str_stage_bytes<R>(ld));
 }
 
 template <typename R, int P>
@@ -92,7 +92,7 @@ static void launch_inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaSt
                              const int* skip, int fs, int km) {
   const PcGeom& g = p->g;
   const int stages = str_stages<R>(p->ld, P);
-  const dim3 grid((p->ld + kStrRows - 1) / kStrRows, p->Lf);
+  const dim3 grid(p->Lf);
   k_pc_inv_stream<R, P><<<grid, kStrThreads, str_smem<R>(p->ld, P, stages), st>>>(
       g, p->paired, p->ld, stages, pc_A<R>(p), T, T2, skip, fs, km);
 }
@@ -106,7 +106,8 @@ static vox_status inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStr
   for (int m0 = 0; m0 < km; m0 += apply_members<R>()) {
     const int kg = std::min(apply_members<R>(), km - m0);
     const int P = lu_cols(kg);
-    if (str_stages<R>(p->ld, P) < 2 || str_smem<R>(p->ld, P, 2) > (size_t)kSmemCap) {
+    if (p->ld > 2 * kStrConsumers || str_stages<R>(p->ld, P) < 2 ||
+        str_smem<R>(p->ld, P, 2) > (size_t)kSmemCap) {
       set_error("preconditioner: blocks of " + std::to_string(p->ld) +
                 " rows leave no room for the streaming ring at " + std::to_string(kg) +
                 " members in this precision");
@@ -374,7 +375,8 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p, int L, int M, int N,
   // (two 16 KiB stages + 32 B * ld) under the cap
   if (lu && ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
              lu_stream2_smem<double>(lu_npad(g.n3), kInvBuildCols) > (size_t)kSmemCap ||
-             str_smem<double>((g.n3 + 31) / 32 * 32, 2, 2) > (size_t)kSmemCap)) {
+             str_smem<double>((g.n3 + 31) / 32 * 32, 2, 2) > (size_t)kSmemCap ||
+             (g.n3 + 31) / 32 * 32 > 2 * kStrConsumers)) {
     set_error("preconditioner: 3*M*N too large for the batched LU panel");
     return VOX_ERR_UNSUPPORTED;
   }
@@ -894,9 +896,9 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
       // CGS2 in two reads of the basis
       const dim3 gp(kGsBlocks, km);
       const size_t sm = gs_pass_smem<R>(k + 1);
-      const int ns = gs_stages<R>(k + 1);
-      k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns);
-      k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns);
+      const int ns = gs_stages<R>(k + 1), rw = gs_rows<R>(k + 1);
+      k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns, rw);
+      k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns, rw);
       k_gs_finish<R><<<ge, kRedThreads, 0, st>>>(d, k, w.V, ld, wv,
                                                  w.V + (long long)(k + 1) * ld, n, w.vs);
       *nk += 3 + ((right || left) ? 3 : 0) + 3;
@@ -1559,12 +1561,12 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
   if (restart + 1 <= kGsMaxCols) {
     const dim3 gp(kGsBlocks, km);
     const size_t sm = gs_pass_smem<R>(k + 1);
-    const int ns = gs_stages<R>(k + 1);
+    const int ns = gs_stages<R>(k + 1), rw = gs_rows<R>(k + 1);
     out[6] = timeit([&] {
-      k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs, ns);
+      k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs, ns, rw);
     });
     out[7] = timed_clear([&] {
-      k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs, ns);
+      k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(w.st, k, w.V, ld, w.w, n, w.vs, ns, rw);
     });
     clear();
     out[8] = timeit([&] {
