@@ -531,13 +531,13 @@ def run_sweep(args, world, rank, local):
     mvb = kernel_bytes(op_m.info(), fmid.p.shape, fmid.idx.size, info_m, 20)
     mv_bytes = K * (mvb["mv_xfwd"] + mvb["mv_plane"] + mvb["mv_xinv"])
     mv_ms = stage["mv_xfwd"] + stage["mv_plane"] + stage["mv_xinv"]
-    roof = {"bound": "hbm", "kernel": f"pc_solve (k_pc_inv_apply, {K} members, "
+    roof = {"bound": "hbm", "kernel": f"pc_solve (k_pc_inv_stream, {K} members, "
                                       f"{L}x{M}x{N})",
             "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
             "traffic": measured_traffic("pc_solve", alg), "peak_source": src,
             "bytes_per_launch": alg, "ms_per_launch": stage["pc_solve"],
             "stage_ms": stage,
-            "matvec": {"kernels": "k_xfwd + k_plane + k_xinv", "members": K,
+            "matvec": {"kernels": "k_xfwd + k_plane64 + k_xinv", "members": K,
                        "bytes_per_launch": mv_bytes, "ms": mv_ms,
                        "achieved": mv_bytes / (mv_ms * 1e-3) / 1e9,
                        "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm}}

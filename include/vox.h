@@ -111,6 +111,12 @@ int vox_abi_version(void);
  * reference has no counterpart (MATLAB blocks on gpuArray results). */
 vox_status vox_set_wait_timeout(double seconds);
 double vox_get_wait_timeout(void);
+/* Device bytes the library holds on `device` (operators, preconditioners,
+ * lanes and their arenas), excluding the CUDA context, loaded modules and other
+ * libraries' pools: the difference across creating a handle is what that
+ * handle holds.  A serving loop admits lanes against an HBM budget with it.
+ * The reference has no counterpart (MATLAB's gpuArray memory is implicit). */
+vox_status vox_mem_in_use(int device, long long* bytes);
 
 vox_status vox_op_create(const vox_op_desc* desc, vox_op_t* out);
 /* An operator with `members` (1..8) independent copies of fN and of all solve

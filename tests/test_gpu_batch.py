@@ -148,3 +148,50 @@ def test_lane_refills_members_and_matches_solo_solves(family):
     lane.close()
     pcb.close()
     op.close()
+
+
+@pytest.fixture(scope="module")
+def wide():
+    # the sweep's cross-section (30 x 11 cells at 20 nm): level-1 blocks of 990
+    # rows (leading dimension 992), where the streamed apply's right-hand sides
+    # and ring fill the shared-memory budget at every member count
+    p = geo.bragg(periods=2, M=30)
+    assert 3 * p.shape[1] * p.shape[2] == 990
+    idx = p.idxS3()
+    Gs = [vb.assemble_toeplitz(p.shape, p.with_wavelength(l).ko, p.res) for l in NODES]
+    nodes = [vb.Operator(p.Mop(), p.Gram, idx, G=G) for G in Gs]
+    pc = vb.Preconditioner.level1(nodes[1], Gs[1], p.e_r)
+    assert pc.info()["ld"] == 992
+    rhs = sv._RhsBuilder(p, idx)
+    yield p, idx, Gs, nodes, pc, rhs
+    pc.close()
+    for op in nodes:
+        op.close()
+
+
+@pytest.mark.parametrize("members", [2, 4, 5])
+def test_batch_equals_solo_at_the_sweep_cross_section(wide, members):
+    # 2 and 4 members: one apply launch of 4 and 8 columns; 5: a group of 4
+    # and a group of 1
+    p, idx, Gs, nodes, pc, rhs = wide
+    lams = np.linspace(1510e-9, 1590e-9, members)
+    bs = [rhs(geo.C0 / l * geo.N_EXT) for l in lams]
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=Gs[1], members=members)
+    pcb = pc.share(op)
+    for m, l in enumerate(lams):
+        op.interp(nodes, sv.lagrange_weights(l, NODES), member=m)
+    out = vb.solve_refined_batch(op, bs, tol=1e-5, restart=50, maxit_inner=40, inner_tol=0.0,
+                                 R1=pcb)
+    for (x, info), l, b in zip(out, lams, bs):
+        so = vb.Operator(p.Mop(), p.Gram, idx, G=Gs[1])
+        pcs = pc.share(so)
+        so.interp(nodes, sv.lagrange_weights(l, NODES))
+        xs, is_ = vb.solve_refined(so, b, tol=1e-5, restart=50, maxit_inner=40, inner_tol=0.0,
+                                   R1=pcs)
+        pcs.close()
+        so.close()
+        assert info["flag"] == 0 and info["relres"] <= 1e-5
+        assert info["iters"] == is_["iters"]
+        assert np.array_equal(x, xs)
+    pcb.close()
+    op.close()

@@ -158,3 +158,19 @@ def test_wait_limit_returns_timeout_and_the_operator_recovers(case):
     x, flag, relres, it, resvec = vb.pgmres(op, b, 50, 1e-8, 10)
     assert flag == 0 and relres <= 1e-8
     op.close()
+
+
+def test_memory_count_follows_the_handles(case):
+    p, G, Einc = case
+    idx = p.idxS3()
+    m0 = _lib.mem_in_use(0)
+    op = vb.Operator(p.Mop(), p.Gram, idx, G=G)
+    m1 = _lib.mem_in_use(0)
+    pc = vb.Preconditioner.level1(op, G, p.e_r)
+    m2 = _lib.mem_in_use(0)
+    # at least the operator's two complex128 vectors and the blocks' c128 copy
+    assert m1 - m0 >= 2 * 16 * idx.size
+    assert m2 - m1 >= 16 * pc.info()["n_blocks"] * pc.info()["ld"] ** 2
+    pc.close()
+    op.close()
+    assert _lib.mem_in_use(0) == m0

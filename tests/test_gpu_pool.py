@@ -3,7 +3,9 @@ of every device length share one device-memory budget, a length whose
 arrived requests outnumber its free member slots gets a new lane when the
 lane's measured footprint fits, and an idle lane of a length with nothing
 waiting is retired to make room.  Here the stream switches from one length to
-the other part-way, under a budget of three lanes: lanes move between the
+the other part-way, under a budget that holds two lanes of the shorter length
+beside one of the longer but not a second lane of the longer beside them
+(footprints as the library counts its own device bytes): lanes move between the
 lengths, the budget is never exceeded, and every result is bit-identical to
 the same request solved alone."""
 import numpy as np
@@ -25,7 +27,10 @@ def test_lanes_follow_the_mix_and_results_match_alone():
     cfg = sv.ServeConfig(tol=1e-5, keep_x=True)
     srv = sv.SweepServer(fams, cfg, pool_bytes=1 << 60)
     srv.prepare_pool(1)  # one measured lane per length
-    srv.pool_bytes = 3 * max(srv.lane_bytes.values())
+    lb = srv.lane_bytes
+    # room for two lanes of length 2 beside one of length 4, not for a second
+    # lane of length 4 beside them
+    srv.pool_bytes = 2 * lb[2] + lb[4] + lb[4] // 2
     lams = np.linspace(band[0], band[1], 8)
     reqs = ([sv.Request(i, 2, float(l), 0.0) for i, l in enumerate(lams)] +
             [sv.Request(100 + i, 4, float(l), 0.4) for i, l in enumerate(lams)])

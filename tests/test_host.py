@@ -116,6 +116,18 @@ def test_wait_limit_setter_validates_and_defaults():
     assert lib.vox_get_wait_timeout() > 0
 
 
+def test_memory_count_checks_its_arguments():
+    """vox_mem_in_use (no device work): NULL and out-of-range devices are
+    refused; with nothing created the library holds no device bytes."""
+    import ctypes
+    lib = _lib.lib()
+    b = ctypes.c_longlong(-1)
+    assert lib.vox_mem_in_use(-1, ctypes.byref(b)) == _lib.VOX_ERR_BAD_ARG
+    assert lib.vox_mem_in_use(64, ctypes.byref(b)) == _lib.VOX_ERR_BAD_ARG
+    assert lib.vox_mem_in_use(0, None) == _lib.VOX_ERR_BAD_ARG
+    assert lib.vox_mem_in_use(0, ctypes.byref(b)) == _lib.VOX_OK and b.value >= 0
+
+
 def test_jvie_solve_argument_checks_need_no_device():
     """vox_jvie_solve refuses what it does not implement (form 1, solvers other
     than GMRES) and malformed descriptors before any device call."""

@@ -93,6 +93,7 @@ SIGNATURES = [
     ("vox_abi_version", ctypes.c_int, []),
     ("vox_set_wait_timeout", ctypes.c_int, [ctypes.c_double]),
     ("vox_get_wait_timeout", ctypes.c_double, []),
+    ("vox_mem_in_use", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
     ("vox_jvie_solve", ctypes.c_int, [ctypes.POINTER(JvieDesc), _dp, _dp,
                                       ctypes.POINTER(GmresInfo)]),
     ("vox_op_create", ctypes.c_int, [ctypes.POINTER(OpDesc), ctypes.POINTER(ctypes.c_void_p)]),
@@ -225,6 +226,13 @@ def check(status):
     if status != VOX_OK:
         msg = lib().vox_last_error()
         raise VoxError(status, msg.decode() if msg else "")
+
+
+def mem_in_use(device=0):
+    """Device bytes libvox holds on `device` (vox_mem_in_use)."""
+    b = ctypes.c_longlong(0)
+    check(lib().vox_mem_in_use(int(device), ctypes.byref(b)))
+    return int(b.value)
 
 
 def dptr(a):

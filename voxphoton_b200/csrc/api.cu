@@ -101,6 +101,28 @@ static std::vector<double2> twiddles(int n) {
   return w;
 }
 
+// Device bytes held by the library, per device: every device allocation goes
+// through dalloc and every release through dfree, so a caller can measure what
+// an object (an operator, a lane) holds apart from the CUDA context, the loaded
+// modules and other libraries' pools (vox_mem_in_use).
+constexpr int kMemDevices = 64;
+static std::mutex g_mem_mu;
+static std::map<void*, std::pair<int, size_t>> g_mem_blocks;
+static long long g_mem_bytes[kMemDevices];
+
+static cudaError_t dfree(void* p) {
+  if (!p) return cudaSuccess;
+  {
+    std::lock_guard<std::mutex> lk(g_mem_mu);
+    auto it = g_mem_blocks.find(p);
+    if (it != g_mem_blocks.end()) {
+      g_mem_bytes[it->second.first] -= (long long)it->second.second;
+      g_mem_blocks.erase(it);
+    }
+  }
+  return cudaFree(p);
+}
+
 template <typename T>
 static vox_status dalloc(T** p, size_t count) {
   *p = nullptr;
@@ -112,6 +134,12 @@ static vox_status dalloc(T** p, size_t count) {
               " bytes failed: " + cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? VOX_ERR_OOM : VOX_ERR_CUDA;
   }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= kMemDevices) dev = 0;
+  std::lock_guard<std::mutex> lk(g_mem_mu);
+  g_mem_blocks[(void*)*p] = {dev, count * sizeof(T)};
+  g_mem_bytes[dev] += (long long)(count * sizeof(T));
   return VOX_OK;
 }
 
@@ -245,8 +273,8 @@ struct GmresWork {
   void release() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     graphs.clear();
-    cudaFree(arena);
-    cudaFree(st);
+    dfree(arena);
+    dfree(st);
     if (hst) cudaFreeHost(hst);
     if (hflag) cudaFreeHost(hflag);
     if (hscal) cudaFreeHost(hscal);
@@ -519,7 +547,7 @@ static vox_status fft_axis_d(double2* data, int d0, int d1, int d2, long long s0
   k_fft_axis<double><<<grid, 256, smem, st>>>(a, p, dtw, sign, data);
   VOX_CUDA(cudaGetLastError());
   VOX_TRY(wait_stream(st));
-  cudaFree(dtw);
+  dfree(dtw);
   return VOX_OK;
 }
 
@@ -566,7 +594,7 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
   VOX_CUDA(cudaMemcpyAsync(tmp, Mc.data(), g.V * sizeof(double2), cudaMemcpyHostToDevice, st));
   k_to_prec<R><<<nblk(g.V), 256, 0, st>>>(g.V, tmp, 1.0, b.Mc);
   VOX_TRY(wait_stream(st));
-  cudaFree(tmp);
+  dfree(tmp);
   auto up_tw = [&](int n, Cx<R>** dst) -> vox_status {
     std::vector<double2> w = twiddles(n);
     std::vector<Cx<R>> wc(n);
@@ -589,15 +617,15 @@ static vox_status upload_precision(vox_op_s* op, const double2* fN_packed_src /*
 
 template <typename R>
 static void free_bufs(OpBuffers<R>& b) {
-  cudaFree(b.fN);
-  cudaFree(b.Mr);
-  cudaFree(b.Mc);
-  cudaFree(b.twX);
-  cudaFree(b.twY);
-  cudaFree(b.twZ);
-  cudaFree(b.T1);
-  cudaFree(b.T2);
-  cudaFree(b.TY);
+  dfree(b.fN);
+  dfree(b.Mr);
+  dfree(b.Mc);
+  dfree(b.twX);
+  dfree(b.twY);
+  dfree(b.twZ);
+  dfree(b.T1);
+  dfree(b.T2);
+  dfree(b.TY);
   b = OpBuffers<R>();
 }
 
@@ -620,13 +648,13 @@ static void destroy_op(vox_op_s* op) {
   op->wf.release();
   free_bufs(op->d);
   free_bufs(op->f);
-  cudaFree(op->vmap);
+  dfree(op->vmap);
   if (op->h_in) cudaFreeHost(op->h_in);
   if (op->h_out) cudaFreeHost(op->h_out);
-  cudaFree(op->d_in);
-  cudaFree(op->d_out);
-  cudaFree(op->f_in);
-  cudaFree(op->f_out);
+  dfree(op->d_in);
+  dfree(op->d_out);
+  dfree(op->f_in);
+  dfree(op->f_out);
   if (op->own_stream) cudaStreamDestroy(op->own_stream);
   delete op;
 }
@@ -650,6 +678,16 @@ vox_status vox_set_wait_timeout(double seconds) {
 }
 
 double vox_get_wait_timeout(void) { return vox::wait_limit_s(); }
+
+vox_status vox_mem_in_use(int device, long long* bytes) {
+  if (!bytes || device < 0 || device >= vox::kMemDevices) {
+    vox::set_error("vox_mem_in_use: NULL bytes or device out of range");
+    return VOX_ERR_BAD_ARG;
+  }
+  std::lock_guard<std::mutex> lk(vox::g_mem_mu);
+  *bytes = vox::g_mem_bytes[device];
+  return VOX_OK;
+}
 
 static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out);
 
@@ -773,7 +811,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
   const long long P = (long long)g.Px * g.Py * g.Pz;
   double2* emb;
   VOX_TRY(dalloc(&emb, 6 * P));
-  std::unique_ptr<double2, decltype(&cudaFree)> emb_guard(emb, cudaFree);
+  std::unique_ptr<double2, decltype(&dfree)> emb_guard(emb, dfree);
   if (desc->G_re) {
     std::vector<double2> G(6 * V);
     for (long long i = 0; i < 6 * V; i++)
@@ -785,7 +823,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
     k_embed_from_toeplitz<<<nblk(6 * P), 256, 0, st>>>(g, dG, emb);
     VOX_CUDA(cudaGetLastError());
     VOX_TRY(wait_stream(st));
-    cudaFree(dG);
+    dfree(dG);
   } else {
     const int L2 = 2 * L, M2 = 2 * M, N2 = 2 * N;
     const long long Q = (long long)L2 * M2 * N2;
@@ -794,7 +832,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
       F[i] = make_double2(desc->fN_re[i], desc->fN_im ? desc->fN_im[i] : 0.0);
     double2* dF;
     VOX_TRY(dalloc(&dF, 6 * Q));
-    std::unique_ptr<double2, decltype(&cudaFree)> dF_guard(dF, cudaFree);
+    std::unique_ptr<double2, decltype(&dfree)> dF_guard(dF, dfree);
     VOX_CUDA(cudaMemcpyAsync(dF, F.data(), 6 * Q * sizeof(double2), cudaMemcpyHostToDevice,
                              st));
     // inverse 3-D FFT (unscaled) of each component: x stride 1, y 2L, z 4LM
@@ -812,7 +850,7 @@ static vox_status create_op(const vox_op_desc* desc, int K, vox_op_t* out) {
   {
     unsigned* dd;
     VOX_TRY(dalloc(&dd, 2));
-    std::unique_ptr<unsigned, decltype(&cudaFree)> gd(dd, cudaFree);
+    std::unique_ptr<unsigned, decltype(&dfree)> gd(dd, dfree);
     VOX_CUDA(cudaMemsetAsync(dd, 0, 2 * sizeof(unsigned), st));
     k_sym_defect<<<nblk(6 * P), 256, 0, st>>>(g, emb, dd);
     unsigned hv[2];
@@ -1062,9 +1100,9 @@ vox_status vox_assemble_toeplitz_device(int L, int M, int N, double ko, double d
     double2* Ipair = nullptr;
     double2* G = nullptr;
     ~Cleanup() {
-      cudaFree(rules);
-      cudaFree(Ipair);
-      cudaFree(G);
+      dfree(rules);
+      dfree(Ipair);
+      dfree(G);
       cudaStreamDestroy(st);
     }
   } c{st};

@@ -19,6 +19,8 @@
 // plain per-mode GEMV instead.
 #pragma once
 
+#include <type_traits>
+
 #include "bulk.cuh"
 #include "fft.cuh"
 #include "krylov.cuh"
@@ -992,145 +994,54 @@ __global__ void __launch_bounds__(32 * kRoundTiles) k_lu_inv_cols(
   }
 }
 
-// ------------------------------------------- apply: per-mode inverse blocks
-// T2_f = inv(B_f) T_f for every mode, with P right-hand-side columns per mode:
-// for each of km members, mode f and (paired) mode L-f through
-// inv(B_{L-f}) = D inv(B_f) D, so every block is read from HBM once for all
-// members and both modes.  Blocks are column-major with leading dimension ld
-// (a multiple of 32, zero padded); block f of Binv serves mode f (and L-f).
-// One CTA per (128-row chunk, block): 64 row pairs x 4 column groups; the
-// group g sums columns k = g, g+4, ... and the four partial sums are added in
-// that fixed order, so each column's result does not depend on P or on the
-// other members.  grid (ld / 128 rounded up, nblocks); shared memory
-// max(n3, 512) * P complex values.
-constexpr int kInvRows = 128;
-constexpr int kInvKG = 4;
-constexpr int kInvThreads = (kInvRows / 2) * kInvKG;
-
-template <typename R>
-constexpr size_t inv_apply_smem(int n3, int P) {
-  return (size_t)(n3 > kInvKG * kInvRows ? n3 : kInvKG * kInvRows) * P * sizeof(Cx<R>);
-}
-
-template <typename R, int P>
-__global__ void __launch_bounds__(kInvThreads) k_pc_inv_apply(
-    PcGeom g, int paired, int ld, const Cx<R>* __restrict__ Binv, const Cx<R>* __restrict__ Tin,
-    Cx<R>* __restrict__ Tout, const int* skip, int fs, int km) {
-  using C = Cx<R>;
-  constexpr int KS = P / 2;
-  static_assert(P % 2 == 0, "columns come in mode pairs");
-  if (skip) {
-    bool all = true;
-    for (int b = 0; b < km; b++) all = all && skip[(long long)b * fs] != 0;
-    if (all) return;
-  }
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  C* X = reinterpret_cast<C*>(smem_raw);  // X[k * P + col]; later the partial sums
-  const int n = g.n3;
-  const int MN = n / 3;
-  const int f = blockIdx.y;
-  const int i2 = g.L - f;
-  const bool two = paired && f != 0 && i2 != f;
-  const long long wstride = pc_work_elems(g);
-  const int tid = threadIdx.x;
-  for (int b = 0; b < KS; b++) {
-    const C* T1 = Tin + b * wstride + (long long)f * n;
-    const C* T2 = Tin + b * wstride + (long long)(two ? i2 : f) * n;
-    for (int k = tid; k < n; k += blockDim.x) {
-      C v1 = czero<C>(), v2 = czero<C>();
-      if (b < km) {
-        v1 = T1[k];
-        if (two) {
-          v2 = T2[k];
-          if (k < MN) v2 = cscale(v2, (R)-1);
-        }
-      }
-      X[P * k + 2 * b] = v1;
-      X[P * k + 2 * b + 1] = v2;
-    }
-  }
-  __syncthreads();
-  const int rp = tid % (kInvRows / 2);  // row pair within the chunk
-  const int kg = tid / (kInvRows / 2);  // column group
-  const int r = blockIdx.x * kInvRows + 2 * rp;
-  C a0[P], a1[P];
-#pragma unroll
-  for (int q = 0; q < P; q++) a0[q] = a1[q] = czero<C>();
-  if (r < ld) {
-    const C* Bf = Binv + (long long)f * ld * ld + r;
-#pragma unroll 4
-    for (int k = kg; k < n; k += kInvKG) {
-      C b0, b1;
-      ld_pair(Bf + (long long)k * ld, b0, b1);
-      const C* xk = X + P * k;
-#pragma unroll
-      for (int q = 0; q < P; q += 2) {
-        C x0, x1;
-        ld_pair(xk + q, x0, x1);
-        cmac(a0[q], b0, x0);
-        cmac(a0[q + 1], b0, x1);
-        cmac(a1[q], b1, x0);
-        cmac(a1[q + 1], b1, x1);
-      }
-    }
-  }
-  __syncthreads();
-  // partial sums: red[(kg * kInvRows + row) * P + col]
-  C* red = X;
-#pragma unroll
-  for (int q = 0; q < P; q++) {
-    red[(kg * kInvRows + 2 * rp) * P + q] = a0[q];
-    red[(kg * kInvRows + 2 * rp + 1) * P + q] = a1[q];
-  }
-  __syncthreads();
-  for (int idx = tid; idx < kInvRows * P; idx += blockDim.x) {
-    const int q = idx / kInvRows;
-    const int rl = idx - q * kInvRows;
-    const int row = blockIdx.x * kInvRows + rl;
-    const int b = q >> 1;
-    if (row >= n || b >= km) continue;
-    C s = red[rl * P + q];
-#pragma unroll
-    for (int gg = 1; gg < kInvKG; gg++) s = cadd(s, red[(gg * kInvRows + rl) * P + q]);
-    if ((q & 1) == 0) {
-      Tout[b * wstride + (long long)f * n + row] = s;
-    } else if (two) {
-      Tout[b * wstride + (long long)i2 * n + row] = (row < MN) ? cscale(s, (R)-1) : s;
-    }
-  }
-}
-
-
 // ------------------------------------------------ apply: streamed inverse blocks
 // The product T2_f = inv(B_f) T_f for P columns (the modes f and L-f of every
 // member) with one CTA per stored block: the block (column-major, ld rows) is
 // streamed through a ring of shared-memory stages, each stage KC whole
 // consecutive columns, which are contiguous in memory and so arrive as ONE bulk
-// asynchronous copy of KC * ld values (16 KB in either precision); a producer
-// warp issues the copies and 512 consumer threads, two rows each, multiply out
-// of shared memory.  Up to kStrMaxStages stages are in flight per CTA, which is
-// what keeps HBM busy; the producer starts while the consumers gather the
-// right-hand sides.  Each row's sums run over the columns in increasing order,
-// so a column's result does not depend on P or on the other members (batched
-// and single solves agree bit for bit).  grid (blocks), kStrThreads threads,
-// shared memory str_smem().
+// asynchronous copy of KC * ld values (32 KB at ld = 1024 in either
+// precision); a producer warp issues the copies and 512 consumer threads, two
+// rows each, multiply out of shared memory.  Up to kStrMaxStages stages are in
+// flight per CTA, which is what keeps HBM busy; the producer starts while the
+// consumers gather the right-hand sides.
+//
+// complex64 runs on the packed FP32 pipe (fma.rn.f32x2, two FMAs per issue):
+// a row's accumulator (re, im) is one register pair, updated as
+//   (re, im) += xr (bx, by) ;  (re, im) += (-xi, xi) (by, bx)
+// with the right-hand side held in shared memory as (xr, xr, -xi, xi), so each
+// complex multiply-add is two packed FMAs and the block element's swap is made
+// once per row for all P columns.  The real part is rounded exactly as a scalar
+// fma chain bx xr - by xi; the imaginary part adds by xr before bx xi.
+// complex128 uses the scalar FP64 pipe.
+//
+// Columns n..ld-1 of every stored block are zero (both block builders clear
+// the padding) and so are the gathered right-hand-side rows k >= n, so the
+// last stage may run past n without a guard: the extra terms add exact zeros.
+// Each row's sums run over the columns in increasing order, so a column's
+// result does not depend on P or on the other members (batched and single
+// solves agree bit for bit).  The ring slot and its phase advance by counting,
+// with no division in the loop.  grid (blocks), kStrThreads threads, shared
+// memory str_smem().
 constexpr int kStrConsumers = 512;
 constexpr int kStrThreads = kStrConsumers + 32;  // + one producer warp
 constexpr int kStrMaxStages = 8;
 
-// whole columns per stage: 16 KB at ld = 1024 in either precision
+// whole columns per stage: 32 KB at ld = 1024 in either precision
 template <typename R>
 constexpr int str_kc() {
-  return sizeof(R) == 4 ? 2 : 1;
+  return sizeof(R) == 4 ? 4 : 2;
 }
 template <typename R>
 inline size_t str_stage_bytes(int ld) {
   return (size_t)str_kc<R>() * ld * sizeof(Cx<R>);
 }
+// one right-hand-side entry in shared memory: 16 bytes in either precision
+// (complex128, or complex64 expanded to xr, xr, -xi, xi)
+constexpr size_t kStrXBytes = 16;
 // right-hand sides [ld][P] + ring [stages][KC][ld]
 template <typename R>
 inline size_t str_smem(int ld, int P, int stages) {
-  return (size_t)ld * P * sizeof(Cx<R>) + (size_t)stages * str_stage_bytes<R>(ld);
+  return (size_t)ld * P * kStrXBytes + (size_t)stages * str_stage_bytes<R>(ld);
 }
 
 // named barrier of the consumer threads (the producer warp may have left)
@@ -1138,11 +1049,22 @@ __device__ __forceinline__ int consumers_sync_or(int pred) {
   return named_bar_or<kStrConsumers>(1, pred);
 }
 
+__device__ __forceinline__ float4 x_expand(float2 v) { return make_float4(v.x, v.x, -v.y, v.y); }
+
+// (re, im) of one row += x * b for the packed layout of x
+__device__ __forceinline__ void pmac(float2& acc, float4 x, float2 b, float2 bs) {
+  acc = __ffma2_rn(make_float2(x.x, x.y), b, acc);
+  acc = __ffma2_rn(make_float2(x.z, x.w), bs, acc);
+}
+
 template <typename R, int P>
 __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     PcGeom g, int paired, int ld, int stages, const Cx<R>* __restrict__ Binv,
     const Cx<R>* __restrict__ Tin, Cx<R>* __restrict__ Tout, const int* skip, int fs, int km) {
   using C = Cx<R>;
+  constexpr bool kPacked = sizeof(R) == 4;
+  using XE = typename std::conditional<kPacked, float4, C>::type;  // 16 bytes
+  static_assert(sizeof(XE) == kStrXBytes, "right-hand-side entry size");
   constexpr int KS = P / 2;
   constexpr int KC = str_kc<R>();
   static_assert(P % 2 == 0, "columns come in mode pairs");
@@ -1155,15 +1077,17 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full[kStrMaxStages];
   __shared__ __align__(8) uint64_t empty[kStrMaxStages];
-  C* X = reinterpret_cast<C*>(smem_raw);  // X[k * P + col], k < ld
-  C* ring = X + (size_t)ld * P;          // [stages][KC][ld]
+  XE* X = reinterpret_cast<XE*>(smem_raw);                      // X[k * P + col], k < ld
+  C* ring = reinterpret_cast<C*>(smem_raw + (size_t)ld * P * kStrXBytes);  // [stages][KC][ld]
   const int n = g.n3;
   const int MN = n / 3;
   const int f = blockIdx.x;
   const int i2 = g.L - f;
   const bool two = paired && f != 0 && i2 != f;
   const long long wstride = pc_work_elems(g);
-  const int nkb = (n + KC - 1) / KC;  // stages of columns < n (padding columns skipped)
+  // stages of KC columns up to n; KC divides 32 and ld is a multiple of 32,
+  // so the last stage stays inside the block
+  const int nkb = (n + KC - 1) / KC;
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < stages; s++) {
@@ -1176,21 +1100,29 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   if (tid >= kStrConsumers) {
     // producer warp: stage kb = columns kb*KC .. kb*KC+KC-1, one contiguous copy
     const int lane = tid & 31;
-    const C* Bf = Binv + (long long)f * ld * ld;
-    const unsigned bytes = (unsigned)(KC * ld * sizeof(C));
+    const C* src = Binv + (long long)f * ld * ld;
+    const size_t step = (size_t)KC * ld;
+    const unsigned bytes = (unsigned)(step * sizeof(C));
+    int s = 0;
+    unsigned ph = 0;  // phase of the slot's previous fill (waited on from the second lap)
     for (int kb = 0; kb < nkb; kb++) {
-      const int s = kb % stages;
-      if (kb >= stages && !mbar_wait(&empty[s], ((kb / stages) - 1) & 1)) return;
+      if (kb >= stages && !mbar_wait(&empty[s], ph ^ 1u)) return;
       if (lane == 0) {
         mbar_arrive_expect_tx(&full[s], bytes);
-        bulk_g2s(ring + (size_t)s * KC * ld, Bf + (long long)kb * KC * ld, bytes, &full[s]);
+        bulk_g2s(ring + (size_t)s * step, src, bytes, &full[s]);
       }
       __syncwarp();
+      src += step;
+      if (++s == stages) {
+        s = 0;
+        ph ^= 1u;
+      }
     }
     return;
   }
   // right-hand sides X[k][2b + (0 | 1)] = (T_f, D T_{L-f}) of member b, member
-  // fastest (one 16-byte pair per thread and row), loads issued in batches
+  // fastest (one 32-byte pair of entries per thread and row), loads issued in
+  // batches; rows n..ld-1 zero
   {
     constexpr int kU = 4;
     const int tot = KS * ld;
@@ -1212,44 +1144,63 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
 #pragma unroll
       for (int u = 0; u < kU; u++) {
         const int t = t0 + u * kStrConsumers;
-        if (t < tot) st_pair(X + (size_t)P * (t / KS) + 2 * (t % KS), v1[u], v2[u]);
+        if (t >= tot) continue;
+        XE* dst = X + (size_t)P * (t / KS) + 2 * (t % KS);
+        if constexpr (kPacked) {
+          dst[0] = x_expand(v1[u]);
+          dst[1] = x_expand(v2[u]);
+        } else {
+          dst[0] = v1[u];
+          dst[1] = v2[u];
+        }
       }
     }
   }
   consumers_sync_or(0);
-  const int r = 2 * tid;  // this thread's rows r, r + 1
+  const int r = 2 * tid;  // this thread's rows r, r + 1 (both < ld)
   const bool active = r < n;
   C a0[P], a1[P];
 #pragma unroll
   for (int q = 0; q < P; q++) a0[q] = a1[q] = czero<C>();
   int failed = 0;
+  const XE* xk = X;
+  int s = 0;
+  unsigned ph = 0;
   for (int kb = 0; kb < nkb; kb++) {
-    const int s = kb % stages;
-    const bool ok = mbar_wait(&full[s], (kb / stages) & 1);
+    const bool ok = mbar_wait(&full[s], ph);
     failed |= !ok;
     if (ok && active) {
       const C* st = ring + (size_t)s * KC * ld + r;
 #pragma unroll
       for (int c = 0; c < KC; c++) {
-        const int k = kb * KC + c;
-        if (k < n) {
-          C b0, b1;
-          ld_pair(st + (size_t)c * ld, b0, b1);
-          const C* xk = X + P * k;
+        C b0, b1;
+        ld_pair(st + (size_t)c * ld, b0, b1);
+        const XE* xc = xk + P * c;
+        if constexpr (kPacked) {
+          const float2 b0s = make_float2(b0.y, b0.x), b1s = make_float2(b1.y, b1.x);
 #pragma unroll
-          for (int q = 0; q < P; q += 2) {
-            C x0, x1;
-            ld_pair(xk + q, x0, x1);
-            cmac(a0[q], b0, x0);
-            cmac(a0[q + 1], b0, x1);
-            cmac(a1[q], b1, x0);
-            cmac(a1[q + 1], b1, x1);
+          for (int q = 0; q < P; q++) {
+            const float4 x = xc[q];
+            pmac(a0[q], x, b0, b0s);
+            pmac(a1[q], x, b1, b1s);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < P; q++) {
+            const C x = xc[q];
+            cmac(a0[q], b0, x);
+            cmac(a1[q], b1, x);
           }
         }
       }
     }
     __syncwarp();
     if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+    xk += P * KC;
+    if (++s == stages) {
+      s = 0;
+      ph ^= 1u;
+    }
   }
   if (consumers_sync_or(failed) || !active) return;
 #pragma unroll

@@ -71,20 +71,20 @@ static int lu_cols(int km) {
   return 2 * ks;
 }
 // Members per launch: every block is streamed once per launch, and the FMAs
-// per streamed byte grow with the members; complex64 takes up to 8 members
-// (16 columns: FP32 issue and HBM time about balance), complex128 up to 4
-// (its right-hand sides fill shared memory).  More members are applied in
-// groups of this size.
+// per streamed byte grow with the members; up to 4 members (8 columns, whose
+// 16-byte right-hand-side entries take 124 KiB of shared memory at ld = 992)
+// in either precision.  More members are applied in groups of this size.
 template <typename R>
 constexpr int apply_members() {
-  return sizeof(R) == 4 ? 8 : 4;
+  return 4;
 }
 
 // Ring stages that fit beside the right-hand sides (at least 2 needed).
 template <typename R>
 static int str_stages(int ld, int P) {
-  const long long room = (long long)kSmemCap - (long long)ld * P * sizeof(Cx<R>);
-  return (int)std::min<long long>(kStrMaxStages, room / (long long)str_stage_bytes<R>(ld));
+  int s = 0;
+  while (s < kStrMaxStages && str_smem<R>(ld, P, s + 1) <= (size_t)kSmemCap) s++;
+  return s;
 }
 
 template <typename R, int P>
@@ -119,10 +119,7 @@ static vox_status inv_apply(vox_precond_s* p, const Cx<R>* T, Cx<R>* T2, cudaStr
     switch (P) {
       case 2: launch_inv_apply<R, 2>(p, Tg, T2g, st, sg, fs, kg); break;
       case 4: launch_inv_apply<R, 4>(p, Tg, T2g, st, sg, fs, kg); break;
-      case 8: launch_inv_apply<R, 8>(p, Tg, T2g, st, sg, fs, kg); break;
-      default:
-        if constexpr (sizeof(R) == 4) launch_inv_apply<R, 16>(p, Tg, T2g, st, sg, fs, kg);
-        break;
+      default: launch_inv_apply<R, 8>(p, Tg, T2g, st, sg, fs, kg); break;
     }
   }
   return VOX_OK;
@@ -212,7 +209,6 @@ static vox_status pc_apply(vox_precond_s* p, const Cx<R>* in, Cx<R>* out, cudaSt
     return VOX_ERR_BAD_ARG;
   }
   const PcGeom& g = p->g;
-  const size_t cs = sizeof(Cx<R>);
   const int nb = (g.n3 + g.ybx - 1) / g.ybx;
   const dim3 gx(nb, mm.km);
   Cx<R>* T = pc_T<R>(p, 0) + mm.m0 * pc_work_elems(g);
@@ -245,7 +241,6 @@ static vox_status pc_attrs() {
   VOX_TRY(smem_cap(k_pc_inv_stream<R, 2>));
   VOX_TRY(smem_cap(k_pc_inv_stream<R, 4>));
   VOX_TRY(smem_cap(k_pc_inv_stream<R, 8>));
-  if constexpr (sizeof(R) == 4) VOX_TRY(smem_cap(k_pc_inv_stream<R, 16>));
   VOX_TRY(smem_cap(k_l2_yfwd<R>));
   VOX_TRY(smem_cap(k_l2_yinv<R>));
   VOX_TRY(smem_cap(k_l2_gemv<R, 1>));
@@ -277,21 +272,21 @@ struct PcFactors {
   float2* twyf = nullptr;
   int* vmap = nullptr;  // a box's own index map
   ~PcFactors() {
-    cudaFree(twyd);
-    cudaFree(twyf);
-    cudaFree(vmap);
-    cudaFree(Ad);
-    cudaFree(Af);
-    cudaFree(piv);
-    cudaFree(perm);
-    cudaFree(Dld);
-    cudaFree(Dud);
-    cudaFree(Dlf);
-    cudaFree(Duf);
-    cudaFree(tiles_d);
-    cudaFree(tiles_f);
-    cudaFree(twd);
-    cudaFree(twf);
+    dfree(twyd);
+    dfree(twyf);
+    dfree(vmap);
+    dfree(Ad);
+    dfree(Af);
+    dfree(piv);
+    dfree(perm);
+    dfree(Dld);
+    dfree(Dud);
+    dfree(Dlf);
+    dfree(Duf);
+    dfree(tiles_d);
+    dfree(tiles_f);
+    dfree(twd);
+    dfree(twf);
   }
 };
 
@@ -340,10 +335,10 @@ static void pc_free(vox_precond_s* p) {
     own.twyf = p->twyf;
     if (p->op && p->vmap && p->vmap != p->op->vmap) own.vmap = const_cast<int*>(p->vmap);
   }
-  cudaFree(p->Td);
-  cudaFree(p->Td2);
-  cudaFree(p->Tf);
-  cudaFree(p->Tf2);
+  dfree(p->Td);
+  dfree(p->Td2);
+  dfree(p->Tf);
+  dfree(p->Tf2);
   delete p;
 }
 
@@ -372,7 +367,7 @@ static vox_status pc_common(vox_op_s* op, vox_precond_s* p, int L, int M, int N,
   }
   // the LU panel bound (n3 <= 1760) also keeps the streamed solve's
   // ring + right-hand sides (64 KiB + 32 B * n3) and the streamed apply's
-  // (two 16 KiB stages + 32 B * ld) under the cap
+  // (two 32 KiB stages + 32 B * ld) under the cap
   if (lu && ((size_t)g.n3 * kLuNb * sizeof(double2) > (size_t)kSmemCap ||
              lu_stream2_smem<double>(lu_npad(g.n3), kInvBuildCols) > (size_t)kSmemCap ||
              str_smem<double>((g.n3 + 31) / 32 * 32, 2, 2) > (size_t)kSmemCap ||
@@ -412,9 +407,9 @@ static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector
   // Toeplitz -> Chan circulants -> FFT along x
   double2 *dG, *dC;
   VOX_TRY(dalloc(&dG, 6 * V));
-  std::unique_ptr<double2, decltype(&cudaFree)> gG(dG, cudaFree);
+  std::unique_ptr<double2, decltype(&dfree)> gG(dG, dfree);
   VOX_TRY(dalloc(&dC, 6 * V));
-  std::unique_ptr<double2, decltype(&cudaFree)> gC(dC, cudaFree);
+  std::unique_ptr<double2, decltype(&dfree)> gC(dC, dfree);
   VOX_CUDA(cudaMemcpyAsync(dG, G.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice,
                            st));
   k_chan<<<nblk(6 * V), 256, 0, st>>>(g.L, V, dG, dC);
@@ -422,7 +417,7 @@ static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector
   VOX_TRY(fft_axis_d(dC, g.L, g.M, g.N, 1, g.L, (long long)g.L * g.M, V, 6, 0, -1, st));
   double* dface;
   VOX_TRY(dalloc(&dface, g.n3));
-  std::unique_ptr<double, decltype(&cudaFree)> gF(dface, cudaFree);
+  std::unique_ptr<double, decltype(&dfree)> gF(dface, dfree);
   VOX_CUDA(cudaMemcpyAsync(dface, face3.data(), g.n3 * sizeof(double), cudaMemcpyHostToDevice,
                            st));
   // Pairing: the Chan circulants satisfy c[L-j] = s*c[j] (s = -1 for xy, xz),
@@ -458,7 +453,7 @@ static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector
   VOX_CUDA(cudaGetLastError());
   int* dinfo;
   VOX_TRY(dalloc(&dinfo, Lf));
-  std::unique_ptr<int, decltype(&cudaFree)> gI(dinfo, cudaFree);
+  std::unique_ptr<int, decltype(&dfree)> gI(dinfo, dfree);
   VOX_CUDA(cudaMemsetAsync(dinfo, 0, Lf * sizeof(int), st));
   k_lu_batched<double><<<Lf, 512, (size_t)g.n3 * kLuNb * sizeof(double2), st>>>(g.n3, ld, p->Ad,
                                                                                 p->piv, dinfo);
@@ -497,9 +492,9 @@ static vox_status build_level1(vox_op_s* op, vox_precond_s* p, const std::vector
     VOX_CUDA(cudaGetLastError());
   }
   VOX_TRY(wait_stream(st));
-  cudaFree(p->tiles_d);
-  cudaFree(p->Dld);
-  cudaFree(p->Dud);
+  dfree(p->tiles_d);
+  dfree(p->Dld);
+  dfree(p->Dud);
   p->tiles_d = nullptr;
   p->Dld = p->Dud = nullptr;
   (void)dsz;
@@ -540,9 +535,9 @@ static vox_status build_level2(vox_op_s* op, vox_precond_s* p, const std::vector
                            st));
   double2 *dA, *dC;
   VOX_TRY(dalloc(&dA, 6 * V));
-  std::unique_ptr<double2, decltype(&cudaFree)> gA(dA, cudaFree);
+  std::unique_ptr<double2, decltype(&dfree)> gA(dA, dfree);
   VOX_TRY(dalloc(&dC, 6 * V));
-  std::unique_ptr<double2, decltype(&cudaFree)> gC(dC, cudaFree);
+  std::unique_ptr<double2, decltype(&dfree)> gC(dC, dfree);
   VOX_CUDA(cudaMemcpyAsync(dA, A.data(), 6 * V * sizeof(double2), cudaMemcpyHostToDevice,
                            st));
   k_chan<<<nblk(6 * V), 256, 0, st>>>(g.L, V, dA, dC);
@@ -558,7 +553,7 @@ static vox_status build_level2(vox_op_s* op, vox_precond_s* p, const std::vector
   VOX_CUDA(cudaGetLastError());
   int* dinfo;
   VOX_TRY(dalloc(&dinfo, nblocks));
-  std::unique_ptr<int, decltype(&cudaFree)> gI(dinfo, cudaFree);
+  std::unique_ptr<int, decltype(&dfree)> gI(dinfo, dfree);
   VOX_CUDA(cudaMemsetAsync(dinfo, 0, nblocks * sizeof(int), st));
   k_small_inv<<<(unsigned)nblocks, 128, (size_t)2 * n2 * n2 * sizeof(double2), st>>>(n2, p->Ad,
                                                                                      dinfo);
@@ -648,7 +643,7 @@ vox_status vox_precond_create_box(vox_op_t op, int level, int x0, int y0, int Ls
                                                      op->vmap, dmask, vm);
     VOX_CUDA(cudaGetLastError());
     VOX_TRY(wait_stream(op->stream));
-    cudaFree(dmask);
+    dfree(dmask);
   }
   VOX_TRY(pc_common(op, p.get(), Ls, Ms, Ns, level == 1));
   // A = -Mc .* G, Gram * Mr(1) added at the origin of the diagonal components

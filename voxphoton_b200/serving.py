@@ -38,6 +38,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import _lib
 from . import geometry as geo
 from .vie import Lane, Operator, Preconditioner, assemble_toeplitz
 
@@ -424,11 +425,13 @@ class SweepServer:
         measured once per family (operator, work, Krylov arenas)."""
         import torch
         torch.cuda.synchronize()
-        free0, _ = torch.cuda.mem_get_info()
+        held0 = _lib.mem_in_use(fam.device)
         op, pc = fam.add_slot(torch.cuda.Stream())
         lane = self._lane(fam, op, pc)
         if fam.key not in self.lane_bytes:
-            # one warm solve allocates the lane's arenas and captures its graph
+            # one warm solve allocates the lane's arenas and captures its graph;
+            # the library's own count of device bytes, so the CUDA context,
+            # modules loaded on first use and torch's pool do not enter it
             lam = float(np.mean(fam.nodes))
             op.interp(fam.node_ops, lagrange_weights(lam, fam.nodes), member=0)
             lane.submit(0, fam.rhs(geo.C0 / lam * geo.N_EXT))
@@ -436,8 +439,7 @@ class SweepServer:
                 pass
             lane.collect(0, host=False)
             torch.cuda.synchronize()
-            free1, _ = torch.cuda.mem_get_info()
-            self.lane_bytes[fam.key] = max(int(free0 - free1), 1)
+            self.lane_bytes[fam.key] = max(_lib.mem_in_use(fam.device) - held0, 1)
         ctx = _LaneCtx(fam, op, pc, lane, self.lane_bytes[fam.key])
         self._pool.append(ctx)
         self.pool_events.append(("add", fam.key, ctx.nbytes, time.perf_counter()))
