@@ -433,11 +433,26 @@ __global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>*
   const int c = blockIdx.z - 3 * mb;
   const int YB = g.ybx;
   const int ny = min(YB, g.M - y0);
-  for (int t = threadIdx.x; t < YB * g.Px; t += blockDim.x) {
-    const int kx = t / YB;
-    const int yb = t - kx * YB;
-    bufA[(size_t)yb * g.sx + kx] =
-        (yb < ny) ? T2[(((long long)kx * 3 + c) * g.N + z) * g.M + y0 + yb] : czero<C>();
+  // the pencils' values of every plane, kLoad loads in flight per thread
+  // before their stores
+  constexpr int kLoad = 8;
+  const int tot = YB * g.Px;
+  for (int t0 = threadIdx.x; t0 < tot; t0 += kLoad * blockDim.x) {
+    C v[kLoad];
+#pragma unroll
+    for (int u = 0; u < kLoad; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int kx = t / YB;
+      const int yb = t - kx * YB;
+      v[u] = (t < tot && yb < ny) ? T2[(((long long)kx * 3 + c) * g.N + z) * g.M + y0 + yb]
+                                  : czero<C>();
+    }
+#pragma unroll
+    for (int u = 0; u < kLoad; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int kx = t / YB;
+      if (t < tot) bufA[(size_t)(t - kx * YB) * g.sx + kx] = v[u];
+    }
   }
   __syncthreads();
   C* res = block_fft(bufA, bufB, px, YB, g.sx, tw, +1);

@@ -18,6 +18,7 @@
 // k_plane (no scaling here: 1/P is applied by k_xinv).
 #pragma once
 
+#include "bulk.cuh"
 #include "mvp.cuh"
 
 namespace vox {
@@ -35,10 +36,15 @@ constexpr int kPlFn = (kPlPy / 2 + 1) * (kPlPz / 2 + 1) * 6;
 constexpr int kPlRowsPerWarp = 5;
 
 // shared memory: y-transformed rows [3N][65] + z spectra [3][64][24 + 1] + the
-// plane's octant of fN
+// plane's octant of fN (from a 16-byte boundary: it arrives by a bulk copy)
+template <typename R>
+constexpr size_t plane64_fn_offset(int N) {
+  return (((size_t)3 * N * kPlSy + (size_t)3 * kPlPy * (kPlPz + 1)) * sizeof(Cx<R>) + 15) /
+         16 * 16;
+}
 template <typename R>
 constexpr size_t plane64_smem(int N) {
-  return ((size_t)3 * N * kPlSy + (size_t)3 * kPlPy * (kPlPz + 1) + kPlFn) * sizeof(Cx<R>);
+  return plane64_fn_offset<R>(N) + (size_t)kPlFn * sizeof(Cx<R>);
 }
 
 template <typename C>
@@ -126,21 +132,27 @@ __global__ void __launch_bounds__(kPlThreads, 2)
   T2 += mb * plane_elems(g);
   fN += mb * fN_elems(g);
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t fbar;
   const int N = g.N, M = g.M;
   const int rows = 3 * N;
   C* yb = reinterpret_cast<C*>(smem_raw);  // [3N][kPlSy], columns bit-reversed
   C* zb = yb + (size_t)rows * kPlSy;        // [3][64][25] z spectra
-  C* fsm = zb + (size_t)3 * kPlPy * (kPlPz + 1);  // the plane's fN octant
+  C* fsm = reinterpret_cast<C*>(smem_raw + plane64_fn_offset<R>(N));  // the plane's fN octant
   const int kx = blockIdx.x;
   const C* tin = T1 + (long long)kx * rows * M;
   C* tout = T2 + (long long)kx * rows * M;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // fN is stored as one octant (the operator's parity holds: plane64_ok)
+  // fN is stored as one octant (the operator's parity holds: plane64_ok); the
+  // plane's octant is contiguous (kPlFn values from a 16-byte boundary) and
+  // arrives by one bulk copy while the rows are transformed
   const int fx = 2 * kx > g.Px;
   const int hy = g.Py / 2 + 1, hz = g.Pz / 2 + 1;
-  {
+  if (tid == 0) {
     const C* fplane = fN + (long long)(fx ? g.Px - kx : kx) * hy * hz * 6;
-    for (int t = tid; t < kPlFn; t += kPlThreads) fsm[t] = fplane[t];
+    mbar_init(&fbar, 1);
+    mbar_init_fence();
+    mbar_arrive_expect_tx(&fbar, (unsigned)(kPlFn * sizeof(C)));
+    bulk_g2s(fsm, fplane, (unsigned)(kPlFn * sizeof(C)), &fbar);
   }
 
   // ---- A: forward y-FFT, one warp per row (the warp's rows loaded first)
@@ -188,7 +200,8 @@ __global__ void __launch_bounds__(kPlThreads, 2)
 #pragma unroll
     for (int kz = 0; kz < kPlPz; kz++) zr[kz] = Z[kz];
   }
-  __syncthreads();
+  // the fN octant has landed (bounded wait; every thread leaves if any gave up)
+  if (__syncthreads_or(!mbar_wait(&fbar, 0))) return;
   if (c < 3) {
     const int fy = 2 * ky > g.Py;
     const int yo = fy ? g.Py - ky : ky;

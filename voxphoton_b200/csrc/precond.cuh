@@ -88,6 +88,11 @@ __device__ __forceinline__ void st_pair(double2* p, double2 a, double2 b) {
 // --------------------------------------------------------------- apply: x-FFT
 // kBig: the x length L has a prime factor above 13 (compiled big-prime
 // butterflies; a separate instantiation keeps the others' register budget).
+// Global loads are issued kPcBatch (gathers) or 2 kPcBatch (the transformed
+// lines) per thread before their stores, so each thread keeps several reads in
+// flight.
+constexpr int kPcBatch = 4;
+
 template <typename R, bool kBig>
 __global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,
                                                  const Cx<R>* __restrict__ in,
@@ -104,15 +109,26 @@ __global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xfwd
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int col0 = blockIdx.x * g.ybx;
   const int nl = min(g.ybx, g.n3 - col0);
-  for (int t = threadIdx.x; t < g.ybx * g.L; t += blockDim.x) {
-    const int l = t / g.L;
-    const int x = t - l * g.L;
-    C v = czero<C>();
-    if (l < nl) {
-      const int m = vmap[(long long)(col0 + l) * g.L + x];
-      if (m >= 0) v = in[m];
+  // gather in batches of kPcBatch per thread: the index-map loads, then the
+  // vector loads, then the stores
+  const int tot = g.ybx * g.L;
+  for (int t0 = threadIdx.x; t0 < tot; t0 += kPcBatch * blockDim.x) {
+    int m[kPcBatch];
+#pragma unroll
+    for (int u = 0; u < kPcBatch; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int l = t / g.L;
+      m[u] = (t < tot && l < nl) ? vmap[(long long)(col0 + l) * g.L + (t - l * g.L)] : -1;
     }
-    bufA[(size_t)l * g.sx + x] = v;
+    C v[kPcBatch];
+#pragma unroll
+    for (int u = 0; u < kPcBatch; u++) v[u] = m[u] >= 0 ? in[m[u]] : czero<C>();
+#pragma unroll
+    for (int u = 0; u < kPcBatch; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int l = t / g.L;
+      if (t < tot) bufA[(size_t)l * g.sx + (t - l * g.L)] = v[u];
+    }
   }
   __syncthreads();
   C* res = block_fft<C, kBig>(bufA, bufB, pl, g.ybx, g.sx, tw, -1);
@@ -139,18 +155,41 @@ __global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xinv
   C* bufB = bufA + (size_t)g.ybx * g.sx;
   const int col0 = blockIdx.x * g.ybx;
   const int nl = min(g.ybx, g.n3 - col0);
-  for (int t = threadIdx.x; t < g.ybx * g.L; t += blockDim.x) {
-    const int i = t / g.ybx;
-    const int l = t - i * g.ybx;
-    bufA[(size_t)l * g.sx + i] = (l < nl) ? T[(long long)i * g.n3 + col0 + l] : czero<C>();
+  const int tot = g.ybx * g.L;
+  for (int t0 = threadIdx.x; t0 < tot; t0 += 2 * kPcBatch * blockDim.x) {
+    C v[2 * kPcBatch];
+#pragma unroll
+    for (int u = 0; u < 2 * kPcBatch; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int i = t / g.ybx;
+      const int l = t - i * g.ybx;
+      v[u] = (t < tot && l < nl) ? T[(long long)i * g.n3 + col0 + l] : czero<C>();
+    }
+#pragma unroll
+    for (int u = 0; u < 2 * kPcBatch; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int i = t / g.ybx;
+      if (t < tot) bufA[(size_t)(t - i * g.ybx) * g.sx + i] = v[u];
+    }
   }
   __syncthreads();
   C* res = block_fft<C, kBig>(bufA, bufB, pl, g.ybx, g.sx, tw, +1);
-  for (int t = threadIdx.x; t < nl * g.L; t += blockDim.x) {
-    const int l = t / g.L;
-    const int x = t - l * g.L;
-    const int m = vmap[(long long)(col0 + l) * g.L + x];
-    if (m >= 0) out[m] = cscale(res[(size_t)l * g.sx + x], scale);
+  const int totw = nl * g.L;
+  for (int t0 = threadIdx.x; t0 < totw; t0 += kPcBatch * blockDim.x) {
+    int m[kPcBatch];
+#pragma unroll
+    for (int u = 0; u < kPcBatch; u++) {
+      const int t = t0 + u * blockDim.x;
+      const int l = t / g.L;
+      m[u] = t < totw ? vmap[(long long)(col0 + l) * g.L + (t - l * g.L)] : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < kPcBatch; u++) {
+      if (m[u] < 0) continue;
+      const int t = t0 + u * blockDim.x;
+      const int l = t / g.L;
+      out[m[u]] = cscale(res[(size_t)l * g.sx + (t - l * g.L)], scale);
+    }
   }
 }
 
@@ -1005,14 +1044,17 @@ __global__ void __launch_bounds__(32 * kRoundTiles) k_lu_inv_cols(
 // flight per CTA, which is what keeps HBM busy; the producer starts while the
 // consumers gather the right-hand sides.
 //
-// complex64 runs on the packed FP32 pipe (fma.rn.f32x2, two FMAs per issue):
-// a row's accumulator (re, im) is one register pair, updated as
-//   (re, im) += xr (bx, by) ;  (re, im) += (-xi, xi) (by, bx)
-// with the right-hand side held in shared memory as (xr, xr, -xi, xi), so each
-// complex multiply-add is two packed FMAs and the block element's swap is made
-// once per row for all P columns.  The real part is rounded exactly as a scalar
-// fma chain bx xr - by xi; the imaginary part adds by xr before bx xi.
-// complex128 uses the scalar FP64 pipe.
+// complex64 runs on the packed FP32 pipe (fma.rn.f32x2: one instruction, two
+// FMAs) with three real multiplies per complex multiply-add (Gauss):
+//   S1 += br xr,  S2 += bi xi,  S3 += (br + bi)(xr + xi);
+//   re = S1 - S2,  im = (S3 - S1) - S2  (once, after the last column).
+// The pair of a register is the two columns of one member (modes f and L-f),
+// so the right-hand sides are held in shared memory as (xr_f, xr_L-f, xi_f,
+// xi_L-f) and (xs_f, xs_L-f) with xs = xr + xi, and the block element's
+// (br, br), (bi, bi), (br + bi, br + bi) are formed once per row for all
+// members.  That is 3 FMAs per complex term instead of 4, on half the issue
+// slots; the sums are the same terms in the same order for every P.
+// complex128 uses the scalar FP64 pipe with the usual four multiplies.
 //
 // Columns n..ld-1 of every stored block are zero (both block builders clear
 // the padding) and so are the gathered right-hand-side rows k >= n, so the
@@ -1035,13 +1077,16 @@ template <typename R>
 inline size_t str_stage_bytes(int ld) {
   return (size_t)str_kc<R>() * ld * sizeof(Cx<R>);
 }
-// one right-hand-side entry in shared memory: 16 bytes in either precision
-// (complex128, or complex64 expanded to xr, xr, -xi, xi)
-constexpr size_t kStrXBytes = 16;
+// shared-memory bytes of one right-hand-side entry (one row of one column):
+// complex128 16; complex64 12 (xr, xi and xr + xi)
+template <typename R>
+constexpr size_t str_x_bytes() {
+  return sizeof(R) == 4 ? 12 : 16;
+}
 // right-hand sides [ld][P] + ring [stages][KC][ld]
 template <typename R>
 inline size_t str_smem(int ld, int P, int stages) {
-  return (size_t)ld * P * kStrXBytes + (size_t)stages * str_stage_bytes<R>(ld);
+  return (size_t)ld * P * str_x_bytes<R>() + (size_t)stages * str_stage_bytes<R>(ld);
 }
 
 // named barrier of the consumer threads (the producer warp may have left)
@@ -1049,13 +1094,10 @@ __device__ __forceinline__ int consumers_sync_or(int pred) {
   return named_bar_or<kStrConsumers>(1, pred);
 }
 
-__device__ __forceinline__ float4 x_expand(float2 v) { return make_float4(v.x, v.x, -v.y, v.y); }
-
-// (re, im) of one row += x * b for the packed layout of x
-__device__ __forceinline__ void pmac(float2& acc, float4 x, float2 b, float2 bs) {
-  acc = __ffma2_rn(make_float2(x.x, x.y), b, acc);
-  acc = __ffma2_rn(make_float2(x.z, x.w), bs, acc);
-}
+// three packed sums of one row and one member's column pair
+struct Sums3 {
+  float2 s1, s2, s3;
+};
 
 template <typename R, int P>
 __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
@@ -1063,8 +1105,6 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     const Cx<R>* __restrict__ Tin, Cx<R>* __restrict__ Tout, const int* skip, int fs, int km) {
   using C = Cx<R>;
   constexpr bool kPacked = sizeof(R) == 4;
-  using XE = typename std::conditional<kPacked, float4, C>::type;  // 16 bytes
-  static_assert(sizeof(XE) == kStrXBytes, "right-hand-side entry size");
   constexpr int KS = P / 2;
   constexpr int KC = str_kc<R>();
   static_assert(P % 2 == 0, "columns come in mode pairs");
@@ -1077,8 +1117,12 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full[kStrMaxStages];
   __shared__ __align__(8) uint64_t empty[kStrMaxStages];
-  XE* X = reinterpret_cast<XE*>(smem_raw);                      // X[k * P + col], k < ld
-  C* ring = reinterpret_cast<C*>(smem_raw + (size_t)ld * P * kStrXBytes);  // [stages][KC][ld]
+  // right-hand sides: complex128 X[k * P + col]; complex64 XA[k * KS + b] =
+  // (xr_f, xr_L-f, xi_f, xi_L-f) and XS[k * KS + b] = (xs_f, xs_L-f) of member b
+  C* X = reinterpret_cast<C*>(smem_raw);
+  float4* XA = reinterpret_cast<float4*>(smem_raw);
+  float2* XS = reinterpret_cast<float2*>(smem_raw + (size_t)ld * KS * sizeof(float4));
+  C* ring = reinterpret_cast<C*>(smem_raw + (size_t)ld * P * str_x_bytes<R>());  // [stages][KC][ld]
   const int n = g.n3;
   const int MN = n / 3;
   const int f = blockIdx.x;
@@ -1120,9 +1164,8 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     }
     return;
   }
-  // right-hand sides X[k][2b + (0 | 1)] = (T_f, D T_{L-f}) of member b, member
-  // fastest (one 32-byte pair of entries per thread and row), loads issued in
-  // batches; rows n..ld-1 zero
+  // right-hand sides (T_f, D T_{L-f}) of member b at row k, member fastest,
+  // loads issued in batches; rows n..ld-1 zero
   {
     constexpr int kU = 4;
     const int tot = KS * ld;
@@ -1145,11 +1188,11 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
       for (int u = 0; u < kU; u++) {
         const int t = t0 + u * kStrConsumers;
         if (t >= tot) continue;
-        XE* dst = X + (size_t)P * (t / KS) + 2 * (t % KS);
         if constexpr (kPacked) {
-          dst[0] = x_expand(v1[u]);
-          dst[1] = x_expand(v2[u]);
+          XA[t] = make_float4(v1[u].x, v2[u].x, v1[u].y, v2[u].y);
+          XS[t] = make_float2(v1[u].x + v1[u].y, v2[u].x + v2[u].y);
         } else {
+          C* dst = X + (size_t)2 * t;  // X[k * P + 2b], t = k * KS + b
           dst[0] = v1[u];
           dst[1] = v2[u];
         }
@@ -1159,11 +1202,20 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   consumers_sync_or(0);
   const int r = 2 * tid;  // this thread's rows r, r + 1 (both < ld)
   const bool active = r < n;
-  C a0[P], a1[P];
+  // complex64: sums [row][member]; complex128: accumulators [row][column]
+  Sums3 q3[2][kPacked ? KS : 1];
+  C a0[kPacked ? 1 : P], a1[kPacked ? 1 : P];
+  if constexpr (kPacked) {
 #pragma unroll
-  for (int q = 0; q < P; q++) a0[q] = a1[q] = czero<C>();
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int b = 0; b < KS; b++) q3[h][b].s1 = q3[h][b].s2 = q3[h][b].s3 = make_float2(0.f, 0.f);
+  } else {
+#pragma unroll
+    for (int q = 0; q < P; q++) a0[q] = a1[q] = czero<C>();
+  }
   int failed = 0;
-  const XE* xk = X;
+  int k0 = 0;  // first block column of the stage
   int s = 0;
   unsigned ph = 0;
   for (int kb = 0; kb < nkb; kb++) {
@@ -1171,20 +1223,30 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     failed |= !ok;
     if (ok && active) {
       const C* st = ring + (size_t)s * KC * ld + r;
-#pragma unroll
+#pragma unroll 2
       for (int c = 0; c < KC; c++) {
         C b0, b1;
         ld_pair(st + (size_t)c * ld, b0, b1);
-        const XE* xc = xk + P * c;
+        const int k = k0 + c;
         if constexpr (kPacked) {
-          const float2 b0s = make_float2(b0.y, b0.x), b1s = make_float2(b1.y, b1.x);
+          const float2 br[2] = {make_float2(b0.x, b0.x), make_float2(b1.x, b1.x)};
+          const float2 bi[2] = {make_float2(b0.y, b0.y), make_float2(b1.y, b1.y)};
+          const float2 bs[2] = {__fadd2_rn(br[0], bi[0]), __fadd2_rn(br[1], bi[1])};
+          const float4* xa = XA + (size_t)k * KS;
+          const float2* xs = XS + (size_t)k * KS;
 #pragma unroll
-          for (int q = 0; q < P; q++) {
-            const float4 x = xc[q];
-            pmac(a0[q], x, b0, b0s);
-            pmac(a1[q], x, b1, b1s);
+          for (int b = 0; b < KS; b++) {
+            const float4 a = xa[b];
+            const float2 xr = make_float2(a.x, a.y), xi = make_float2(a.z, a.w), xsb = xs[b];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              q3[h][b].s1 = __ffma2_rn(br[h], xr, q3[h][b].s1);
+              q3[h][b].s2 = __ffma2_rn(bi[h], xi, q3[h][b].s2);
+              q3[h][b].s3 = __ffma2_rn(bs[h], xsb, q3[h][b].s3);
+            }
           }
         } else {
+          const C* xc = X + (size_t)P * k;
 #pragma unroll
           for (int q = 0; q < P; q++) {
             const C x = xc[q];
@@ -1196,7 +1258,7 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
     }
     __syncwarp();
     if ((tid & 31) == 0) mbar_arrive(&empty[s]);
-    xk += P * KC;
+    k0 += KC;
     if (++s == stages) {
       s = 0;
       ph ^= 1u;
@@ -1207,10 +1269,19 @@ __global__ void __launch_bounds__(kStrThreads, 1) k_pc_inv_stream(
   for (int q = 0; q < P; q++) {
     const int b = q >> 1;
     if (b >= km) continue;
+#pragma unroll
     for (int h = 0; h < 2; h++) {
       const int row = r + h;
       if (row >= n) continue;
-      const C v = h ? a1[q] : a0[q];
+      C v;
+      if constexpr (kPacked) {
+        const Sums3& t = q3[h][b];
+        const float s1 = (q & 1) ? t.s1.y : t.s1.x, s2 = (q & 1) ? t.s2.y : t.s2.x,
+                    s3 = (q & 1) ? t.s3.y : t.s3.x;
+        v = make_float2(s1 - s2, (s3 - s1) - s2);
+      } else {
+        v = h ? a1[q] : a0[q];
+      }
       if ((q & 1) == 0) {
         Tout[b * wstride + (long long)f * n + row] = v;
       } else if (two) {

@@ -72,8 +72,9 @@ static int lu_cols(int km) {
 }
 // Members per launch: every block is streamed once per launch, and the FMAs
 // per streamed byte grow with the members; up to 4 members (8 columns, whose
-// 16-byte right-hand-side entries take 124 KiB of shared memory at ld = 992)
-// in either precision.  More members are applied in groups of this size.
+// right-hand sides take 93 KiB (complex64) or 124 KiB (complex128) of shared
+// memory at ld = 992) in either precision.  More members are applied in groups
+// of this size.
 template <typename R>
 constexpr int apply_members() {
   return 4;
