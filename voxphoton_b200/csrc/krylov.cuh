@@ -581,8 +581,8 @@ __global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x
 
 
 // ------------------------------------------- Gram-Schmidt in two basis reads
-// For restart lengths up to kGsMaxCols - 1 an Arnoldi step reads the basis
-// twice (it read it four times in the kernels above):
+// For restart lengths up to kGsMaxCols - 1 an Arnoldi step reads the basis in
+// two passes and a finishing sweep (CGS2; the kernels above read it four times):
 //   k_gs_pass<false>: h1 = V^H w;
 //   k_gs_pass<true>:  w' = w - V h1 (written back), h2 = V^H w' and ||w'||^2
 //                     in the same read; its last CTA forms the Hessenberg
@@ -592,10 +592,11 @@ __global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x
 // The two passes are producer/consumer pipelines: one producer warp streams
 // chunks of gs_rows() rows of all k+1 basis columns and of w into a ring of
 // shared-memory stages with bulk asynchronous copies (mbarrier completion,
-// bounded waits), and eight consumer warps take the dot products out of shared
-// memory, one warp per column, accumulating in FP64 in a fixed order
-// (deterministic); the update of w' (pass<true>) runs one thread per row
-// before the dots of the same stage.
+// bounded waits), and sixteen consumer warps take the dot products out of
+// shared memory, one warp per column, accumulating in FP64 in a fixed order
+// (deterministic; in complex64 a lane sums its rows of one chunk with FP32
+// FMAs first, so FP64 conversions are per chunk, not per element); the update
+// of w' (pass<true>) runs one thread per row before the dots of the same stage.
 constexpr int kGsMaxCols = 51;
 constexpr int kGsConsumers = 512;
 constexpr int kGsWarps = kGsConsumers / 32;  // consumer warps
@@ -704,7 +705,10 @@ __global__ void __launch_bounds__(kGsThreads, 1) k_gs_pass(GmresDev* st, int k,
         }
         ws[tid] = wi;
         w[r0 + tid] = wi;
-        nrm += (double)wi.x * wi.x + (double)wi.y * wi.y;
+        if constexpr (sizeof(R) == 4)
+          nrm += (double)fmaf(wi.x, wi.x, wi.y * wi.y);
+        else
+          nrm += (double)wi.x * wi.x + (double)wi.y * wi.y;
       }
       consumer_bar();
     }
@@ -712,10 +716,27 @@ __global__ void __launch_bounds__(kGsThreads, 1) k_gs_pass(GmresDev* st, int k,
     for (int q = 0; q < kGsColsPerWarp; q++) {
       const int j = warp + q * kGsWarps;
       if (j < nj) {
-        for (int r = lane; r < rows; r += 32) {
-          const double2 v = to_d2(Vs[(size_t)j * RW + r]);
-          const double2 x = to_d2(ws[r]);
-          acc_cdot(acc[q], v.x, v.y, x.x, x.y);
+        if constexpr (sizeof(R) == 4) {
+          // complex64: a lane's rows of the chunk (at most RW / 32 = 16) summed
+          // with FP32 FMAs, the partial sum carried in FP64 across chunks (a
+          // conversion per lane, column and chunk, not per element)
+          float2 p = make_float2(0.f, 0.f);
+          for (int r = lane; r < rows; r += 32) {
+            const C v = Vs[(size_t)j * RW + r];
+            const C x = ws[r];
+            p.x = fmaf(v.x, x.x, p.x);
+            p.x = fmaf(v.y, x.y, p.x);
+            p.y = fmaf(v.x, x.y, p.y);
+            p.y = fmaf(-v.y, x.x, p.y);
+          }
+          acc[q].x += (double)p.x;
+          acc[q].y += (double)p.y;
+        } else {
+          for (int r = lane; r < rows; r += 32) {
+            const double2 v = to_d2(Vs[(size_t)j * RW + r]);
+            const double2 x = to_d2(ws[r]);
+            acc_cdot(acc[q], v.x, v.y, x.x, x.y);
+          }
         }
       }
     }
