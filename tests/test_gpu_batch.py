@@ -30,12 +30,12 @@ def family():
         op.close()
 
 
-def _solo(p, idx, Gs, nodes, pc, lam, b):
+def _solo(p, idx, Gs, nodes, pc, lam, b, side="left"):
     op = vb.Operator(p.Mop(), p.Gram, idx, G=Gs[1])
     pcs = pc.share(op)
     op.interp(nodes, sv.lagrange_weights(lam, NODES))
-    x, info = vb.solve_refined(op, b, tol=1e-5, restart=50, maxit_inner=40, inner_tol=0.0,
-                               L1=pcs)
+    kw = {"L1": pcs} if side == "left" else {"R1": pcs}
+    x, info = vb.solve_refined(op, b, tol=1e-5, restart=50, maxit_inner=40, inner_tol=0.0, **kw)
     pcs.close()
     op.close()
     return x, info
@@ -118,14 +118,18 @@ def test_stage_profile_of_a_batch(family):
     op.close()
 
 
-def test_lane_refills_members_and_matches_solo_solves(family):
+@pytest.mark.parametrize("side,steps", [("left", "4"), ("right", "4"), ("right", "1"),
+                                        ("right", "7"), ("left", "0")])
+def test_lane_refills_members_and_matches_solo_solves(family, monkeypatch, side, steps):
     # 5 requests on 3 members: slots are refilled while other members are
-    # mid-solve; every result must equal the single-right-hand-side solve
+    # mid-solve; every result must equal the single-right-hand-side solve.
+    # VOX_LANE_STEPS: out-of-phase steps per lane step (0: in-phase cycles)
+    monkeypatch.setenv("VOX_LANE_STEPS", steps)
     p, idx, Gs, nodes, pc, rhs = family
     lams = np.linspace(1502e-9, 1598e-9, 5)
     op = vb.Operator(p.Mop(), p.Gram, idx, G=Gs[1], members=3)
     pcb = pc.share(op)
-    lane = vb.Lane(op, pcb, side="left", tol=1e-5, restart=50, maxit_inner=40)
+    lane = vb.Lane(op, pcb, side=side, tol=1e-5, restart=50, maxit_inner=40)
     queue = list(range(len(lams)))
     inflight, out = {}, {}
     while queue or inflight:
@@ -140,7 +144,7 @@ def test_lane_refills_members_and_matches_solo_solves(family):
     assert sorted(out) == list(range(len(lams)))
     for i, l in enumerate(lams):
         x, info = out[i]
-        xs, is_ = _solo(p, idx, Gs, nodes, pc, l, rhs(geo.C0 / l * geo.N_EXT))
+        xs, is_ = _solo(p, idx, Gs, nodes, pc, l, rhs(geo.C0 / l * geo.N_EXT), side=side)
         assert info["flag"] == 0 and info["relres"] <= 1e-5
         assert info["iters"] == is_["iters"] and info["refinements"] == is_["refinements"]
         assert np.array_equal(x, xs)

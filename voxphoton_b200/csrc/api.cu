@@ -248,13 +248,14 @@ constexpr size_t kGmresHdr = (offsetof(GmresDev, sn) + 15) / 16 * 16;
 
 // GMRES workspace for one precision and restart length, for every member of
 // the operator.  Member b's vectors form one arena, vs elements after member
-// 0's: [V (m+1 columns) | w | t | r | x | b], each column ldv elements long.
+// 0's: [V (m+1 columns) | w | t | r | x | b | c], each column ldv elements long
+// (c: the column the next out-of-phase step multiplies, step mode).
 template <typename R>
 struct GmresWork {
   int m = 0;
   int K = 0;
   long long ldv = 0;        // column length (n rounded up to 32)
-  long long vs = 0;         // member stride = (m + 6) * ldv
+  long long vs = 0;         // member stride = (m + 7) * ldv
   Cx<R>* arena = nullptr;
   Cx<R>* V = nullptr;       // member 0's pointers into the arena
   Cx<R>* w = nullptr;
@@ -262,11 +263,13 @@ struct GmresWork {
   Cx<R>* r = nullptr;
   Cx<R>* x = nullptr;
   Cx<R>* b = nullptr;
+  Cx<R>* c = nullptr;       // step mode: each member's current basis column
   GmresDev* st = nullptr;   // K records
   unsigned char* hst = nullptr;  // pinned: K headers of kGmresHdr bytes
   int* hflag = nullptr;          // pinned: K frozen flags
   double* hscal = nullptr;       // pinned: K scalars
-  // (precond, side, members launched) -> captured cycle
+  // (precond, side, members launched [+ 1000 x steps in step mode]) -> captured
+  // cycle or step sequence
   std::map<std::tuple<void*, int, int>, cudaGraphExec_t> graphs;
   GmresDev* hdr(int mb) { return reinterpret_cast<GmresDev*>(hst + (size_t)mb * kGmresHdr); }
   template <typename T> T* mem(T* p, int mb) const { return p + mb * vs; }
@@ -278,7 +281,7 @@ struct GmresWork {
     if (hst) cudaFreeHost(hst);
     if (hflag) cudaFreeHost(hflag);
     if (hscal) cudaFreeHost(hscal);
-    arena = V = w = t = r = x = b = nullptr;
+    arena = V = w = t = r = x = b = c = nullptr;
     st = nullptr;
     hst = nullptr;
     hflag = nullptr;

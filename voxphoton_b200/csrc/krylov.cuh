@@ -27,6 +27,7 @@ namespace vox {
 constexpr int kMaxRestart = 128;
 constexpr int kRedBlocks = 592;  // 4 CTAs per SM on 148 SMs
 constexpr int kRedThreads = 256;
+constexpr int kHist = 2048;       // residual history kept on the device per inner solve
 
 struct GmresDev {
   int done;          // cycle finished (converged / breakdown / m reached)
@@ -36,6 +37,20 @@ struct GmresDev {
   unsigned ticket;   // last-block counter
   int m;             // restart length
   int frozen;        // member takes no part in this cycle (batched launches)
+  // step mode (lanes): members advance one Arnoldi step per launch sequence,
+  // each at its own k, and restart on their own (k_step_begin / k_step_end)
+  int start;         // begin a cycle at the next step (r holds its residual)
+  int stepped;       // this member took the current step (set by gs_column)
+  int endnow;        // its cycle ended in the current step
+  int noend;         // !endnow (skip flag of the end-of-cycle launches)
+  int ifin;          // its inner solve ended (converged, breakdown or maxit cycles)
+  int cycles;        // cycles of the current inner solve
+  int maxit;         // cycle limit of the inner solve
+  int nhist;         // entries of hist
+  int itot;          // iterations of the current inner solve
+  int kdone;         // iterations of its last cycle
+  double ibn;        // the inner right-hand side's norm (relative residuals)
+  double itol;       // relative target of the inner solve
   double tol_abs;    // tol * bnorm
   double beta;       // ||r|| at cycle start
   double inv_norm;   // 1/H(k+1,k) for the pending basis vector
@@ -51,6 +66,7 @@ struct GmresDev {
   double2 Rm[(kMaxRestart + 1) * kMaxRestart];  // rotated (upper triangular part used)
   double2 partial[(kMaxRestart + 1) * kRedBlocks];
   double scal[4];    // misc reductions (norms)
+  double hist[kHist];  // step mode: the LS residuals of every cycle of the inner solve
 };
 
 __device__ __forceinline__ double2 warp_sum(double2 v) {
@@ -371,7 +387,12 @@ __device__ __forceinline__ void gs_column(GmresDev* st, int k, double nrm) {
   st->inv_norm = (nrm > 0.0) ? 1.0 / nrm : 0.0;
   if (resid < st->tol_abs) st->converged = 1;
   if (nrm == 0.0) st->breakdown = 1;
-  if (st->converged || st->breakdown || k + 1 >= m) st->done = 1;
+  st->stepped = 1;
+  if (st->converged || st->breakdown || k + 1 >= m) {
+    st->done = 1;
+    st->endnow = 1;
+    st->noend = 0;
+  }
 }
 
 // w <- w - V h2 ; ||w||^2 ; last block: Hessenberg column, Givens, residual.
@@ -419,7 +440,8 @@ __global__ void k_gs_scale(GmresDev* st, int k, Cx<R>* __restrict__ Vnext,
 }
 
 // ||x||^2 -> st->scal[slot] (deterministic, grid = (kRedBlocks, members));
-// with `in_cycle` a frozen member is skipped.
+// with in_cycle == 1 a frozen member is skipped, with in_cycle == 2 every
+// member that does not start a cycle at this step (step mode).
 template <typename R>
 __global__ void __launch_bounds__(kRedThreads) k_norm2(GmresDev* st, const Cx<R>* __restrict__ x,
                                                        long long n, int slot, long long vs,
@@ -427,7 +449,8 @@ __global__ void __launch_bounds__(kRedThreads) k_norm2(GmresDev* st, const Cx<R>
   __shared__ double2 sh[32];
   st += blockIdx.y;
   x += blockIdx.y * vs;
-  if (in_cycle && st->frozen) return;
+  if (in_cycle == 1 && st->frozen) return;
+  if (in_cycle == 2 && !st->start) return;  // step mode: members starting a cycle
   double2 acc = make_double2(0.0, 0.0);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -447,10 +470,12 @@ __global__ void __launch_bounds__(kRedThreads) k_norm2(GmresDev* st, const Cx<R>
 }
 
 // Start a cycle: beta = sqrt(scal[0]); V(:,0) = r / beta; g = beta e1.
-// A frozen member ends its cycle before it starts (done, k = 0).
-__global__ void k_cycle_init(GmresDev* st) {
+// A frozen member ends its cycle before it starts (done, k = 0).  In step mode
+// (step != 0) only the members flagged to start a cycle take part.
+__global__ void k_cycle_init(GmresDev* st, int step) {
   st += blockIdx.y;
-  if (st->frozen) {
+  if (step && !st->start) return;
+  if (!step && st->frozen) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
       st->done = 1;
       st->k = 0;
@@ -469,25 +494,30 @@ __global__ void k_cycle_init(GmresDev* st) {
   }
 }
 
+// V(:,0) = r / beta; in step mode also into vcur, the column the next step
+// multiplies (the Arnoldi input of every member at its own k).
 template <typename R>
 __global__ void k_cycle_v0(const GmresDev* st, Cx<R>* __restrict__ V0, const Cx<R>* __restrict__ r,
-                           long long n, long long vs) {
+                           long long n, long long vs, Cx<R>* vcur, int step) {
   st += blockIdx.y;
   V0 += blockIdx.y * vs;
   r += blockIdx.y * vs;
-  if (st->frozen) return;
+  if (step ? !st->start : st->frozen) return;
+  if (vcur) vcur += blockIdx.y * vs;
   const R s = (R)st->inv_norm;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    V0[i] = cscale(r[i], s);
+    const Cx<R> v = cscale(r[i], s);
+    V0[i] = v;
+    if (vcur) vcur[i] = v;
   }
 }
 
 // Least squares after the cycle: y = Rm(0:kk-1,0:kk-1) \ g(0:kk-1) (back
 // substitution), res = beta e1 - H(0:kk,0:kk-1) y  (pgmres_iter.m:117-119).
-__global__ void k_cycle_ls(GmresDev* st) {
+__global__ void k_cycle_ls(GmresDev* st, int step) {
   st += blockIdx.y;
-  if (threadIdx.x != 0 || blockIdx.x != 0 || st->frozen) return;
+  if (threadIdx.x != 0 || blockIdx.x != 0 || (step ? !st->endnow : st->frozen)) return;
   const int kk = st->k;
   const int ld = st->m + 1;
   for (int i = kk - 1; i >= 0; i--) {
@@ -518,14 +548,14 @@ __global__ void k_cycle_ls(GmresDev* st) {
 // x += V(:,0:kk-1) y ; r = V(:,0:kk) res   (pgmres_iter.m:133-150, no right preconditioner)
 template <typename R>
 __global__ void k_cycle_update(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
-                               Cx<R>* x, Cx<R>* r, long long n, long long vs) {
+                               Cx<R>* x, Cx<R>* r, long long n, long long vs, int step) {
   __shared__ Cx<R> ys[kMaxRestart];
   __shared__ Cx<R> rs[kMaxRestart + 1];
   st += blockIdx.y;
   V += blockIdx.y * vs;
   if (x) x += blockIdx.y * vs;
   r += blockIdx.y * vs;
-  if (st->frozen) return;
+  if (step ? !st->endnow : st->frozen) return;
   const int kk = st->k;
   for (int j = threadIdx.x; j <= kk; j += blockDim.x) {
     if (j < kk) ys[j] = from_d2<Cx<R>>(st->y[j]);
@@ -549,12 +579,12 @@ __global__ void k_cycle_update(const GmresDev* st, const Cx<R>* __restrict__ V, 
 // y = V(:,0:kk-1) * ys (for the right-preconditioned update, into a temp)
 template <typename R>
 __global__ void k_cycle_vy(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
-                           Cx<R>* out, long long n, long long vs) {
+                           Cx<R>* out, long long n, long long vs, int step) {
   __shared__ Cx<R> ys[kMaxRestart];
   st += blockIdx.y;
   V += blockIdx.y * vs;
   out += blockIdx.y * vs;
-  if (st->frozen) return;
+  if (step ? !st->endnow : st->frozen) return;
   const int kk = st->k;
   for (int j = threadIdx.x; j < kk; j += blockDim.x) ys[j] = from_d2<Cx<R>>(st->y[j]);
   __syncthreads();
@@ -569,11 +599,11 @@ __global__ void k_cycle_vy(const GmresDev* st, const Cx<R>* __restrict__ V, long
 // elementwise helpers
 template <typename R>
 __global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x, long long n,
-                       long long vs) {
+                       long long vs, int step) {
   st += blockIdx.y;
   y += blockIdx.y * vs;
   x += blockIdx.y * vs;
-  if (st->frozen) return;
+  if (step ? !st->endnow : st->frozen) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     y[i] = cadd(y[i], x[i]);
@@ -609,18 +639,18 @@ constexpr size_t kGsSmemBudget = 220 * 1024;
 // Rows per chunk: each column segment of a chunk is one bulk copy, 4 KB when
 // two stages of such chunks fit the budget, else 2 KB (long bases).
 template <typename R>
-inline int gs_rows(int nj) {
+__host__ __device__ inline int gs_rows(int nj) {
   const int r4 = 4096 / (int)sizeof(Cx<R>);
   return 2ull * (nj + 1) * r4 * sizeof(Cx<R>) <= kGsSmemBudget ? r4 : r4 / 2;
 }
 template <typename R>
-inline int gs_stages(int nj) {
+__host__ __device__ inline int gs_stages(int nj) {
   const size_t st = ((size_t)nj + 1) * gs_rows<R>(nj) * sizeof(Cx<R>);
   const size_t s = kGsSmemBudget / st;
   return (int)(s < 2 ? 2 : (s > kGsMaxStages ? kGsMaxStages : s));
 }
 template <typename R>
-inline size_t gs_pass_smem(int nj) {
+__host__ __device__ inline size_t gs_pass_smem(int nj) {
   return (size_t)gs_stages<R>(nj) * ((size_t)nj + 1) * gs_rows<R>(nj) * sizeof(Cx<R>);
 }
 
@@ -628,6 +658,9 @@ __device__ __forceinline__ void consumer_bar() {
   asm volatile("bar.sync 1, %0;" ::"n"(kGsConsumers) : "memory");
 }
 
+// k < 0 (step mode): each member's own basis size k = st->k, and the ring's
+// stage count and chunk rows from it as the host computes them (the launch
+// then carries the largest shared-memory size of its restart length).
 template <typename R, bool kUpdate>
 __global__ void __launch_bounds__(kGsThreads, 1) k_gs_pass(GmresDev* st, int k,
                                                            const Cx<R>* __restrict__ V,
@@ -644,6 +677,13 @@ __global__ void __launch_bounds__(kGsThreads, 1) k_gs_pass(GmresDev* st, int k,
   V += blockIdx.y * vs;
   w += blockIdx.y * vs;
   if (st->done || kernel_err_set()) return;
+  if (k < 0) {
+    // read before any CTA of this launch can finish: the last CTA (which
+    // advances st->k in gs_column) arrives only after every CTA has started
+    k = st->k;
+    stages = gs_stages<R>(k + 1);
+    RW = gs_rows<R>(k + 1);
+  }
   const int nj = k + 1;
   const size_t stage = ((size_t)nj + 1) * RW;  // elements of one stage
   C* buf = reinterpret_cast<C*>(smem_raw);
@@ -797,20 +837,30 @@ __global__ void __launch_bounds__(kGsThreads, 1) k_gs_pass(GmresDev* st, int k,
 }
 
 // V(:,k+1) = (w' - V h2) * inv_norm, for the step that just completed (also
-// when it ended the cycle: the restart residual needs that column).
+// when it ended the cycle: the restart residual needs that column).  k < 0
+// (step mode): every member that took this step, at its own k, Vnext = V and
+// the column also goes to vcur (the next step's input).
 template <typename R>
 __global__ void __launch_bounds__(kRedThreads) k_gs_finish(GmresDev* st, int k,
                                                            const Cx<R>* __restrict__ V,
                                                            long long ldv, const Cx<R>* w,
                                                            Cx<R>* __restrict__ Vnext,
-                                                           long long n, long long vs) {
+                                                           long long n, long long vs,
+                                                           Cx<R>* __restrict__ vcur) {
   using C = Cx<R>;
   __shared__ C hs[kGsMaxCols];
   st += blockIdx.y;
   V += blockIdx.y * vs;
   w += blockIdx.y * vs;
   Vnext += blockIdx.y * vs;
-  if (st->frozen || st->k != k + 1) return;
+  if (k < 0) {
+    if (!st->stepped) return;
+    k = st->k - 1;
+    Vnext += (long long)(k + 1) * ldv;
+  } else if (st->frozen || st->k != k + 1) {
+    return;
+  }
+  if (vcur) vcur += blockIdx.y * vs;
   const int nj = k + 1;
   for (int j = threadIdx.x; j < nj; j += blockDim.x) hs[j] = from_d2<C>(st->h2[j]);
   __syncthreads();
@@ -825,7 +875,53 @@ __global__ void __launch_bounds__(kRedThreads) k_gs_finish(GmresDev* st, int k,
       wi.x -= v.x * h.x - v.y * h.y;
       wi.y -= v.x * h.y + v.y * h.x;
     }
-    Vnext[i] = cscale(wi, s);
+    const C o = cscale(wi, s);
+    Vnext[i] = o;
+    if (vcur) vcur[i] = o;
+  }
+}
+
+// ------------------------------------------------------------ step mode
+// A lane runs its members' restart cycles out of phase: a launch sequence
+// takes one Arnoldi step of every member in a cycle, each at its own k, a
+// member whose cycle ended runs its least-squares update in the same
+// sequence, and a member restarts (or begins a new inner solve) at the next
+// step without waiting for the others.  These two kernels (one thread per
+// member) bracket a step; the arithmetic of every member is that of the
+// in-phase cycle.
+
+// After the cycle-start launches: clear the per-step flags.
+__global__ void k_step_begin(GmresDev* st, int km) {
+  const int b = threadIdx.x;
+  if (b >= km) return;
+  GmresDev* s = st + b;
+  s->start = 0;
+  s->stepped = 0;
+  s->endnow = 0;
+  s->noend = 1;
+}
+
+// After the end-of-cycle launches: a member whose cycle ended either stops
+// its inner solve (converged, exact breakdown or its cycle limit: the stopping
+// test of the in-phase driver, on the same numbers) or restarts at the next
+// step.  The cycle's residuals are appended to hist.
+__global__ void k_step_end(GmresDev* st, int km) {
+  const int b = threadIdx.x;
+  if (b >= km) return;
+  GmresDev* s = st + b;
+  if (!s->endnow) return;
+  const int p = s->k;
+  s->cycles += 1;
+  s->itot += p;
+  s->kdone = p;
+  for (int i = 0; i < p && s->nhist < kHist; i++) s->hist[s->nhist++] = s->resvec[i];
+  const double ri = p > 0 ? s->resvec[p - 1] / s->ibn : 1.0;
+  const bool stop = !(ri > s->itol && s->cycles < s->maxit) || (s->breakdown && !s->converged);
+  if (stop) {
+    s->ifin = 1;
+    s->frozen = 1;
+  } else {
+    s->start = 1;
   }
 }
 

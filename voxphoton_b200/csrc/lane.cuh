@@ -2,16 +2,23 @@
 //
 // A lane owns the K members of a batched operator.  Each member runs the
 // solve of vox_solve_refined for its own right-hand side: complex64 GMRES
-// restart cycles inside FP64 iterative refinement.  All members' cycles run
-// as one captured graph (one launch per kernel for every member, the
-// preconditioner's blocks read once for all of them); a member that is not in
-// an inner solve is frozen and skipped.  Between cycles the host advances
-// each member on its own: a member whose inner solve ended gets its FP64
-// refinement step, a member whose solve ended is reported, and a free member
-// can take a new right-hand side at once, so the GPU never waits for the
-// slowest solve of a batch.  Each member's arithmetic is exactly that of the
-// single-right-hand-side solve on the same operator.  Included at the end of
-// api.cu, after solver.cuh.
+// restart cycles inside FP64 iterative refinement.  All members' Arnoldi
+// steps run as one captured graph (one launch per kernel for every member,
+// the preconditioner's blocks read once for all of them); a member that is
+// not in an inner solve is frozen and skipped.
+//
+// Step mode (restart + 1 <= kGsMaxCols, the default): the members' cycles
+// are out of phase.  One vox_lane_step runs a fixed number of steps (one
+// Arnoldi step of every member in a cycle, each at its own k); a member whose
+// cycle ends restarts at the next step by itself, and a member whose inner
+// solve ends waits only until the end of the current steps, not for the
+// other members' cycles.  In-phase mode (longer restarts) runs whole cycles.
+// Between launches the host advances each member on its own: a member whose
+// inner solve ended gets its FP64 refinement step, a member whose solve ended
+// is reported, and a free member can take a new right-hand side at once.
+// Each member's arithmetic is exactly that of the single-right-hand-side
+// solve on the same operator.  Included at the end of api.cu, after
+// solver.cuh.
 #pragma once
 
 struct vox_lane_s {
@@ -23,6 +30,8 @@ struct vox_lane_s {
   int maxit_inner = 40;
   double inner_tol = 0.0;
   int max_refine = 10;
+  int steps = 0;               // step mode: steps per vox_lane_step (0: in-phase cycles)
+  double* hhist = nullptr;     // pinned: K residual histories (step mode)
   struct Member {
     int state = 0;             // 0 free, 1 solving, 2 finished (not yet collected)
     const double2* b = nullptr;
@@ -41,18 +50,44 @@ struct vox_lane_s {
   };
   std::vector<Member> m;
   std::vector<int> pending_done;  // finished at submission (zero right-hand side)
+  ~vox_lane_s() {
+    if (hhist) cudaFreeHost(hhist);
+  }
 };
 
 namespace vox {
 
+// Steps per vox_lane_step in step mode: VOX_LANE_STEPS (1..64; 0 runs whole
+// in-phase cycles instead), default 2.
+static int lane_steps_default() {
+  const char* e = std::getenv("VOX_LANE_STEPS");
+  if (e && *e) {
+    const int v = std::atoi(e);
+    if (v >= 0 && v <= 64) return v;
+  }
+  return 2;
+}
+
 // One member's header: zeroed solve state, restart length, tolerance, frozen.
-static vox_status lane_header(vox_lane_s* L, int b, double tol_abs, int frozen) {
+// A member that begins an inner solve in step mode is flagged to start its
+// first cycle at the next step, with the inner solve's stopping data (its
+// right-hand side's norm, relative target and cycle limit).
+static vox_status lane_header(vox_lane_s* L, int b, double tol_abs, int frozen, double ibn = 0.0,
+                              double itol = 0.0) {
   GmresWork<float>& w = L->op->wf;
   std::vector<unsigned char> hdr(offsetof(GmresDev, resvec), 0);
   GmresDev* h = reinterpret_cast<GmresDev*>(hdr.data());
   h->m = w.m;
   h->tol_abs = tol_abs;
   h->frozen = frozen;
+  h->noend = 1;
+  h->ibn = ibn;
+  h->itol = itol;
+  h->maxit = L->maxit_inner;
+  if (L->steps > 0) {
+    h->start = frozen ? 0 : 1;
+    h->done = 1;  // until its cycle starts (idle members never step)
+  }
   VOX_CUDA(cudaMemcpyAsync(&w.st[b], hdr.data(), hdr.size(), cudaMemcpyHostToDevice,
                            L->op->stream));
   return VOX_OK;
@@ -123,7 +158,7 @@ static vox_status lane_start_inner(vox_lane_s* L, const std::vector<int>& S) {
     }
     mb.rv.push_back(1.0);
     mb.inner = true;
-    VOX_TRY(lane_header(L, b, mb.itol * mb.ibn, 0));
+    VOX_TRY(lane_header(L, b, mb.itol * mb.ibn, 0, mb.ibn, mb.itol));
   }
   return VOX_OK;
 }
@@ -226,7 +261,47 @@ static vox_status lane_step(vox_lane_s* L, int* done, int* n_done) {
   std::vector<int> R;
   bool any = false;
   for (int b = 0; b < K; b++) any = any || (L->m[b].state == 1 && L->m[b].inner);
-  if (any) {
+  if (any && L->steps > 0) {
+    // out-of-phase steps; the device restarts cycles and ends inner solves
+    if (use_cycle_graphs()) {
+      cudaGraphExec_t g = nullptr;
+      VOX_TRY(get_step_graph<float>(op, L->pc, L->side, K, L->steps, &g));
+      VOX_CUDA(cudaGraphLaunch(g, st));
+      op->launches += op->graph_nodes[g];
+    } else {
+      int nk = 0;
+      VOX_TRY(enqueue_steps<float>(op, L->pc, L->side, K, L->steps, st, &nk));
+      op->launches += nk;
+    }
+    for (int b = 0; b < K; b++)
+      if (L->m[b].state == 1 && L->m[b].inner)
+        VOX_CUDA(cudaMemcpyAsync(wf.hdr(b), &wf.st[b], offsetof(GmresDev, resvec),
+                                 cudaMemcpyDeviceToHost, st));
+    VOX_TRY(wait_stream(st));
+    std::vector<int> fin_inner;
+    for (int b = 0; b < K; b++) {
+      vox_lane_s::Member& mb = L->m[b];
+      if (mb.state != 1 || !mb.inner || !wf.hdr(b)->ifin) continue;
+      fin_inner.push_back(b);
+      const int nh = std::min(wf.hdr(b)->nhist, kHist);
+      if (nh > 0)
+        VOX_CUDA(cudaMemcpyAsync(L->hhist + (size_t)b * kHist, wf.st[b].hist, nh * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+    }
+    if (!fin_inner.empty()) VOX_TRY(wait_stream(st));
+    for (int b : fin_inner) {
+      vox_lane_s::Member& mb = L->m[b];
+      const GmresDev* hb = wf.hdr(b);
+      const int nh = std::min(hb->nhist, kHist);
+      for (int i = 0; i < nh; i++) mb.rv.push_back(L->hhist[(size_t)b * kHist + i] / mb.ibn);
+      mb.info.total_iters += hb->itot;
+      mb.outit = hb->cycles;
+      mb.outer_total += hb->cycles;
+      mb.p = hb->kdone;
+      mb.inner = false;
+      R.push_back(b);
+    }
+  } else if (any) {
     if (use_cycle_graphs()) {
       cudaGraphExec_t cyc = nullptr;
       VOX_TRY(get_cycle_graph<float>(op, L->pc, L->side, K, &cyc));
@@ -311,13 +386,19 @@ vox_status vox_lane_create(vox_op_t op, vox_precond_t pc, int side, double tol, 
   L->maxit_inner = maxit_inner;
   L->inner_tol = inner_tol;
   L->max_refine = max_refine < 1 ? 10 : max_refine;
+  L->steps = step_mode_ok(op->wf) ? lane_steps_default() : 0;
+  if (L->steps > 0)
+    VOX_CUDA(cudaMallocHost((void**)&L->hhist, (size_t)op->K * kHist * sizeof(double)));
   L->m.resize(op->K);
   // every member frozen until it takes a right-hand side
   for (int b = 0; b < op->K; b++) VOX_TRY(lane_header(L.get(), b, 0.0, 1));
   VOX_TRY(wait_stream(op->stream));
   if (use_cycle_graphs()) {
     cudaGraphExec_t cyc = nullptr;
-    VOX_TRY(get_cycle_graph<float>(op, pc, L->side, op->K, &cyc));
+    if (L->steps > 0)
+      VOX_TRY(get_step_graph<float>(op, pc, L->side, op->K, L->steps, &cyc));
+    else
+      VOX_TRY(get_cycle_graph<float>(op, pc, L->side, op->K, &cyc));
   }
   op->lanes.push_back(L.get());
   *out = L.release();

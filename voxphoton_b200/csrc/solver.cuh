@@ -830,7 +830,7 @@ static vox_status ensure_work(vox_op_s* op, int m) {
   const int K = op->K;
   w.K = K;
   w.ldv = (n + 31) / 32 * 32;
-  w.vs = (long long)(m + 6) * w.ldv;
+  w.vs = (long long)(m + 7) * w.ldv;
   VOX_TRY(dalloc(&w.arena, w.vs * K));
   w.V = w.arena;
   w.w = w.V + (long long)(m + 1) * w.ldv;
@@ -838,6 +838,7 @@ static vox_status ensure_work(vox_op_s* op, int m) {
   w.r = w.t + w.ldv;
   w.x = w.r + w.ldv;
   w.b = w.x + w.ldv;
+  w.c = w.b + w.ldv;
   VOX_TRY(dalloc(&w.st, K));
   VOX_CUDA(cudaMemsetAsync(w.st, 0, K * sizeof(GmresDev), op->stream));
   VOX_CUDA(cudaMallocHost((void**)&w.hst, K * kGmresHdr));
@@ -872,8 +873,8 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
   const dim3 gr(kRedBlocks, km), ge(nblk(n), km), g1(1, km);
   const bool right = side == VOX_PREC_RIGHT && pc, left = side == VOX_PREC_LEFT && pc;
   k_norm2<R><<<gr, kRedThreads, 0, st>>>(d, w.r, n, 0, w.vs, 1);
-  k_cycle_init<<<g1, 32, 0, st>>>(d);
-  k_cycle_v0<R><<<ge, 256, 0, st>>>(d, w.V, w.r, n, w.vs);
+  k_cycle_init<<<g1, 32, 0, st>>>(d, 0);
+  k_cycle_v0<R><<<ge, 256, 0, st>>>(d, w.V, w.r, n, w.vs, (Cx<R>*)nullptr, 0);
   *nk += 3;
   for (int k = 0; k < m; k++) {
     Cx<R>* vk = w.V + (long long)k * ld;
@@ -896,7 +897,8 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
       k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns, rw);
       k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(d, k, w.V, ld, wv, n, w.vs, ns, rw);
       k_gs_finish<R><<<ge, kRedThreads, 0, st>>>(d, k, w.V, ld, wv,
-                                                 w.V + (long long)(k + 1) * ld, n, w.vs);
+                                                 w.V + (long long)(k + 1) * ld, n, w.vs,
+                                                 (Cx<R>*)nullptr);
       *nk += 3 + ((right || left) ? 3 : 0) + 3;
     } else {
       k_gs_dots<R><<<gr, kRedThreads, 0, st>>>(d, k, w.V, ld, wv, n, w.vs);
@@ -906,18 +908,123 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
       *nk += 3 + ((right || left) ? 3 : 0) + 4;
     }
   }
-  k_cycle_ls<<<g1, 32, 0, st>>>(d);
+  k_cycle_ls<<<g1, 32, 0, st>>>(d, 0);
   if (right) {
-    k_cycle_vy<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.w, n, w.vs);
+    k_cycle_vy<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.w, n, w.vs, 0);
     VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, frozen, mm));
-    k_axpy<R><<<ge, 256, 0, st>>>(d, w.x, w.t, n, w.vs);
-    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, (Cx<R>*)nullptr, w.r, n, w.vs);
+    k_axpy<R><<<ge, 256, 0, st>>>(d, w.x, w.t, n, w.vs, 0);
+    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, (Cx<R>*)nullptr, w.r, n, w.vs, 0);
     *nk += 7;
   } else {
-    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs);
+    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs, 0);
     *nk += 2;
   }
   VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
+// Step mode needs the two-read Gram-Schmidt (restart + 1 <= kGsMaxCols).
+template <typename R>
+static bool step_mode_ok(const GmresWork<R>& w) {
+  return w.m >= 1 && w.m + 1 <= kGsMaxCols;
+}
+
+// Enqueue `steps` out-of-phase steps (step mode) for members 0..km-1: per
+// step the cycle start of every member flagged to start (k_norm2, k_cycle_init,
+// k_cycle_v0 into V(:,0) and vcur), one Arnoldi step of every member in a
+// cycle at its own k (the matvec and preconditioner read vcur; the
+// Gram-Schmidt passes take k from the member's record), the end-of-cycle
+// update of every member whose cycle ended at this step, and k_step_end.
+template <typename R>
+static vox_status enqueue_steps(vox_op_s* op, vox_precond_s* pc, int side, int km, int steps,
+                                cudaStream_t st, int* nk) {
+  GmresWork<R>& w = work<R>(op);
+  if (!step_mode_ok(w)) {
+    set_error("step mode needs restart + 1 <= " + std::to_string(kGsMaxCols));
+    return VOX_ERR_UNSUPPORTED;
+  }
+  const long long n = op->g.n;
+  const long long ld = w.ldv;
+  const int m = w.m;
+  GmresDev* d = w.st;
+  const int* skip = &d->done;
+  const int* noend = &d->noend;
+  const Members mm = wmembers(w, km);
+  const dim3 gr(kRedBlocks, km), ge(nblk(n), km), g1(1, km);
+  const bool right = side == VOX_PREC_RIGHT && pc, left = side == VOX_PREC_LEFT && pc;
+  size_t sm = 0;
+  for (int nj = 1; nj <= m; nj++) sm = std::max(sm, gs_pass_smem<R>(nj));
+  const dim3 gp(kGsBlocks, km);
+  for (int s = 0; s < steps; s++) {
+    k_norm2<R><<<gr, kRedThreads, 0, st>>>(d, w.r, n, 0, w.vs, 2);
+    k_cycle_init<<<g1, 32, 0, st>>>(d, 1);
+    k_cycle_v0<R><<<ge, 256, 0, st>>>(d, w.V, w.r, n, w.vs, w.c, 1);
+    k_step_begin<<<1, 32, 0, st>>>(d, km);
+    const Cx<R>* src = w.c;
+    if (right) {
+      VOX_TRY(pc_apply<R>(pc, w.c, w.t, st, skip, mm));
+      src = w.t;
+    }
+    VOX_TRY(matvec<R>(op, MV_AN, src, w.w, st, skip, mm));
+    Cx<R>* wv = w.w;
+    if (left) {
+      VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, skip, mm));
+      wv = w.t;
+    }
+    k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(d, -1, w.V, ld, wv, n, w.vs, 0, 0);
+    k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(d, -1, w.V, ld, wv, n, w.vs, 0, 0);
+    k_gs_finish<R><<<ge, kRedThreads, 0, st>>>(d, -1, w.V, ld, wv, w.V, n, w.vs, w.c);
+    k_cycle_ls<<<g1, 32, 0, st>>>(d, 1);
+    if (right) {
+      k_cycle_vy<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.w, n, w.vs, 1);
+      VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, noend, mm));
+      k_axpy<R><<<ge, 256, 0, st>>>(d, w.x, w.t, n, w.vs, 1);
+      k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, (Cx<R>*)nullptr, w.r, n, w.vs, 1);
+      *nk += 7;
+    } else {
+      k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs, 1);
+      *nk += 2;
+    }
+    k_step_end<<<1, 32, 0, st>>>(d, km);
+    *nk += 4 + 3 + ((right || left) ? 3 : 0) + 3 + 1;
+  }
+  VOX_CUDA(cudaGetLastError());
+  return VOX_OK;
+}
+
+template <typename R>
+static vox_status get_step_graph(vox_op_s* op, vox_precond_s* pc, int side, int km, int steps,
+                                 cudaGraphExec_t* out) {
+  GmresWork<R>& w = work<R>(op);
+  auto key = std::make_tuple((void*)pc, side, km + 1000 * steps);
+  auto it = w.graphs.find(key);
+  if (it != w.graphs.end()) {
+    *out = it->second;
+    return VOX_OK;
+  }
+  cudaStream_t st = op->stream;
+  cudaGraph_t graph;
+  int nk = 0;
+  VOX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  vox_status s = enqueue_steps<R>(op, pc, side, km, steps, st, &nk);
+  cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (s != VOX_OK) return s;
+  if (e != cudaSuccess) {
+    set_error(std::string("graph capture: ") + cudaGetErrorString(e));
+    return VOX_ERR_CUDA;
+  }
+  size_t nnodes = 0;
+  cudaGraphGetNodes(graph, nullptr, &nnodes);
+  cudaGraphExec_t exec;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    set_error(std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return VOX_ERR_CUDA;
+  }
+  op->graph_nodes[exec] = (int)nnodes;
+  w.graphs[key] = exec;
+  *out = exec;
   return VOX_OK;
 }
 
@@ -1567,7 +1674,7 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
     clear();
     out[8] = timeit([&] {
       k_gs_finish<R><<<dim3(nb, km), kRedThreads, 0, st>>>(
-          w.st, k, w.V, ld, w.w, w.V + (long long)(k + 1) * ld, n, w.vs);
+          w.st, k, w.V, ld, w.w, w.V + (long long)(k + 1) * ld, n, w.vs, (Cx<R>*)nullptr);
     });
   } else {
     out[6] = timeit([&] {
