@@ -393,8 +393,12 @@ static void launch_plane(vox_op_s* op, const OpBuffers<R>& b, const Cx<R>* T1, c
     k_zsplit<R><<<gz, 256, zsm, st>>>(g, op->pz, b.twZ, fN, TY, skip, fs);
     k_ysplit_inv<R><<<gy, 256, ysm, st>>>(g, op->py, b.twY, TY, T2, skip, fs);
   } else if (plane64_ok<R>(g)) {
-    k_plane64<R><<<dim3(g.Px, km), kPlThreads, plane64_smem<R>(g.N), st>>>(g, b.twY, b.twZ, T1,
-                                                                          fN, T2, skip, fs);
+    if (sizeof(R) == 4 && g.pl3)
+      k_plane64<R, 3><<<dim3(g.Px, km), kPlThreads, plane64_smem<R>(g.N), st>>>(
+          g, b.twY, b.twZ, T1, fN, T2, skip, fs);
+    else
+      k_plane64<R, 2><<<dim3(g.Px, km), kPlThreads, plane64_smem<R>(g.N), st>>>(
+          g, b.twY, b.twZ, T1, fN, T2, skip, fs);
   } else {
     k_plane<R><<<dim3(g.Px, km), 256, psmem(g, cs), st>>>(g, op->py, op->pz, b.twY, b.twZ, T1,
                                                            fN, T2, skip, fs);
@@ -426,11 +430,11 @@ static vox_status matvec(vox_op_s* op, int mode, const Cx<R>* in, Cx<R>* out, cu
   Cx<R>* T1 = scratch.T1 ? scratch.T1 : b.T1 + mm.m0 * plane_elems(g);
   Cx<R>* T2 = scratch.T2 ? scratch.T2 : b.T2 + mm.m0 * plane_elems(g);
   const Cx<R>* fN = b.fN + mm.m0 * fN_elems(g);
-  k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1, skip,
+  k_xfwd<R><<<gx, g.xthr, xsmem(g, cs), st>>>(g, op->px, b.twX, in, op->vmap, b.Mc, mode, T1, skip,
                                             mm.vs, mm.fs);
   launch_plane<R>(op, b, T1, fN, T2, g.split ? b.TY + mm.m0 * planey_elems(g) : nullptr, mm.km,
                   skip, mm.fs, st);
-  k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
+  k_xinv<R><<<gx, g.xthr, xsmem(g, cs), st>>>(g, op->px, b.twX, T2, op->vmap, in, b.Mr, b.Mc,
                                             b.gram, scale, b.out_scale, mode, out, skip, mm.vs,
                                             mm.fs);
   VOX_CUDA(cudaGetLastError());
@@ -452,7 +456,8 @@ static vox_status set_smem_attrs() {
   VOX_TRY(smem_cap(k_ysplit_fwd<R>));
   VOX_TRY(smem_cap(k_zsplit<R>));
   VOX_TRY(smem_cap(k_ysplit_inv<R>));
-  VOX_TRY(smem_cap(k_plane64<R>));
+  VOX_TRY(smem_cap(k_plane64<R, 2>));
+  VOX_TRY(smem_cap(k_plane64<R, 3>));
   VOX_TRY(smem_cap(k_gs_pass<R, false>));
   VOX_TRY(smem_cap(k_gs_pass<R, true>));
   return VOX_OK;
@@ -475,6 +480,23 @@ static bool pick_shapes(OpGeom& g, size_t csz) {
     yb = 1;
   }
   g.ybx = std::max(1, std::min({yb, 8, g.M}));
+  g.xthr = 256;
+  // complex64 k_plane64 at three CTAs per SM (80 registers, measured 12% faster
+  // than two CTAs of 113 registers on the 1160 x 30 x 11 grating)
+  g.pl3 = csz == sizeof(float2) ? 1 : 0;
+  if (csz == sizeof(float2)) {
+    // tuning overrides (complex64): pencils per x-kernel CTA, its threads, and
+    // the plane kernel's CTAs per SM
+    if (const char* e = std::getenv("VOX_XK_YB")) {
+      const int v = std::atoi(e);
+      if (v >= 1 && v <= 8 && 2ull * v * g.sx * csz <= (size_t)kSmemCap) g.ybx = std::min(v, g.M);
+    }
+    if (const char* e = std::getenv("VOX_XK_THREADS")) {
+      const int v = std::atoi(e);
+      if (v == 256 || v == 512) g.xthr = v;
+    }
+    if (const char* e = std::getenv("VOX_PL_MINB")) g.pl3 = std::atoi(e) != 2;
+  }
   // kernel 2: try all rows and all ky columns, then shrink the chunks
   const int rows = 3 * g.N;
   g.rc = rows;

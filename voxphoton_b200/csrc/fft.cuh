@@ -337,8 +337,10 @@ __device__ __forceinline__ bool big_prime_stage(int R, const C* __restrict__ src
 // kBigPrimes compiles butterflies for the primes 17..37 as well: lengths with
 // such a factor (the preconditioner's x-FFT of length L, e.g. 1160 = 8*5*29 or
 // 1480 = 8*5*37) then avoid the runtime-radix stage.  Kernels whose lengths
-// are 7-smooth leave it off and keep their register budget.
-template <typename C, bool kBigPrimes = false>
+// are 7-smooth leave it off and keep their register budget; kSmooth7 compiles
+// only the radices 2, 3, 4, 5, 7 and 8 (for lengths known to be 7-smooth, such
+// as the matvec's padded lengths), which lowers the kernel's register need.
+template <typename C, bool kBigPrimes = false, bool kSmooth7 = false>
 __device__ C* block_fft(C* bufA, C* bufB, const FftPlan& p, int nseq, int sstride,
                         const C* __restrict__ tw, int sign) {
   C* src = bufA;
@@ -354,13 +356,21 @@ __device__ C* block_fft(C* bufA, C* bufB, const FftPlan& p, int nseq, int sstrid
       case 5: fft_stage<5>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
       case 7: fft_stage<7>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
       case 8: fft_stage<8>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
-      case 11: fft_stage<11>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
-      case 13: fft_stage<13>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr); break;
       default:
-        if constexpr (kBigPrimes) {
-          if (big_prime_stage(R, src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr)) break;
+        if constexpr (!kSmooth7) {
+          if (R == 11) {
+            fft_stage<11>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr);
+            break;
+          }
+          if (R == 13) {
+            fft_stage<13>(src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr);
+            break;
+          }
+          if constexpr (kBigPrimes) {
+            if (big_prime_stage(R, src, dst, p.n, Ns, nseq, sstride, tw, sign, tid, nthr)) break;
+          }
+          fft_stage_generic(src, dst, p.n, R, Ns, nseq, sstride, tw, sign, tid, nthr);
         }
-        fft_stage_generic(src, dst, p.n, R, Ns, nseq, sstride, tw, sign, tid, nthr);
         break;
     }
     __syncthreads();

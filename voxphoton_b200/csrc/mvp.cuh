@@ -9,6 +9,8 @@
 //   fN      : [Px][Py][Pz][6] the six unique tensor components of each padded cell
 // Px, Py, Pz are the padded lengths (>= 2L-1, 2M-1, 2N-1, 7-smooth), chosen at
 // operator creation; the circulant embedding is exact for any such length.
+// Every FFT of the matvec is 7-smooth, so its kernels compile only the
+// radices 2, 3, 4, 5, 7 and 8 (block_fft<C, false, true>).
 //
 // Kernel 1 (k_xfwd):  per (z,c) and a tile of y: gather J pencils along x,
 //                     zero-pad to Px, forward FFT along x, write T1 planes.
@@ -32,6 +34,8 @@ struct OpGeom {
   long long n;    // vector length
   // launch shapes (chosen on the host)
   int ybx;        // pencils per CTA in kernels 1/3
+  int xthr;       // threads per CTA in kernels 1/3 (256 or 512)
+  int pl3;        // complex64 k_plane64 at three CTAs per SM (80 registers)
   int sx;         // smem stride of an x pencil
   int sy, sz;     // smem strides of y rows / z columns in kernel 2
   int rc, kc;     // rows per chunk / ky columns per chunk in kernel 2
@@ -78,7 +82,7 @@ __host__ __device__ inline long long fN_elems(const OpGeom& g) {
 
 // ---------------------------------------------------------------- kernel 1
 template <typename R>
-__global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>* __restrict__ tw,
+__global__ void __launch_bounds__(512) k_xfwd(OpGeom g, FftPlan px, const Cx<R>* __restrict__ tw,
                                               const Cx<R>* __restrict__ in,
                                               const int* __restrict__ vmap,
                                               const Cx<R>* __restrict__ Mc, int mode,
@@ -97,22 +101,26 @@ __global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>*
   const int c = blockIdx.z - 3 * mb;
   const int YB = g.ybx;
   const long long cellbase = (long long)g.L * ((long long)g.M * z);
-  // gather J along x for YB pencils; zero-pad.  Batches of kGather elements
-  // per thread: the index-map loads, then the vector loads, then the stores,
-  // so a thread keeps several dependent global reads in flight.
-  constexpr int kGather = 4;
-  for (int t0 = threadIdx.x; t0 < YB * g.Px; t0 += kGather * blockDim.x) {
+  // zero padding x in [L, Px) of the YB pencils
+  const int npad = g.Px - g.L;
+  for (int t = threadIdx.x; t < YB * npad; t += blockDim.x) {
+    const int yb = t / npad;
+    bufA[(size_t)yb * g.sx + g.L + (t - yb * npad)] = czero<C>();
+  }
+  // gather J along x (x < L) for YB pencils in batches of kGather elements per
+  // thread: the index-map loads, then the vector loads, then the stores, so a
+  // thread keeps its dependent global reads in flight together
+  constexpr int kGather = sizeof(R) == 4 ? 12 : 6;
+  const int tot = YB * g.L;
+  const int* vm = vmap + (long long)c * g.V + cellbase;
+  for (int t0 = threadIdx.x; t0 < tot; t0 += kGather * blockDim.x) {
     int mm[kGather];
-    long long cl[kGather];
 #pragma unroll
     for (int u = 0; u < kGather; u++) {
       const int t = t0 + u * blockDim.x;
-      const int yb = t / g.Px;
-      const int x = t - yb * g.Px;
+      const int yb = t / g.L;
       const int y = y0 + yb;
-      mm[u] = -1;
-      cl[u] = cellbase + (long long)g.L * y + x;
-      if (t < YB * g.Px && x < g.L && y < g.M) mm[u] = vmap[(long long)c * g.V + cl[u]];
+      mm[u] = (t < tot && y < g.M) ? vm[g.L * y + (t - yb * g.L)] : -1;
     }
     C v[kGather];
 #pragma unroll
@@ -120,16 +128,17 @@ __global__ void __launch_bounds__(256) k_xfwd(OpGeom g, FftPlan px, const Cx<R>*
 #pragma unroll
     for (int u = 0; u < kGather; u++) {
       const int t = t0 + u * blockDim.x;
-      if (t >= YB * g.Px) break;
-      const int yb = t / g.Px;
-      const int x = t - yb * g.Px;
+      if (t >= tot) break;
+      const int yb = t / g.L;
+      const int x = t - yb * g.L;
       C w = v[u];
-      if (mode == MV_AN_T && mm[u] >= 0) w = cmul(Mc[cl[u]], cconj(w));  // conj(conj(Mc) .* J)
+      if (mode == MV_AN_T && mm[u] >= 0)
+        w = cmul(Mc[cellbase + (long long)g.L * (y0 + yb) + x], cconj(w));  // conj(conj(Mc) .* J)
       bufA[(size_t)yb * g.sx + x] = w;
     }
   }
   __syncthreads();
-  C* res = block_fft(bufA, bufB, px, YB, g.sx, tw, -1);
+  C* res = block_fft<C, false, true>(bufA, bufB, px, YB, g.sx, tw, -1);
   // write planes: T1[kx][c][z][y]
   const int ny = min(YB, g.M - y0);
   for (int t = threadIdx.x; t < YB * g.Px; t += blockDim.x) {
@@ -178,7 +187,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
       wA[(size_t)r * g.sy + y] = (y < g.M) ? tin[(long long)(r0 + r) * g.M + y] : czero<C>();
     }
     __syncthreads();
-    C* res = block_fft(wA, wB, py, nr, g.sy, tys, -1);
+    C* res = block_fft<C, false, true>(wA, wB, py, nr, g.sy, tys, -1);
     for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
       const int r = t / g.Py;
       const int y = t - r * g.Py;
@@ -205,7 +214,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
           (zz < g.N) ? ybuf[(size_t)(c * g.N + zz) * g.sy + k0 + j] : czero<C>();
     }
     __syncthreads();
-    C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, tzs, -1);
+    C* res = block_fft<C, false, true>(wA, wB, pz, 3 * nk, g.sz, tzs, -1);
     // tensor product (in place in res)
     for (int t = threadIdx.x; t < nk * g.Pz; t += blockDim.x) {
       const int j = t / g.Pz;
@@ -236,7 +245,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
     }
     __syncthreads();
     C* other = (res == wA) ? wB : wA;
-    C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, tzs, +1);
+    C* res2 = block_fft<C, false, true>(res, other, pz, 3 * nk, g.sz, tzs, +1);
     for (int t = threadIdx.x; t < 3 * nk * g.N; t += blockDim.x) {
       const int s = t / g.N;
       const int zz = t - s * g.N;
@@ -256,7 +265,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1)
       wA[(size_t)r * g.sy + y] = ybuf[(size_t)(r0 + r) * g.sy + y];
     }
     __syncthreads();
-    C* res = block_fft(wA, wB, py, nr, g.sy, tys, +1);
+    C* res = block_fft<C, false, true>(wA, wB, py, nr, g.sy, tys, +1);
     for (int t = threadIdx.x; t < nr * g.M; t += blockDim.x) {
       const int r = t / g.M;
       const int y = t - r * g.M;
@@ -297,7 +306,7 @@ __global__ void __launch_bounds__(256) k_ysplit_fwd(OpGeom g, FftPlan py,
     wA[(size_t)r * g.sy + y] = (y < g.M) ? tin[(long long)(r0 + r) * g.M + y] : czero<C>();
   }
   __syncthreads();
-  C* res = block_fft(wA, wB, py, nr, g.sy, tys, -1);
+  C* res = block_fft<C, false, true>(wA, wB, py, nr, g.sy, tys, -1);
   for (int t = threadIdx.x; t < nr * g.Py; t += blockDim.x) {
     const int r = t / g.Py;
     const int y = t - r * g.Py;
@@ -332,7 +341,7 @@ __global__ void __launch_bounds__(256) k_zsplit(OpGeom g, FftPlan pz,
         (zz < g.N) ? ty[(long long)(c * g.N + zz) * g.Py + k0 + j] : czero<C>();
   }
   __syncthreads();
-  C* res = block_fft(wA, wB, pz, 3 * nk, g.sz, tzs, -1);
+  C* res = block_fft<C, false, true>(wA, wB, pz, 3 * nk, g.sz, tzs, -1);
   // tensor product (octant storage: see k_plane)
   const int fx = g.sym && (2 * kx > g.Px);
   const int hy = g.sym ? g.Py / 2 + 1 : g.Py, hz = g.sym ? g.Pz / 2 + 1 : g.Pz;
@@ -366,7 +375,7 @@ __global__ void __launch_bounds__(256) k_zsplit(OpGeom g, FftPlan pz,
   }
   __syncthreads();
   C* other = (res == wA) ? wB : wA;
-  C* res2 = block_fft(res, other, pz, 3 * nk, g.sz, tzs, +1);
+  C* res2 = block_fft<C, false, true>(res, other, pz, 3 * nk, g.sz, tzs, +1);
   for (int t = threadIdx.x; t < 3 * nk * g.N; t += blockDim.x) {
     const int s = t / g.N;
     const int zz = t - s * g.N;
@@ -402,7 +411,7 @@ __global__ void __launch_bounds__(256) k_ysplit_inv(OpGeom g, FftPlan py,
     wA[(size_t)r * g.sy + y] = ty[(long long)(r0 + r) * g.Py + y];
   }
   __syncthreads();
-  C* res = block_fft(wA, wB, py, nr, g.sy, tys, +1);
+  C* res = block_fft<C, false, true>(wA, wB, py, nr, g.sy, tys, +1);
   for (int t = threadIdx.x; t < nr * g.M; t += blockDim.x) {
     const int r = t / g.M;
     const int y = t - r * g.M;
@@ -412,7 +421,7 @@ __global__ void __launch_bounds__(256) k_ysplit_inv(OpGeom g, FftPlan py,
 
 // ---------------------------------------------------------------- kernel 3
 template <typename R>
-__global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>* __restrict__ tw,
+__global__ void __launch_bounds__(512) k_xinv(OpGeom g, FftPlan px, const Cx<R>* __restrict__ tw,
                                               const Cx<R>* __restrict__ T2,
                                               const int* __restrict__ vmap,
                                               const Cx<R>* in, const Cx<R>* __restrict__ Mr,
@@ -435,7 +444,7 @@ __global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>*
   const int ny = min(YB, g.M - y0);
   // the pencils' values of every plane, kLoad loads in flight per thread
   // before their stores
-  constexpr int kLoad = 8;
+  constexpr int kLoad = sizeof(R) == 4 ? 16 : 8;
   const int tot = YB * g.Px;
   for (int t0 = threadIdx.x; t0 < tot; t0 += kLoad * blockDim.x) {
     C v[kLoad];
@@ -455,11 +464,11 @@ __global__ void __launch_bounds__(256) k_xinv(OpGeom g, FftPlan px, const Cx<R>*
     }
   }
   __syncthreads();
-  C* res = block_fft(bufA, bufB, px, YB, g.sx, tw, +1);
+  C* res = block_fft<C, false, true>(bufA, bufB, px, YB, g.sx, tw, +1);
   const long long cellbase = (long long)g.L * ((long long)g.M * z);
   // batches of kScatter elements per thread: index-map loads, then the
   // vector and contrast loads, then the combination and the stores
-  constexpr int kScatter = 4;
+  constexpr int kScatter = sizeof(R) == 4 ? 8 : 4;
   for (int t0 = threadIdx.x; t0 < YB * g.L; t0 += kScatter * blockDim.x) {
     int mm[kScatter];
     long long cl[kScatter];

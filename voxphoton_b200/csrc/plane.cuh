@@ -120,8 +120,8 @@ __device__ __forceinline__ void fft24_regs(const C (&in)[kPlPz], C (&out)[kPlPz]
   }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(kPlThreads, 2)
+template <typename R, int kMinBlocks>
+__global__ void __launch_bounds__(kPlThreads, kMinBlocks)
     k_plane64(OpGeom g, const Cx<R>* __restrict__ twY, const Cx<R>* __restrict__ twZ,
               const Cx<R>* __restrict__ T1, const Cx<R>* __restrict__ fN, Cx<R>* __restrict__ T2,
               const int* skip, int fs) {

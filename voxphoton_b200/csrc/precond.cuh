@@ -91,7 +91,7 @@ __device__ __forceinline__ void st_pair(double2* p, double2 a, double2 b) {
 // Global loads are issued kPcBatch (gathers) or 2 kPcBatch (the transformed
 // lines) per thread before their stores, so each thread keeps several reads in
 // flight.
-constexpr int kPcBatch = 4;
+constexpr int kPcBatch = 6;
 
 template <typename R, bool kBig>
 __global__ void __launch_bounds__(256, kBig && sizeof(R) == 4 ? 2 : 1) k_pc_xfwd(PcGeom g, FftPlan pl, const Cx<R>* __restrict__ tw,

@@ -1597,12 +1597,12 @@ static vox_status profile_stages(vox_op_s* op, vox_precond_s* pc, int restart, i
   dim3 gx((g.M + g.ybx - 1) / g.ybx, g.N, 3 * km);
   const R scale = (R)(1.0 / ((double)g.Px * g.Py * g.Pz));
   out[0] = timeit([&] {
-    k_xfwd<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, w.V, op->vmap, b.Mc, MV_AN, b.T1,
+    k_xfwd<R><<<gx, g.xthr, xsmem(g, cs), st>>>(g, op->px, b.twX, w.V, op->vmap, b.Mc, MV_AN, b.T1,
                                               nullptr, w.vs, 0);
   });
   out[1] = timeit([&] { launch_plane<R>(op, b, b.T1, b.fN, b.T2, b.TY, km, nullptr, 0, st); });
   out[2] = timeit([&] {
-    k_xinv<R><<<gx, 256, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, w.V, b.Mr, b.Mc,
+    k_xinv<R><<<gx, g.xthr, xsmem(g, cs), st>>>(g, op->px, b.twX, b.T2, op->vmap, w.V, b.Mr, b.Mc,
                                               b.gram, scale, b.out_scale, MV_AN, w.w, nullptr,
                                               w.vs, 0);
   });
