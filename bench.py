@@ -61,7 +61,9 @@ def parse():
     ap.add_argument("--sweep-lambdas", type=int, default=201)
     ap.add_argument("--sweep-rate", type=float, default=200.0,
                     help="Poisson arrival rate (requests/s) of the sweep stream")
-    ap.add_argument("--sweep-slots", type=int, default=4, help="lanes per device length")
+    ap.add_argument("--sweep-slots", type=int, default=1,
+                    help="most lanes per device length in the HBM pool (more lanes share "
+                         "the GPU's L2 and measured slower on the sweep)")
     ap.add_argument("--sweep-members", type=int, default=4,
                     help="solves per lane advanced in lockstep (batched operator members)")
     ap.add_argument("--sweep-side", default="right", choices=["left", "right"],
@@ -749,12 +751,10 @@ def run_microdisk(args, world, rank, local):
     clk = clocks.stop() if clocks else {"sm_mhz": None, "sm_max_mhz": None,
                                         "reasons": ["not sampled (--no-clocks)"]}
     dev_s = e0.elapsed_time(e1) / 1e3
-    lane_ops_end = [op for f in fams for op, _ in f.slots]
+    lane_ops_end = [op for op, _ in fam.slots]
     launches = (sum(op.launches() for op in lane_ops_end if op in lane_ops) - l0 +
                 sum(op.launches() for op in lane_ops_end if op not in lane_ops) +
                 10 * len(reqs))
-    pool = srv.pool_summary()
-    pool["peak_bytes"] = srv.pool_peak()
     summ = sv.summarize(res, wall)
     _progress(f"device-resident: {len(reqs)} solves in {dev_s:.2f} s")
     res_h, wall_h = srv.serve(reqs, realtime=False)

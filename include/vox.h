@@ -324,9 +324,15 @@ vox_status vox_lane_submit_device(vox_lane_t lane, int member, const void* b, vo
 /* The same from host buffers (split complex, length n_idx); the solution is
  * returned by vox_lane_collect. */
 vox_status vox_lane_submit(vox_lane_t lane, int member, const double* b_re, const double* b_im);
-/* One restart cycle for every solving member plus their refinement steps;
- * the members that finished are written to done (room for `members`
- * entries), their count to *n_done. */
+/* Advance every solving member, then run the refinement steps of the members
+ * whose inner solve ended; the members that finished are written to done
+ * (room for `members` entries), their count to *n_done.  For restart + 1 <= 51
+ * a call runs VOX_LANE_STEPS (default 2; 0 selects whole cycles) Arnoldi steps
+ * with the members' cycles out of phase: each member restarts on its own and
+ * a member whose inner solve ends waits only for the rest of this call.  For
+ * longer restarts a call runs one restart cycle of every solving member.
+ * Either way each member's result equals the single-member solve bit for
+ * bit. */
 vox_status vox_lane_step(vox_lane_t lane, int* done, int* n_done);
 /* Result of a finished member (x_re/x_im: host copy of the solution for host
  * submissions, or NULL), which then becomes free. */

@@ -268,6 +268,8 @@ struct GmresWork {
   unsigned char* hst = nullptr;  // pinned: K headers of kGmresHdr bytes
   int* hflag = nullptr;          // pinned: K frozen flags
   double* hscal = nullptr;       // pinned: K scalars
+  int* hsel = nullptr;           // pinned: K skip flags (right_finish)
+  int* dsel = nullptr;           // device copy of hsel
   // (precond, side, members launched [+ 1000 x steps in step mode]) -> captured
   // cycle or step sequence
   std::map<std::tuple<void*, int, int>, cudaGraphExec_t> graphs;
@@ -281,11 +283,15 @@ struct GmresWork {
     if (hst) cudaFreeHost(hst);
     if (hflag) cudaFreeHost(hflag);
     if (hscal) cudaFreeHost(hscal);
+    if (hsel) cudaFreeHost(hsel);
+    dfree(dsel);
     arena = V = w = t = r = x = b = c = nullptr;
     st = nullptr;
     hst = nullptr;
     hflag = nullptr;
     hscal = nullptr;
+    hsel = nullptr;
+    dsel = nullptr;
     m = 0;
   }
 };

@@ -42,7 +42,6 @@ struct GmresDev {
   int start;         // begin a cycle at the next step (r holds its residual)
   int stepped;       // this member took the current step (set by gs_column)
   int endnow;        // its cycle ended in the current step
-  int noend;         // !endnow (skip flag of the end-of-cycle launches)
   int ifin;          // its inner solve ended (converged, breakdown or maxit cycles)
   int cycles;        // cycles of the current inner solve
   int maxit;         // cycle limit of the inner solve
@@ -391,7 +390,6 @@ __device__ __forceinline__ void gs_column(GmresDev* st, int k, double nrm) {
   if (st->converged || st->breakdown || k + 1 >= m) {
     st->done = 1;
     st->endnow = 1;
-    st->noend = 0;
   }
 }
 
@@ -898,7 +896,6 @@ __global__ void k_step_begin(GmresDev* st, int km) {
   s->start = 0;
   s->stepped = 0;
   s->endnow = 0;
-  s->noend = 1;
 }
 
 // After the end-of-cycle launches: a member whose cycle ended either stops

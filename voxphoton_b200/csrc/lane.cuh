@@ -80,7 +80,6 @@ static vox_status lane_header(vox_lane_s* L, int b, double tol_abs, int frozen, 
   h->m = w.m;
   h->tol_abs = tol_abs;
   h->frozen = frozen;
-  h->noend = 1;
   h->ibn = ibn;
   h->itol = itol;
   h->maxit = L->maxit_inner;
@@ -341,6 +340,13 @@ static vox_status lane_step(vox_lane_s* L, int* done, int* n_done) {
     if (L->m[b].state == 1 && !L->m[b].inner &&
         std::find(R.begin(), R.end(), b) == R.end())
       R.push_back(b);
+  // right preconditioning: each ended inner solve's x holds u = sum of its
+  // cycles' V y; one apply of M^{-1} for all of them (as the single solve does)
+  if (L->side == VOX_PREC_RIGHT && L->pc && !R.empty()) {
+    std::vector<char> sel(K, 0);
+    for (int b : R) sel[b] = L->m[b].ibn != 0.0;
+    VOX_TRY(right_finish<float>(op, L->pc, K, sel.data(), st));
+  }
   std::vector<int> again;
   VOX_TRY(lane_refine(L, R, &fin, &again));
   VOX_TRY(lane_start_inner(L, again));

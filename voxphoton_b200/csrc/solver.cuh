@@ -844,6 +844,8 @@ static vox_status ensure_work(vox_op_s* op, int m) {
   VOX_CUDA(cudaMallocHost((void**)&w.hst, K * kGmresHdr));
   VOX_CUDA(cudaMallocHost((void**)&w.hflag, K * sizeof(int)));
   VOX_CUDA(cudaMallocHost((void**)&w.hscal, K * sizeof(double)));
+  VOX_CUDA(cudaMallocHost((void**)&w.hsel, K * sizeof(int)));
+  VOX_TRY(dalloc(&w.dsel, K));
   w.m = m;
   return VOX_OK;
 }
@@ -868,7 +870,6 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
   const int m = w.m;
   GmresDev* d = w.st;
   const int* skip = &d->done;
-  const int* frozen = &d->frozen;
   const Members mm = wmembers(w, km);
   const dim3 gr(kRedBlocks, km), ge(nblk(n), km), g1(1, km);
   const bool right = side == VOX_PREC_RIGHT && pc, left = side == VOX_PREC_LEFT && pc;
@@ -908,19 +909,41 @@ static vox_status enqueue_cycle(vox_op_s* op, vox_precond_s* pc, int side, int k
       *nk += 3 + ((right || left) ? 3 : 0) + 4;
     }
   }
+  // x += V y and r = V res (pgmres_iter.m:133-150).  With a right
+  // preconditioner x accumulates u = sum over the cycles of V y, and the solve
+  // applies M^{-1} to it once, after its last cycle (right_finish): x = M^{-1} u
+  // by linearity, with one preconditioner apply per solve instead of one per
+  // cycle (the restart residual r = V res needs no x)
   k_cycle_ls<<<g1, 32, 0, st>>>(d, 0);
-  if (right) {
-    k_cycle_vy<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.w, n, w.vs, 0);
-    VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, frozen, mm));
-    k_axpy<R><<<ge, 256, 0, st>>>(d, w.x, w.t, n, w.vs, 0);
-    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, (Cx<R>*)nullptr, w.r, n, w.vs, 0);
-    *nk += 7;
-  } else {
-    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs, 0);
-    *nk += 2;
-  }
+  k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs, 0);
+  *nk += 2;
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
+}
+
+// Right preconditioning: x = M^{-1} x for the members with sel[b] != 0, after
+// their last cycle (x holds u = sum of the cycles' V y).  One launch sequence
+// for all selected members.
+template <typename R>
+static vox_status right_finish(vox_op_s* op, vox_precond_s* pc, int km, const char* sel,
+                               cudaStream_t st) {
+  GmresWork<R>& w = work<R>(op);
+  bool any = false;
+  for (int b = 0; b < km; b++) {
+    w.hsel[b] = sel[b] ? 0 : 1;  // skip flags
+    any = any || sel[b];
+  }
+  if (!any) return VOX_OK;
+  VOX_CUDA(cudaMemcpyAsync(w.dsel, w.hsel, km * sizeof(int), cudaMemcpyHostToDevice, st));
+  Members mm = wmembers(w, km);
+  mm.fs = 1;
+  VOX_TRY(pc_apply<R>(pc, w.x, w.t, st, w.dsel, mm));
+  const long long n = op->g.n;
+  k_copy_members<R><<<dim3(nblk(n), km), 256, 0, st>>>(n, w.t, w.x, w.dsel, w.vs, 1);
+  VOX_CUDA(cudaGetLastError());
+  op->launches += 4;
+  // the pinned skip flags are reused by the next call: wait for the copy
+  return wait_stream(st);
 }
 
 // Step mode needs the two-read Gram-Schmidt (restart + 1 <= kGsMaxCols).
@@ -948,7 +971,6 @@ static vox_status enqueue_steps(vox_op_s* op, vox_precond_s* pc, int side, int k
   const int m = w.m;
   GmresDev* d = w.st;
   const int* skip = &d->done;
-  const int* noend = &d->noend;
   const Members mm = wmembers(w, km);
   const dim3 gr(kRedBlocks, km), ge(nblk(n), km), g1(1, km);
   const bool right = side == VOX_PREC_RIGHT && pc, left = side == VOX_PREC_LEFT && pc;
@@ -974,19 +996,12 @@ static vox_status enqueue_steps(vox_op_s* op, vox_precond_s* pc, int side, int k
     k_gs_pass<R, false><<<gp, kGsThreads, sm, st>>>(d, -1, w.V, ld, wv, n, w.vs, 0, 0);
     k_gs_pass<R, true><<<gp, kGsThreads, sm, st>>>(d, -1, w.V, ld, wv, n, w.vs, 0, 0);
     k_gs_finish<R><<<ge, kRedThreads, 0, st>>>(d, -1, w.V, ld, wv, w.V, n, w.vs, w.c);
+    // x += V y, r = V res (with a right preconditioner x accumulates u; the
+    // lane applies M^{-1} when the inner solve ends: right_finish)
     k_cycle_ls<<<g1, 32, 0, st>>>(d, 1);
-    if (right) {
-      k_cycle_vy<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.w, n, w.vs, 1);
-      VOX_TRY(pc_apply<R>(pc, w.w, w.t, st, noend, mm));
-      k_axpy<R><<<ge, 256, 0, st>>>(d, w.x, w.t, n, w.vs, 1);
-      k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, (Cx<R>*)nullptr, w.r, n, w.vs, 1);
-      *nk += 7;
-    } else {
-      k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs, 1);
-      *nk += 2;
-    }
+    k_cycle_update<R><<<ge, 256, 0, st>>>(d, w.V, ld, w.x, w.r, n, w.vs, 1);
     k_step_end<<<1, 32, 0, st>>>(d, km);
-    *nk += 4 + 3 + ((right || left) ? 3 : 0) + 3 + 1;
+    *nk += 4 + 3 + ((right || left) ? 3 : 0) + 3 + 3;
   }
   VOX_CUDA(cudaGetLastError());
   return VOX_OK;
@@ -1201,6 +1216,11 @@ static vox_status pgmres_dev(vox_op_s* op, vox_precond_s* pc, int side, int km, 
     if (!take[b] || bnorm[b] == 0.0) continue;
     info[b]->iter_inner = p[b];
     info[b]->iter_outer = outit[b];
+  }
+  if (side == VOX_PREC_RIGHT) {
+    std::vector<char> sel(km, 0);
+    for (int b = 0; b < km; b++) sel[b] = take[b] && bnorm[b] != 0.0;
+    VOX_TRY(right_finish<R>(op, pc, km, sel.data(), st));
   }
   return VOX_OK;
 }
