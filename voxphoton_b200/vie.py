@@ -414,10 +414,11 @@ def solve_refined(A: Operator, b, tol=1e-5, restart=50, maxit_inner=20, inner_to
 
 class Lane:
     """Continuous batching on a batched operator (vox_lane_*): every member
-    runs its own complex64 + FP64-refinement solve, all members' restart
-    cycles share one launch per kernel, and a member takes a new right-hand
-    side as soon as its previous solve is collected.  Each result equals
-    solve_refined on that member alone."""
+    runs its own complex64 + FP64-refinement solve, all members' Arnoldi steps
+    share one launch per kernel (each member at its own point of its own
+    cycle), and a member takes a new right-hand side as soon as its previous
+    solve is collected.  Each result equals solve_refined on that member
+    alone."""
 
     def __init__(self, op: Operator, pc=None, side="left", tol=1e-5, restart=50, maxit_inner=40,
                  inner_tol=0.0, max_refine=10):
@@ -443,8 +444,10 @@ class Lane:
                                            ctypes.c_void_p(x_ptr)))
 
     def step(self):
-        """One restart cycle of every solving member; returns the members that
-        finished."""
+        """Advance every solving member (VOX_LANE_STEPS Arnoldi steps with the
+        members' cycles out of phase, default 2; whole restart cycles for
+        restart > 50 or VOX_LANE_STEPS=0), refine the members whose inner solve
+        ended; returns the members that finished."""
         nd = ctypes.c_int()
         check(lib().vox_lane_step(self._h, self._done, ctypes.byref(nd)))
         return [self._done[i] for i in range(nd.value)]
