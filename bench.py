@@ -217,6 +217,26 @@ def kernel_bytes(op_info, shape, n, pc_info, k, c=8):
     return b
 
 
+def matvec_roofline(op_info, shape, n, pc_info, members, ms, hbm, c=8):
+    """The matvec chain's bytes, achieved GB/s and fraction of the HBM peak for
+    one launch of `members` members taking `ms` milliseconds, on two byte
+    counts: the kernels' own (kernel_bytes: vector, index map, the x-frequency
+    planes once each way, the stored fN octant) and the compulsory figure of
+    the full padded product, c * (7V + 6P) per member (J in, Mc, out and the
+    six fN components over the P = Px Py Pz padded cells)."""
+    L, M, N = shape
+    V = L * M * N
+    P = op_info["Px"] * op_info["Py"] * op_info["Pz"]
+    kb = kernel_bytes(op_info, shape, n, pc_info, 20, c)
+    own = members * (kb["mv_xfwd"] + kb["mv_plane"] + kb["mv_xinv"])
+    full = members * c * (7 * V + 6 * P)
+    s = ms * 1e-3
+    return {"bytes_per_launch": own, "ms": ms, "achieved": own / s / 1e9,
+            "frac": own / s / 1e9 / hbm,
+            "compulsory_full_fN": {"bytes_per_launch": full, "achieved": full / s / 1e9,
+                                   "frac": full / s / 1e9 / hbm}}
+
+
 def _cpu_geometry():
     """voxphoton_b200/geometry.py (numpy only) loaded from its file: importing
     the package would load libvox, which the CPU reference path never touches."""
@@ -530,19 +550,15 @@ def run_sweep(args, world, rank, local):
     alg = info_m["n_blocks"] * n3 * n3 * 8 + 2 * K * L * n3 * 8
     hbm, src = peaks()
     ach = alg / (stage["pc_solve"] * 1e-3) / 1e9
-    mvb = kernel_bytes(op_m.info(), fmid.p.shape, fmid.idx.size, info_m, 20)
-    mv_bytes = K * (mvb["mv_xfwd"] + mvb["mv_plane"] + mvb["mv_xinv"])
     mv_ms = stage["mv_xfwd"] + stage["mv_plane"] + stage["mv_xinv"]
+    mv_roof = matvec_roofline(op_m.info(), fmid.p.shape, fmid.idx.size, info_m, K, mv_ms, hbm)
     roof = {"bound": "hbm", "kernel": f"pc_solve (k_pc_inv_stream, {K} members, "
                                       f"{L}x{M}x{N})",
             "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
             "traffic": measured_traffic("pc_solve", alg), "peak_source": src,
             "bytes_per_launch": alg, "ms_per_launch": stage["pc_solve"],
             "stage_ms": stage,
-            "matvec": {"kernels": "k_xfwd + k_plane64 + k_xinv", "members": K,
-                       "bytes_per_launch": mv_bytes, "ms": mv_ms,
-                       "achieved": mv_bytes / (mv_ms * 1e-3) / 1e9,
-                       "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm}}
+            "matvec": {"kernels": "k_xfwd + k_plane64 + k_xinv", "members": K, **mv_roof}}
     # the lanes are done: free them and the staged vectors before the baseline
     del dev_b, dev_x
     srv.close_pool()

@@ -157,3 +157,19 @@ def test_jvie_solve_argument_checks_need_no_device():
     d.dx = 0.0
     st = lib.vox_jvie_solve(ctypes.byref(d), _lib.dptr(out_re), _lib.dptr(out_im), None)
     assert st == _lib.VOX_ERR_BAD_ARG
+
+
+def test_bench_matvec_roofline_byte_counts():
+    # the bench's matvec line on the 1160 x 30 x 11 grating at 4 members: its
+    # own bytes and the compulsory full-fN figure c (7V + 6P) per member
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    info = {"Px": 2560, "Py": 64, "Pz": 24, "n": 963600, "octant_fN": True}
+    pcinfo = {"n_blocks": 581, "ld": 992, "paired": True}
+    r = bench.matvec_roofline(info, (1160, 30, 11), 963600, pcinfo, 4, 0.6, 6536.7)
+    V, P = 1160 * 30 * 11, 2560 * 64 * 24
+    assert r["compulsory_full_fN"]["bytes_per_launch"] == 4 * 8 * (7 * V + 6 * P)
+    assert abs(r["bytes_per_launch"] - 571420608) < 1
+    assert abs(r["frac"] - r["bytes_per_launch"] / 0.6e-3 / 1e9 / 6536.7) < 1e-12
