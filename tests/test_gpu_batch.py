@@ -119,7 +119,7 @@ def test_stage_profile_of_a_batch(family):
 
 
 @pytest.mark.parametrize("side,steps", [("left", "4"), ("right", "4"), ("right", "1"),
-                                        ("right", "7"), ("left", "0")])
+                                        ("right", "7"), ("left", "0"), ("right", "0")])
 def test_lane_refills_members_and_matches_solo_solves(family, monkeypatch, side, steps):
     # 5 requests on 3 members: slots are refilled while other members are
     # mid-solve; every result must equal the single-right-hand-side solve.
