@@ -543,7 +543,9 @@ __global__ void k_cycle_ls(GmresDev* st, int step) {
   }
 }
 
-// x += V(:,0:kk-1) y ; r = V(:,0:kk) res   (pgmres_iter.m:133-150, no right preconditioner)
+// x += V(:,0:kk-1) y ; r = V(:,0:kk) res   (pgmres_iter.m:133-150).  With a right
+// preconditioner x accumulates u = sum of the cycles' V y, to which the solve
+// applies M^{-1} once after its last cycle.
 template <typename R>
 __global__ void k_cycle_update(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
                                Cx<R>* x, Cx<R>* r, long long n, long long vs, int step) {
@@ -573,40 +575,6 @@ __global__ void k_cycle_update(const GmresDev* st, const Cx<R>* __restrict__ V, 
     r[i] = ri;
   }
 }
-
-// y = V(:,0:kk-1) * ys (for the right-preconditioned update, into a temp)
-template <typename R>
-__global__ void k_cycle_vy(const GmresDev* st, const Cx<R>* __restrict__ V, long long ldv,
-                           Cx<R>* out, long long n, long long vs, int step) {
-  __shared__ Cx<R> ys[kMaxRestart];
-  st += blockIdx.y;
-  V += blockIdx.y * vs;
-  out += blockIdx.y * vs;
-  if (step ? !st->endnow : st->frozen) return;
-  const int kk = st->k;
-  for (int j = threadIdx.x; j < kk; j += blockDim.x) ys[j] = from_d2<Cx<R>>(st->y[j]);
-  __syncthreads();
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    Cx<R> acc = czero<Cx<R>>();
-    for (int j = 0; j < kk; j++) cfma(acc, V[j * ldv + i], ys[j]);
-    out[i] = acc;
-  }
-}
-
-// elementwise helpers
-template <typename R>
-__global__ void k_axpy(const GmresDev* st, Cx<R>* y, const Cx<R>* __restrict__ x, long long n,
-                       long long vs, int step) {
-  st += blockIdx.y;
-  y += blockIdx.y * vs;
-  x += blockIdx.y * vs;
-  if (step ? !st->endnow : st->frozen) return;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    y[i] = cadd(y[i], x[i]);
-}
-
 
 // ------------------------------------------- Gram-Schmidt in two basis reads
 // For restart lengths up to kGsMaxCols - 1 an Arnoldi step reads the basis in
