@@ -84,6 +84,10 @@ def test_bragg10_matvec_c64_against_oracle_and_100_inputs(bragg10):
     del fN
     assert _rel(op.mv_AN(xs[0], prec="c128"), ref) < 1e-12
     assert _rel(op.mv_AN(xs[0], prec="c64"), ref) < 1e-5
+    # the oracle takes minutes per input at this size (24.5 M padded cells), so
+    # the other 99 inputs are checked against the complex128 product, which the
+    # line above ties to the oracle at 1e-12: the complex64 error bound holds
+    # against the oracle to within that
     worst = max(_rel(op.mv_AN(x, prec="c64"), op.mv_AN(x, prec="c128")) for x in xs)
     assert worst < 1e-5
 
